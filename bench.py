@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Decoded info Gbit/s of the fixed-point LDPC decoder on B200 GPUs.
+
+Workload (one step = one decode of one batch):
+  seeded regular (3,6) QC-LDPC, 8x16 base of Z=256 circulants (N=4096, K=2048,
+  4-cycle free), random info bits through the systematic encoder, BPSK over AWGN
+  at Eb/N0 = 2.0 dB, int8 LLRs quantised like the reference channel
+  (q = trunc(clamp(8y, -31, 31)), awgn_channel/CChanel_AWGN_SIMD.cu:21-24),
+  offset-min-sum (offset 1), 10 layered iterations, 65536 frames per GPU.
+
+  value : kernel-only throughput, LLRs already resident in HBM (268 MB per batch,
+          larger than the 126 MB L2, so no flush is needed between steps)
+  e2e   : the same metric through the reference-facing host call
+          (ldpc_decode_host: pinned host LLRs in, 0/1 bytes out, copies timed)
+
+python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU: torchrun ... bench.py --gpus N (weak scaling: every rank decodes its own batch).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "qc(3,6) N=4096 K=2048 Z=256 OMS offset1 10 layered iterations, 65536 frames, Eb/N0 2.0 dB"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=65536)
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--kind", default="OMS")
+    ap.add_argument("--pack", default="AUTO")
+    ap.add_argument("--ebn0", type=float, default=2.0)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    return ap.parse_args()
+
+
+def make_workload(frames, ebn0, seed, rank=0):
+    """Codewords + quantised channel LLRs (int8, frame-major) for `frames` frames."""
+    from fast_ldpc_decoder_for_gpu_fixed_b200.codes import Encoder, qc_regular
+    code = qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
+    enc = Encoder(code)
+    rng = np.random.default_rng(seed + 7919 * rank)
+    distinct = min(frames, 1024)
+    cws = enc.encode(rng.integers(0, 2, size=(distinct, enc.k)))
+    idx = np.arange(frames) % distinct
+    rate = enc.k / code.n
+    sigma = np.sqrt(10.0 ** (-(ebn0 + 10 * np.log10(rate)) / 10.0) / 2.0)
+    llr = np.empty((frames, code.n), dtype=np.int8)
+    step = 4096
+    for f0 in range(0, frames, step):
+        f1 = min(frames, f0 + step)
+        y = (2.0 * cws[idx[f0:f1]].astype(np.float32) - 1.0) + sigma * rng.standard_normal((f1 - f0, code.n), dtype=np.float32)
+        llr[f0:f1] = np.trunc(np.clip(8.0 * y, -31.0, 31.0)).astype(np.int8)
+    return code, enc, cws, idx, llr, sigma
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.t.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(code, llr, iters, kind, budget_s, info_bits):
+    """The reference's kernel arithmetic restated on the host CPU (AVX2, all threads) on a
+    bounded sample of the same batch; returns (Gbit/s, cores, sample description)."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    probe = min(llr.shape[0], 1024)
+    t = time.perf_counter()
+    oracle.decode_batch(code, kind, llr[:probe], iters, nthreads=cores)
+    dt = time.perf_counter() - t
+    frames = int(min(llr.shape[0], max(probe, probe * budget_s / max(dt, 1e-6)))) // 32 * 32
+    t = time.perf_counter()
+    oracle.decode_batch(code, kind, llr[:frames], iters, nthreads=cores)
+    dt = time.perf_counter() - t
+    return frames * info_bits / dt / 1e9, cores, "%d of the batch's frames, %d iterations, %.1f s" % (frames, iters, dt)
+
+
+def run_reference(args):
+    """Reference arm: the reference has no CPU decoder, so its fixed-point kernel arithmetic is
+    timed as the CPU port (oracle/ldpc_oracle_batch.c) on the host cores, per step a bounded sample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    code, enc, cws, idx, llr, sigma = make_workload(min(args.frames, 65536), args.ebn0, args.seed)
+    per_step = max(1.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(code, llr, args.iters, args.kind, min(per_step, 2.0), enc.k)
+    vals, samples = [], []
+    cores = os.cpu_count() or 1
+    for _ in range(args.steps):
+        v, cores, s = cpu_baseline(code, llr, args.iters, args.kind, per_step, enc.k)
+        vals.append(v)
+        samples.append(s)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 4096 * 1000.0 / (value * 1e9) * 1e3 * 0 + (65536 * enc.k / (value * 1e9)) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+            "data": "synthetic (seeded QC codewords, AWGN)",
+            "config": {"workload": WORKLOAD, "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": "Gbit/s", "cores": cores, "kind": "port",
+                             "sample": samples[-1]},
+            "e2e": {"value": value, "unit": "Gbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    code, enc, cws, idx, llr, sigma = make_workload(args.frames, args.ebn0, args.seed, rank)
+    words = args.frames // 4
+    dec = Decoder(code, args.kind, nb_frames=words, pack=args.pack)
+    info = dec.info()
+    stream = torch.cuda.current_stream()
+    d_llr = torch.from_numpy(llr.reshape(-1)).cuda()
+    d_out = torch.empty(args.frames * code.n, dtype=torch.uint8, device="cuda")
+    launches = 0
+
+    def step():
+        dec.decode_device(d_llr, d_out, words, args.iters, _lib.OUT_BYTES, None, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # error rates of this batch (not timed)
+    hard = d_out.view(args.frames, code.n)
+    ref_bits = torch.from_numpy(cws).cuda()[torch.from_numpy(idx).cuda()]
+    err = (hard != ref_bits).sum(dim=1)
+    fer = float((err > 0).float().mean())
+    ber = float(err.sum()) / (args.frames * code.n)
+    del ref_bits, err, hard
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    info_bits = args.frames * enc.k
+    value = world * info_bits * args.steps / (ms_max * 1e-3) / 1e9
+
+    # roofline of the decode kernel (one launch per step)
+    edge_updates = args.frames * code.e * args.iters
+    int_peak = _int_peak()
+    alg_ops = 2.0 * edge_updates          # 8 int8 lane-ops per edge-update at 4 lanes per 32-bit word
+    achieved = alg_ops / (ms_step * 1e-3) / 1e12
+    hbm_bytes = args.frames * code.n * 2  # int8 LLRs in + 0/1 bytes out
+    peaks = _measured_peaks()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = _e2e(dec, llr, args, info_bits, world)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        v, cores, sample = cpu_baseline(code, llr, args.iters, args.kind, args.cpu_seconds, enc.k)
+        cpu = {"value": v, "unit": "Gbit/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+            "data": "synthetic (seeded QC codewords, AWGN, reference quantiser)",
+            "config": {"workload": WORKLOAD, "kind": args.kind, "pack": info["pack"], "frames_per_gpu": args.frames,
+                       "iterations": args.iters, "ebn0_db": args.ebn0, "fer": fer, "ber": ber,
+                       "l2": "inputs (268 MB) larger than L2; no flush", "parallelism": "replicas" if world > 1 else "1gpu",
+                       "threads_per_cta": info["threads"], "smem_per_cta": info["smem"],
+                       "ctas_per_sm": info["ctas_per_sm"], "regs": info["regs"]},
+            "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
+                         "frac": achieved / int_peak, "traffic": None,
+                         "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
+                         "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, all SMs)"},
+            "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
+                             "unit": "GB/s", "frac": (hbm_bytes / (ms_step * 1e-3) / 1e9) / peaks["hbm_gbs"]
+                             if peaks.get("hbm_gbs") else None, "alg_bytes_per_launch": hbm_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    dec.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def _int_peak():
+    """INT32 lane-op peak of one B200 in T ops/s: measured issue rate of independent
+    LOP3/IADD3 chains (profiles/int_peak.md) x 148 SMs x the max SM clock."""
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
+    import ctypes
+    v = ctypes.c_double()
+    _lib.check(_lib.lib().ldpc_probe_int_peak(ctypes.byref(v), None))
+    return v.value / 1e12
+
+
+def _e2e(dec, llr, args, info_bits, world):
+    """Host-buffer decode through the reference-facing call, copies inside the timed region."""
+    import torch
+    n = llr.shape[1]
+    h_in = torch.from_numpy(llr.reshape(-1)).pin_memory()
+    h_out = torch.empty(args.frames * n, dtype=torch.uint8).pin_memory()
+    a_in, a_out = h_in.numpy(), h_out.numpy()
+    steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        dec.decode_host(a_in, a_out, args.iters)
+    t = time.perf_counter()
+    for _ in range(steps):
+        dec.decode_host(a_in, a_out, args.iters)
+    dt = time.perf_counter() - t
+    chunks = min(8, max(1, (args.frames // 4) // 256))
+    return {"value": world * info_bits * steps / dt / 1e9, "unit": "Gbit/s", "ms_per_step": dt * 1e3 / steps,
+            "h2d_bytes_per_step": int(llr.size), "d2h_bytes_per_step": int(llr.size),
+            "host_buffers": "pinned", "gpu_launches_per_step": chunks, "steps": steps}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,304 @@
+// Level-scheduled, row-layered fixed-point LDPC decoder kernel for sm_100a.
+//
+// One CTA decodes one group of 4 frames (the 4 frames 4g..4g+3 that the
+// reference packs into 32-bit word g), with the whole decoder state on chip:
+// the APP array and every c->v message of the group live in shared memory for
+// all iterations.  The reference instead gives one thread per word and walks
+// every check row serially with APP and messages in global memory
+// (decoder_oms/cuda/CUDA_OMS_SIMD.cu:25-248, launched with nb_frames/128 CTAs
+// of 128 threads, decoder_oms/CGPU_Decoder_OMS_SIMD.cu:119).
+//
+// Bit-exactness with the reference's strictly row-serial, update-in-place
+// order comes from the schedule built on the host (ldpc_b200.cu): rows are
+// grouped into "levels" such that a row's level is one more than the highest
+// level of any earlier row sharing a variable with it.  Rows of one level touch
+// disjoint variables, so the CTA's threads update them concurrently and the
+// result equals the serial order; a barrier separates levels and iterations.
+// Rows are renumbered in schedule order (r'), so the threads of a level read
+// consecutive entries of the column table and of the message store.
+//
+// Per-word early termination (2NMS): the OR over rows of the extrinsic sign
+// parity decides, from the second iteration on, whether the word stops
+// (decoder_2nms/cuda/CUDA_2NMS_SIMD.cu:160-290); here that OR is reduced over
+// the CTA with __syncthreads_or.
+#pragma once
+#include <cstdint>
+#include "packs.cuh"
+
+namespace ldpc {
+
+struct Plan {
+    int n;           // variables
+    int npad;        // n rounded up to 16 (APP row stride in shared memory)
+    int m;           // rows (checks)
+    int dmax;        // largest row degree
+    int nlevels;     // levels per iteration
+    const uint16_t* cols;   // [dmax][m] variable of edge j of row r' (schedule order)
+    const uint8_t* rowdeg;  // [m]
+    const uint8_t* rowcls;  // [m] 1 = reference's second degree group
+    const int2* levels;     // [nlevels] (first r', row count)
+    const int32_t* edge_orig;  // [dmax][m] edge index in table order (state dumps)
+};
+
+struct Job {
+    const int8_t* llr;    // frame-major int8 [4*words][n] (or word-interleaved, see interleaved)
+    void* out;            // hard decisions (LDPC_OUT_BYTES or LDPC_OUT_PACKED)
+    int out_packed;
+    int interleaved;      // 1: llr is word[v*total_words + g] (xMS input)
+    long long total_words;  // word stride of the interleaved layout and of the state dumps
+    long long word0;      // first word of this launch within the batch
+    int iters;
+    int quirk;            // 1: OMS first-iteration no-clip on second-group rows
+    int32_t* iters_out;   // [words] or null
+    int8_t* app_out;      // state dumps (reference device layouts) or null
+    int8_t* msg_out;
+};
+
+// ---- prologue / epilogue: frame-major global <-> packed shared memory ----
+
+// 4x4 byte transpose: in[k] = 4 consecutive bytes of frame k; out[j] = byte j of all 4 frames
+__device__ __forceinline__ void transpose4x4(const uint32_t (&a)[4], uint32_t (&w)[4])
+{
+    uint32_t t0 = __byte_perm(a[0], a[1], 0x5140), t1 = __byte_perm(a[2], a[3], 0x5140);
+    uint32_t t2 = __byte_perm(a[0], a[1], 0x7362), t3 = __byte_perm(a[2], a[3], 0x7362);
+    w[0] = __byte_perm(t0, t1, 0x5410);
+    w[1] = __byte_perm(t0, t1, 0x7632);
+    w[2] = __byte_perm(t2, t3, 0x5410);
+    w[3] = __byte_perm(t2, t3, 0x7632);
+}
+
+// Reads the group's 4 frames; calls put(v, word) with the 4-frame byte word of variable v.
+template <class F>
+__device__ __forceinline__ void read_group(const Plan& P, const Job& J, long long g, F put)
+{
+    const int n = P.n;
+    if (J.interleaved) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(J.llr);
+        for (int v = threadIdx.x; v < n; v += blockDim.x) put(v, __ldg(src + (long long)v * J.total_words + g));
+    } else if ((n & 3) == 0) {
+        const uint32_t* f0 = reinterpret_cast<const uint32_t*>(J.llr + (4 * (g - J.word0)) * (long long)n);
+        const int n4 = n >> 2;
+        for (int q = threadIdx.x; q < n4; q += blockDim.x) {
+            uint32_t a[4], w[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) a[k] = __ldg(f0 + k * n4 + q);
+            transpose4x4(a, w);
+#pragma unroll
+            for (int j = 0; j < 4; j++) put(4 * q + j, w[j]);
+        }
+    } else {
+        const int8_t* f0 = J.llr + (4 * (g - J.word0)) * (long long)n;
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) w |= (uint32_t)(uint8_t)__ldg(f0 + k * n + v) << (8 * k);
+            put(v, w);
+        }
+    }
+}
+
+// Writes hard decisions; get(v) returns the 4-frame byte word (values as x) of variable v.
+template <class F>
+__device__ __forceinline__ void write_group(const Plan& P, const Job& J, long long g, F get)
+{
+    const int n = P.n;
+    const long long lg = g - J.word0;
+    if (!J.out_packed) {
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + 4 * lg * n;
+        if ((n & 3) == 0) {
+            const int n4 = n >> 2;
+            uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+            for (int q = threadIdx.x; q < n4; q += blockDim.x) {
+                uint32_t a[4], w[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) a[j] = __vsetgts4(get(4 * q + j), 0u);
+                transpose4x4(a, w);
+#pragma unroll
+                for (int k = 0; k < 4; k++) o32[k * n4 + q] = w[k];
+            }
+        } else {
+            for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                uint32_t h = __vsetgts4(get(v), 0u);
+#pragma unroll
+                for (int k = 0; k < 4; k++) o[k * n + v] = (h >> (8 * k)) & 1;
+            }
+        }
+    } else {
+        const int nb = (n + 7) >> 3;
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + 4 * lg * nb;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            uint32_t acc = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                int v = 8 * b + j;
+                if (v < n) acc |= __vsetgts4(get(v), 0u) << j;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k * nb + b] = (acc >> (8 * k)) & 0xff;
+        }
+    }
+}
+
+// ---- pack-specific state access (x values as 4-frame byte words) ----
+
+template <class PK> struct Access;
+
+template <> struct Access<PackSIMD4> {
+    __device__ __forceinline__ static void put(uint32_t* app, int npad, int v, uint32_t w) { app[v] = w; }
+    __device__ __forceinline__ static uint32_t get(const uint32_t* app, int npad, int v) { return app[v]; }
+    __device__ __forceinline__ static uint32_t get_msg(const uint32_t* msg, int stride, int idx) { return msg[idx]; }
+};
+
+__device__ __forceinline__ uint32_t neg_half_to_byte(uint16_t h)
+{
+    // integer-valued fp16 u in [-127,128] -> byte of x = -u (x in [-128,127])
+    int u = __half2int_rn(__ushort_as_half(h));
+    return (uint32_t)(uint8_t)(int8_t)(-u);
+}
+
+template <> struct Access<PackF16x2> {
+    __device__ __forceinline__ static uint32_t pair(uint32_t w, int k0)
+    {
+        int a = -(int)(int8_t)(w >> (8 * k0)), b = -(int)(int8_t)(w >> (8 * k0 + 8));
+        __half2 h = __halves2half2(__int2half_rn(a), __int2half_rn(b));
+        return h2u(h);
+    }
+    __device__ __forceinline__ static void put(uint32_t* app, int npad, int v, uint32_t w)
+    {
+        app[v] = pair(w, 0);
+        app[npad + v] = pair(w, 2);
+    }
+    __device__ __forceinline__ static uint32_t unpair(uint32_t lo, uint32_t hi)
+    {
+        return neg_half_to_byte(lo & 0xffff) | (neg_half_to_byte(lo >> 16) << 8) |
+               (neg_half_to_byte(hi & 0xffff) << 16) | (neg_half_to_byte(hi >> 16) << 24);
+    }
+    __device__ __forceinline__ static uint32_t get(const uint32_t* app, int npad, int v)
+    {
+        return unpair(app[v], app[npad + v]);
+    }
+    __device__ __forceinline__ static uint32_t get_msg(const uint32_t* msg, int stride, int idx)
+    {
+        return unpair(msg[idx], msg[stride + idx]);
+    }
+};
+
+template <> struct Access<PackI8> {
+    __device__ __forceinline__ static void put(int8_t* app, int npad, int v, uint32_t w)
+    {
+#pragma unroll
+        for (int k = 0; k < 4; k++) app[k * npad + v] = (int8_t)(w >> (8 * k));
+    }
+    __device__ __forceinline__ static uint32_t get(const int8_t* app, int npad, int v)
+    {
+        uint32_t w = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) w |= (uint32_t)(uint8_t)app[k * npad + v] << (8 * k);
+        return w;
+    }
+    __device__ __forceinline__ static uint32_t get_msg(const int8_t* msg, int stride, int idx)
+    {
+        uint32_t w = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) w |= (uint32_t)(uint8_t)(int8_t)(-msg[k * stride + idx]) << (8 * k);
+        return w;
+    }
+};
+
+// ---- one check row over all storage words of the group ----
+
+template <class PK, int KIND, int DT, bool EXACT>
+__device__ __forceinline__ void row_update(typename PK::S* app, typename PK::S* msg, const Plan& P,
+                                           int r, int d, bool noclip, typename PK::R& ov)
+{
+    using R = typename PK::R;
+    int v[DT];
+#pragma unroll
+    for (int j = 0; j < DT; j++)
+        if (EXACT || j < d) v[j] = __ldg(P.cols + j * P.m + r);
+    const int mstride = P.dmax * P.m;
+#pragma unroll
+    for (int w = 0; w < PK::WPC; w++) {
+        typename PK::S* A = app + w * P.npad;
+        typename PK::S* M = msg + w * mstride;
+        R x[DT], mm[DT];
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                x[j] = PK::ld_app(A + v[j]);
+                mm[j] = PK::ld_msg(M + j * P.m + r);
+            }
+        }
+        PK::template update<KIND, DT, EXACT>(x, mm, d, noclip, ov);
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                PK::st_msg(M + j * P.m + r, mm[j]);
+                PK::st_app(A + v[j], x[j]);
+            }
+        }
+    }
+}
+
+template <class PK, int KIND, int DT, bool EXACT>
+__global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const Job J)
+{
+    using S = typename PK::S;
+    using R = typename PK::R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S* app = reinterpret_cast<S*>(smem_raw);
+    S* msg = app + PK::WPC * P.npad;
+    const long long g = J.word0 + blockIdx.x;
+
+    read_group(P, J, g, [&](int v, uint32_t w) { Access<PK>::put(app, P.npad, v, w); });
+    {
+        const int msg_bytes = PK::WPC * P.dmax * P.m * (int)sizeof(S);
+        uint32_t* mz = reinterpret_cast<uint32_t*>(msg);
+        for (int i = threadIdx.x; i < msg_bytes / 4; i += blockDim.x) mz[i] = 0;
+    }
+    __syncthreads();
+
+    int executed = 0;
+    for (int it = 0; it < J.iters; it++) {
+        R ov = 0;
+        const bool first = (it == 0);
+        for (int l = 0; l < P.nlevels; l++) {
+            const int2 lv = __ldg(P.levels + l);
+            for (int r = lv.x + threadIdx.x; r < lv.x + lv.y; r += blockDim.x) {
+                const int d = EXACT ? DT : __ldg(P.rowdeg + r);
+                const bool noclip = J.quirk && first && __ldg(P.rowcls + r);
+                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov);
+            }
+            __syncthreads();
+        }
+        executed = it + 1;
+        if (KIND == KIND_2NMS && it >= 1) {
+            if (!__syncthreads_or(ov != 0)) break;
+        }
+    }
+
+    write_group(P, J, g, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+    if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
+    if (J.app_out) {
+        uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x)
+            ao[(long long)v * J.total_words + g] = Access<PK>::get(app, P.npad, v);
+    }
+    if (J.msg_out) {
+        uint32_t* mo = reinterpret_cast<uint32_t*>(J.msg_out);
+        const int mstride = P.dmax * P.m;
+        for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) {
+            const int j = i / P.m, r = i - j * P.m;
+            if (j < P.rowdeg[r])
+                mo[(long long)P.edge_orig[i] * J.total_words + g] = Access<PK>::get_msg(msg, mstride, i);
+        }
+    }
+}
+
+}  // namespace ldpc
+
+// Kernel variants: EXACT<D> for codes whose rows all have degree D, else the
+// smallest bucket DT >= the largest row degree (rows shorter than DT predicate
+// the unused edge slots off).
+#define LDPC_DEGREE_VARIANTS(X, PK, KIND) \
+    X(PK, KIND, 6, true) X(PK, KIND, 7, true) X(PK, KIND, 8, false) X(PK, KIND, 16, false) X(PK, KIND, 32, false)

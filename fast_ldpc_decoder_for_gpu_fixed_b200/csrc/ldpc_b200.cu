@@ -1,0 +1,615 @@
+// C ABI of the B200 fixed-point LDPC decoding engine (declared in include/ldpc_b200.h).
+//
+// Host-side responsibilities:
+//   * code objects: the H matrix as CSR rows in the reference's layer order
+//     (src/matrix/<code>/constantes_decoder.h:3 + constantes_gpu.h:6-16), and
+//     the level schedule that lets rows of one level run concurrently while
+//     reproducing the reference's serial in-place row order bit for bit;
+//   * decoder objects (src/decoder_template/CGPUDecoder.cpp:14-54 and the
+//     plugin constructors): device copies of the schedule, the I/O staging
+//     buffers the reference keeps in device_V / d_MSG_C_2_V, streams;
+//   * decode calls: host buffers (the reference's synchronous decode(),
+//     src/decoder_oms/CGPU_Decoder_OMS_SIMD.cu:97-147) with the H2D copy,
+//     decoding and D2H copy pipelined over chunks of words; device buffers on a
+//     caller stream.
+// Errors are status codes plus a per-thread message; nothing exits the
+// process (the reference's ERROR_CHECK prints and exit(0)s,
+// src/custom_api/custom_cuda.cu:5-17).
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ldpc_b200.h"
+#include "decode_kernel.cuh"
+
+using namespace ldpc;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(x)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (x);                                                                \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? LDPC_ERR_NOMEM : LDPC_ERR_CUDA,    \
+                        "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+static const int kMaxDegree = 32;
+
+struct ldpc_code {
+    int n = 0, m = 0, e = 0, dmax = 0;
+    std::vector<int32_t> row_ptr, cols;
+    std::vector<uint8_t> row_class;
+    // schedule
+    std::vector<int32_t> order;   // order[r'] = row in table order
+    std::vector<int2> levels;     // (first r', count)
+    int widest = 0;
+};
+
+struct ldpc_decoder {
+    int kind = 0, pack = 0, device = 0;
+    size_t nb_words = 0;
+    int n = 0, m = 0, e = 0;
+    Plan plan{};
+    uint16_t* d_cols = nullptr;
+    uint8_t* d_rowdeg = nullptr;
+    uint8_t* d_rowcls = nullptr;
+    int2* d_levels = nullptr;
+    int32_t* d_edge_orig = nullptr;
+    int8_t* d_in = nullptr;    // staging for decode_host (reference: d_MSG_C_2_V as input staging)
+    uint8_t* d_out = nullptr;  // staging for decode_host (reference: d_MSG_C_2_V as output staging)
+    cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+    int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
+    const void* kfn = nullptr;
+};
+
+// ------------------------------------------------------------------------
+// codes
+// ------------------------------------------------------------------------
+
+static int build_schedule(ldpc_code* c)
+{
+    std::vector<int> lastlev(c->n, -1), level(c->m, 0);
+    int nlev = 0;
+    for (int r = 0; r < c->m; r++) {
+        int L = 0;
+        for (int k = c->row_ptr[r]; k < c->row_ptr[r + 1]; k++) L = std::max(L, lastlev[c->cols[k]] + 1);
+        level[r] = L;
+        for (int k = c->row_ptr[r]; k < c->row_ptr[r + 1]; k++) lastlev[c->cols[k]] = L;
+        nlev = std::max(nlev, L + 1);
+    }
+    c->order.resize(c->m);
+    for (int r = 0; r < c->m; r++) c->order[r] = r;
+    // any order inside a level is exact; group equal degrees to keep warps uniform
+    std::stable_sort(c->order.begin(), c->order.end(), [&](int a, int b) {
+        if (level[a] != level[b]) return level[a] < level[b];
+        int da = c->row_ptr[a + 1] - c->row_ptr[a], db = c->row_ptr[b + 1] - c->row_ptr[b];
+        return da > db;
+    });
+    c->levels.assign(nlev, make_int2(0, 0));
+    for (int i = 0; i < c->m; i++) {
+        int L = level[c->order[i]];
+        if (c->levels[L].y == 0) c->levels[L].x = i;
+        c->levels[L].y++;
+    }
+    c->widest = 0;
+    for (auto& l : c->levels) c->widest = std::max(c->widest, l.y);
+    return LDPC_OK;
+}
+
+static int code_init(ldpc_code* c)
+{
+    c->e = c->row_ptr[c->m];
+    c->dmax = 0;
+    for (int r = 0; r < c->m; r++) {
+        int d = c->row_ptr[r + 1] - c->row_ptr[r];
+        if (d < 1) return fail(LDPC_ERR_ARG, "row %d has no edge", r);
+        c->dmax = std::max(c->dmax, d);
+    }
+    for (int k = 0; k < c->e; k++)
+        if (c->cols[k] < 0 || c->cols[k] >= c->n)
+            return fail(LDPC_ERR_ARG, "edge %d: variable index %d outside [0,%d)", k, c->cols[k], c->n);
+    return build_schedule(c);
+}
+
+extern "C" int ldpc_code_create(ldpc_code** out, int n_vars, int n_checks, const int32_t* row_ptr,
+                                const int32_t* cols, const uint8_t* row_class)
+{
+    if (!out || !row_ptr || !cols || n_vars <= 0 || n_checks <= 0)
+        return fail(LDPC_ERR_ARG, "ldpc_code_create: null pointer or empty code");
+    if (n_vars > 65535) return fail(LDPC_ERR_UNSUPPORTED, "ldpc_code_create: n=%d > 65535", n_vars);
+    if (row_ptr[0] != 0) return fail(LDPC_ERR_ARG, "row_ptr[0] must be 0");
+    for (int r = 0; r < n_checks; r++)
+        if (row_ptr[r + 1] < row_ptr[r]) return fail(LDPC_ERR_ARG, "row_ptr not monotone at %d", r);
+    ldpc_code* c = new ldpc_code();
+    c->n = n_vars;
+    c->m = n_checks;
+    c->row_ptr.assign(row_ptr, row_ptr + n_checks + 1);
+    c->cols.assign(cols, cols + row_ptr[n_checks]);
+    c->row_class.assign(n_checks, 0);
+    if (row_class)
+        for (int r = 0; r < n_checks; r++) c->row_class[r] = row_class[r] ? 1 : 0;
+    int rc = code_init(c);
+    if (rc) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_code_create_from_table(ldpc_code** out, int n, int k_checks, int m_edges, int nb_degres,
+                                           int deg1, int deg1_rows, int deg2, int deg2_rows,
+                                           const uint32_t* pos)
+{
+    if (!out || !pos) return fail(LDPC_ERR_ARG, "ldpc_code_create_from_table: null pointer");
+    if (nb_degres < 1 || nb_degres > 2) return fail(LDPC_ERR_ARG, "nb_degres must be 1 or 2");
+    if (nb_degres == 1) deg2_rows = 0;
+    if (deg1 < 1 || deg1_rows < 0 || (nb_degres == 2 && (deg2 < 1 || deg2_rows < 0)))
+        return fail(LDPC_ERR_ARG, "bad degree groups");
+    if (deg1_rows + deg2_rows != k_checks) return fail(LDPC_ERR_ARG, "row groups do not sum to %d checks", k_checks);
+    if ((long long)deg1 * deg1_rows + (long long)deg2 * deg2_rows != m_edges)
+        return fail(LDPC_ERR_ARG, "row groups do not sum to %d edges", m_edges);
+    std::vector<int32_t> rp(k_checks + 1), cols(m_edges);
+    std::vector<uint8_t> cls(k_checks);
+    rp[0] = 0;
+    for (int r = 0; r < k_checks; r++) {
+        rp[r + 1] = rp[r] + (r < deg1_rows ? deg1 : deg2);
+        cls[r] = r < deg1_rows ? 0 : 1;
+    }
+    for (int i = 0; i < m_edges; i++) cols[i] = (int32_t)pos[i];
+    return ldpc_code_create(out, n, k_checks, rp.data(), cols.data(), cls.data());
+}
+
+extern "C" int ldpc_code_load(ldpc_code** out, const char* path)
+{
+    if (!out || !path) return fail(LDPC_ERR_ARG, "ldpc_code_load: null pointer");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(LDPC_ERR_ARG, "cannot open %s", path);
+    char magic[8];
+    uint32_t hdr[6];
+    int rc = LDPC_OK;
+    if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "LDPCH001", 8) || fread(hdr, 4, 6, f) != 6) {
+        fclose(f);
+        return fail(LDPC_ERR_ARG, "%s: not an .ldpc table", path);
+    }
+    uint32_t n = hdr[0], k = hdr[1], m = hdr[2], ng = hdr[3], cb = hdr[4];
+    if (ng < 1 || ng > 1024 || (cb != 2 && cb != 4) || k == 0 || m == 0) {
+        fclose(f);
+        return fail(LDPC_ERR_ARG, "%s: bad header", path);
+    }
+    std::vector<uint32_t> groups(2 * ng);
+    std::vector<uint32_t> pos(m);
+    if (fread(groups.data(), 4, 2 * ng, f) != 2 * ng) rc = fail(LDPC_ERR_ARG, "%s: truncated", path);
+    if (!rc) {
+        if (cb == 2) {
+            std::vector<uint16_t> p16(m);
+            if (fread(p16.data(), 2, m, f) != m) rc = fail(LDPC_ERR_ARG, "%s: truncated", path);
+            for (uint32_t i = 0; i < m; i++) pos[i] = p16[i];
+        } else if (fread(pos.data(), 4, m, f) != m) {
+            rc = fail(LDPC_ERR_ARG, "%s: truncated", path);
+        }
+    }
+    fclose(f);
+    if (rc) return rc;
+    std::vector<int32_t> rp(1, 0), cols(pos.begin(), pos.end());
+    std::vector<uint8_t> cls;
+    for (uint32_t gi = 0; gi < ng; gi++)
+        for (uint32_t i = 0; i < groups[2 * gi + 1]; i++) {
+            rp.push_back(rp.back() + (int32_t)groups[2 * gi]);
+            cls.push_back(gi > 0 ? 1 : 0);
+        }
+    if (rp.size() != k + 1 || (uint32_t)rp.back() != m) return fail(LDPC_ERR_ARG, "%s: inconsistent groups", path);
+    return ldpc_code_create(out, (int)n, (int)k, rp.data(), cols.data(), cls.data());
+}
+
+extern "C" int ldpc_code_info(const ldpc_code* c, int* info)
+{
+    if (!c || !info) return fail(LDPC_ERR_ARG, "ldpc_code_info: null pointer");
+    info[0] = c->n;
+    info[1] = c->m;
+    info[2] = c->e;
+    info[3] = c->dmax;
+    info[4] = (int)c->levels.size();
+    info[5] = c->widest;
+    info[6] = c->n - c->m;
+    info[7] = 0;
+    return LDPC_OK;
+}
+
+extern "C" void ldpc_code_destroy(ldpc_code* c) { delete c; }
+
+// ------------------------------------------------------------------------
+// kernels table
+// ------------------------------------------------------------------------
+
+namespace ldpc {
+const void* kernel_table_simd4(int kind, int variant);
+const void* kernel_table_f16x2(int kind, int variant);
+const void* kernel_table_i8(int kind, int variant);
+}
+
+// variant: 0/1 = every row has degree 6/7 (fully unrolled), 2/3/4 = rows of
+// degree <= 8/16/32 (unused edge slots predicated off)
+static int degree_variant(const ldpc_code* c)
+{
+    bool uniform = true;
+    for (int r = 1; r < c->m && uniform; r++)
+        uniform = (c->row_ptr[r + 1] - c->row_ptr[r]) == (c->row_ptr[1] - c->row_ptr[0]);
+    if (uniform && c->dmax == 6) return 0;
+    if (uniform && c->dmax == 7) return 1;
+    if (c->dmax <= 8) return 2;
+    if (c->dmax <= 16) return 3;
+    return 4;
+}
+
+static const void* kernel_for(int pack, int kind, int variant)
+{
+    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // xMS = OMS arithmetic without the first-iteration quirk
+    switch (pack) {
+    case LDPC_PACK_SIMD4: return kernel_table_simd4(k, variant);
+    case LDPC_PACK_F16X2: return kernel_table_f16x2(k, variant);
+    case LDPC_PACK_I8: return kernel_table_i8(k, variant);
+    }
+    return nullptr;
+}
+
+static size_t smem_bytes(int pack, int npad, int dmax, int m)
+{
+    size_t esz = pack == LDPC_PACK_I8 ? 1 : 4;
+    size_t wpc = pack == LDPC_PACK_SIMD4 ? 1 : (pack == LDPC_PACK_F16X2 ? 2 : 4);
+    return wpc * esz * ((size_t)npad + (size_t)dmax * m);
+}
+
+// ------------------------------------------------------------------------
+// decoders
+// ------------------------------------------------------------------------
+
+static void decoder_free(ldpc_decoder* d)
+{
+    if (!d) return;
+    cudaFree(d->d_cols);
+    cudaFree(d->d_rowdeg);
+    cudaFree(d->d_rowcls);
+    cudaFree(d->d_levels);
+    cudaFree(d->d_edge_orig);
+    cudaFree(d->d_in);
+    cudaFree(d->d_out);
+    if (d->s_comp) cudaStreamDestroy(d->s_comp);
+    if (d->s_h2d) cudaStreamDestroy(d->s_h2d);
+    if (d->s_d2h) cudaStreamDestroy(d->s_d2h);
+    delete d;
+}
+
+static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
+{
+    const int m = c->m, dmax = c->dmax;
+    std::vector<uint16_t> cols((size_t)dmax * m, 0);
+    std::vector<int32_t> eorig((size_t)dmax * m, -1);
+    std::vector<uint8_t> deg(m), cls(m);
+    for (int rp = 0; rp < m; rp++) {
+        int r = c->order[rp], b = c->row_ptr[r], dg = c->row_ptr[r + 1] - b;
+        deg[rp] = (uint8_t)dg;
+        cls[rp] = c->row_class[r];
+        for (int j = 0; j < dg; j++) {
+            cols[(size_t)j * m + rp] = (uint16_t)c->cols[b + j];
+            eorig[(size_t)j * m + rp] = b + j;
+        }
+    }
+    CUDA_TRY(cudaMalloc(&d->d_cols, cols.size() * sizeof(uint16_t)));
+    CUDA_TRY(cudaMalloc(&d->d_edge_orig, eorig.size() * sizeof(int32_t)));
+    CUDA_TRY(cudaMalloc(&d->d_rowdeg, m));
+    CUDA_TRY(cudaMalloc(&d->d_rowcls, m));
+    CUDA_TRY(cudaMalloc(&d->d_levels, c->levels.size() * sizeof(int2)));
+    CUDA_TRY(cudaMemcpy(d->d_cols, cols.data(), cols.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d->d_edge_orig, eorig.data(), eorig.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d->d_rowdeg, deg.data(), m, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d->d_rowcls, cls.data(), m, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d->d_levels, c->levels.data(), c->levels.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    Plan& P = d->plan;
+    P.n = c->n;
+    P.npad = (c->n + 15) / 16 * 16;
+    P.m = m;
+    P.dmax = dmax;
+    P.nlevels = (int)c->levels.size();
+    P.cols = d->d_cols;
+    P.rowdeg = d->d_rowdeg;
+    P.rowcls = d->d_rowcls;
+    P.levels = d->d_levels;
+    P.edge_orig = d->d_edge_orig;
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int kind, size_t nb_frames, int pack,
+                                   int flags)
+{
+    if (!out || !c) return fail(LDPC_ERR_ARG, "ldpc_decoder_create: null pointer");
+    if (kind < LDPC_MS || kind > LDPC_XMS) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
+    if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
+    if (flags != 0) return fail(LDPC_ERR_ARG, "flags must be 0");
+    if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
+    if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
+    if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
+    int npad = (c->n + 15) / 16 * 16;
+    size_t smem = smem_bytes(pack, npad, c->dmax, c->m);
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    int smem_max = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)smem_max)
+        return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
+                    smem, smem_max);
+    ldpc_decoder* d = new ldpc_decoder();
+    d->kind = kind;
+    d->pack = pack;
+    d->device = dev;
+    d->nb_words = nb_frames;
+    d->n = c->n;
+    d->m = c->m;
+    d->e = c->e;
+    int rc = decoder_setup(d, c);
+    if (rc) {
+        decoder_free(d);
+        return rc;
+    }
+    d->kfn = kernel_for(pack, kind, degree_variant(c));
+    d->smem = (int)smem;
+    d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    cudaError_t e1 = cudaFuncSetAttribute(d->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
+    cudaFuncAttributes fa;
+    cudaError_t e2 = cudaFuncGetAttributes(&fa, d->kfn);
+    cudaError_t e3 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->ctas_per_sm, d->kfn, d->threads, d->smem);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+        decoder_free(d);
+        return fail(LDPC_ERR_CUDA, "kernel setup: %s", cudaGetErrorString(e));
+    }
+    d->regs = fa.numRegs;
+    if (d->ctas_per_sm < 1) {
+        decoder_free(d);
+        return fail(LDPC_ERR_UNSUPPORTED, "kernel cannot be resident (smem %d B, %d threads)", d->smem, d->threads);
+    }
+    cudaError_t es = cudaStreamCreateWithFlags(&d->s_comp, cudaStreamNonBlocking);
+    if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&d->s_h2d, cudaStreamNonBlocking);
+    if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&d->s_d2h, cudaStreamNonBlocking);
+    if (es != cudaSuccess) {
+        decoder_free(d);
+        return fail(LDPC_ERR_CUDA, "stream creation: %s", cudaGetErrorString(es));
+    }
+    *out = d;
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decoder_info(const ldpc_decoder* d, int* info)
+{
+    if (!d || !info) return fail(LDPC_ERR_ARG, "ldpc_decoder_info: null pointer");
+    info[0] = d->kind;
+    info[1] = d->pack;
+    info[2] = (int)d->nb_words;
+    info[3] = d->threads;
+    info[4] = d->smem;
+    info[5] = d->ctas_per_sm;
+    info[6] = d->regs;
+    info[7] = 4;
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decoder_destroy(ldpc_decoder* d)
+{
+    if (!d) return LDPC_OK;
+    cudaError_t e = cudaDeviceSynchronize();
+    decoder_free(d);
+    if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "ldpc_decoder_destroy: %s", cudaGetErrorString(e));
+    return LDPC_OK;
+}
+
+static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed, long long word0, long long words,
+                  long long total_words, int iters, int32_t* iters_out, int8_t* app_out, int8_t* msg_out,
+                  cudaStream_t st)
+{
+    Job J;
+    J.llr = llr;
+    J.out = out;
+    J.out_packed = out_packed;
+    J.interleaved = d->kind == LDPC_XMS;
+    J.total_words = total_words;
+    J.word0 = word0;
+    J.iters = iters;
+    J.quirk = d->kind == LDPC_OMS;
+    J.iters_out = iters_out;
+    J.app_out = app_out;
+    J.msg_out = msg_out;
+    void* args[] = {(void*)&d->plan, (void*)&J};
+    CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)words), dim3(d->threads), args, d->smem, st));
+    return LDPC_OK;
+}
+
+static int check_decode_args(ldpc_decoder* d, const void* in, const void* out, size_t n_words, int iters)
+{
+    if (!d || !in || !out) return fail(LDPC_ERR_ARG, "decode: null pointer");
+    if (iters < 1) return fail(LDPC_ERR_ARG, "decode: iterations must be >= 1 (got %d)", iters);
+    if (n_words < 1 || n_words > d->nb_words)
+        return fail(LDPC_ERR_SHAPE, "decode: %zu words requested, decoder holds %zu", n_words, d->nb_words);
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decode_device(ldpc_decoder* d, const int8_t* d_llr, void* d_out, size_t n_words, int iters,
+                                  int out_format, int32_t* d_iters_out, void* stream)
+{
+    int rc = check_decode_args(d, d_llr, d_out, n_words, iters);
+    if (rc) return rc;
+    if (out_format != LDPC_OUT_BYTES && out_format != LDPC_OUT_PACKED)
+        return fail(LDPC_ERR_ARG, "decode: unknown out_format %d", out_format);
+    CUDA_TRY(cudaSetDevice(d->device));
+    return launch(d, d_llr, d_out, out_format == LDPC_OUT_PACKED, 0, (long long)n_words, (long long)n_words, iters,
+                  d_iters_out, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, uint8_t* d_hard, size_t n_words,
+                                        int iters, int32_t* d_iters_out, int8_t* d_app, int8_t* d_msg, void* stream)
+{
+    int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(d->device));
+    return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
+                  (cudaStream_t)stream);
+}
+
+extern "C" int ldpc_decode_host(ldpc_decoder* d, const int8_t* llr, uint8_t* hard, int iters)
+{
+    if (!d) return fail(LDPC_ERR_ARG, "decode: null decoder");
+    int rc = check_decode_args(d, llr, hard, d->nb_words, iters);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(d->device));
+    const size_t W = d->nb_words, fb = 4 * (size_t)d->n;  // bytes per word-group of frames
+    if (!d->d_in) {
+        CUDA_TRY(cudaMalloc(&d->d_in, W * fb));
+        CUDA_TRY(cudaMalloc(&d->d_out, W * fb));
+    }
+    // chunks of words: copy-in of chunk i+1 and copy-out of chunk i-1 overlap decoding of chunk i
+    size_t chunks = (d->kind == LDPC_XMS) ? 1 : std::min<size_t>(8, std::max<size_t>(1, W / 256));
+    size_t per = (W + chunks - 1) / chunks;
+    std::vector<cudaEvent_t> ev_in, ev_dec;
+    for (size_t c0 = 0, i = 0; c0 < W; c0 += per, i++) {
+        size_t words = std::min(per, W - c0);
+        cudaEvent_t a, b;
+        CUDA_TRY(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+        ev_in.push_back(a);
+        ev_dec.push_back(b);
+        size_t off = c0 * fb, bytes = words * fb;
+        if (d->kind == LDPC_XMS) {
+            off = 0;
+            bytes = W * fb;
+        }
+        CUDA_TRY(cudaMemcpyAsync(d->d_in + off, llr + off, bytes, cudaMemcpyHostToDevice, d->s_h2d));
+        CUDA_TRY(cudaEventRecord(a, d->s_h2d));
+        CUDA_TRY(cudaStreamWaitEvent(d->s_comp, a, 0));
+        const int8_t* src = (d->kind == LDPC_XMS) ? d->d_in : d->d_in + c0 * fb;
+        rc = launch(d, src, d->d_out + c0 * fb, 0, (long long)c0, (long long)words, (long long)W, iters, nullptr,
+                    nullptr, nullptr, d->s_comp);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(b, d->s_comp));
+        CUDA_TRY(cudaStreamWaitEvent(d->s_d2h, b, 0));
+        CUDA_TRY(cudaMemcpyAsync(hard + c0 * fb, d->d_out + c0 * fb, words * fb, cudaMemcpyDeviceToHost, d->s_d2h));
+    }
+    cudaError_t e = cudaStreamSynchronize(d->s_d2h);
+    for (auto ev : ev_in) cudaEventDestroy(ev);
+    for (auto ev : ev_dec) cudaEventDestroy(ev);
+    if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "decode_host: %s", cudaGetErrorString(e));
+    return LDPC_OK;
+}
+
+// ------------------------------------------------------------------------
+// misc
+// ------------------------------------------------------------------------
+
+extern "C" const char* ldpc_last_error_string(void) { return g_err.c_str(); }
+extern "C" int ldpc_version(void) { return 1; }
+
+__global__ void simd_selftest_kernel(int op, const uint32_t* a, const uint32_t* b, uint32_t* o, size_t n)
+{
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t x = a[i], y = b[i], r = 0;
+    switch (op) {
+    case 0: r = __vsubss4(x, y); break;
+    case 1: r = __vaddss4(x, y); break;
+    case 2: r = __vabs4(x); break;
+    case 3: r = __vminu4(x, y); break;
+    case 4: r = __vmaxu4(x, y); break;
+    case 5: r = __vsubus4(x, y); break;
+    case 6: r = __vcmpgts4(x, y); break;
+    case 7: r = __vcmpeq4(x, y); break;
+    case 8: r = __vneg4(x); break;
+    case 9: r = __vsetgts4(x, y); break;
+    }
+    o[i] = r;
+}
+
+extern "C" int ldpc_simd_selftest(int op, const uint32_t* a, const uint32_t* b, uint32_t* o, size_t n, void* stream)
+{
+    if (!a || !b || !o || op < 0 || op > 9) return fail(LDPC_ERR_ARG, "ldpc_simd_selftest: bad argument");
+    if (n == 0) return LDPC_OK;
+    simd_selftest_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(op, a, b, o, n);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+// ------------------------------------------------------------------------
+// INT32 issue-rate probe (roofline denominator of the integer decode kernels)
+// ------------------------------------------------------------------------
+
+// 8 independent chains per thread; MIX selects LOP3-only (0), IADD3-only (1) or alternating (2).
+template <int MIX>
+__global__ void __launch_bounds__(256) int_peak_kernel(uint32_t* out, uint32_t seed, int iters)
+{
+    uint32_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = seed * (i + 3) + threadIdx.x;
+    const uint32_t k = seed ^ 0x9e3779b9u;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            if (MIX == 0 || (MIX == 2 && (i & 1)))
+                v[i] = (v[i] ^ k) & (v[i] | 0x0f0f0f0fu);  // one LOP3
+            else
+                v[i] = v[i] + k + 0x1234567u;               // one IADD3
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) x ^= v[i];
+    if (x == 0x12345678u) out[blockIdx.x] = x;  // keeps the chains live
+}
+
+extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
+{
+    if (!lane_ops_per_s) return fail(LDPC_ERR_ARG, "ldpc_probe_int_peak: null pointer");
+    int dev = 0, sms = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint32_t* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(uint32_t) * sms * 8));
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    double best = 0;
+    for (int mix = 0; mix < 3; mix++) {
+        for (int rep = 0; rep < 3; rep++) {
+            CUDA_TRY(cudaEventRecord(a, st));
+            if (mix == 0) int_peak_kernel<0><<<blocks, threads, 0, st>>>(d, 7u + rep, iters);
+            if (mix == 1) int_peak_kernel<1><<<blocks, threads, 0, st>>>(d, 7u + rep, iters);
+            if (mix == 2) int_peak_kernel<2><<<blocks, threads, 0, st>>>(d, 7u + rep, iters);
+            CUDA_TRY(cudaEventRecord(b, st));
+            CUDA_TRY(cudaEventSynchronize(b));
+            float ms = 0;
+            CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+            double ops = (double)blocks * threads * iters * 8;
+            if (ms > 0 && rep > 0) best = std::max(best, ops / (ms * 1e-3));
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    *lane_ops_per_s = best;
+    return LDPC_OK;
+}

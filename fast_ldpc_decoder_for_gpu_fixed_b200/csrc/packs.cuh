@@ -1,0 +1,266 @@
+// Frame packings of the decoder state and their check-node arithmetic.
+//
+// A "pack" decides how the per-frame int8 values of the reference decoder
+// (APP in [-128,127], c->v messages) are laid out in shared memory and
+// registers, and implements one check-row update over them.  All three give
+// bit-identical results to the reference's byte lanes
+// (decoder_oms/cuda/CUDA_OMS_SIMD.cu:64-87 and :164-187; per-byte semantics
+// of the SIMD helper header decoder_oms/cuda/simd_functions.h:89-130):
+//
+//   PackSIMD4  4 frames per 32-bit word, one byte per frame, CUDA's per-byte
+//              SIMD intrinsics (__vsubss4, __vabs4, __vminu4, ...).  Same
+//              packing as the reference; word g holds frames 4g..4g+3.
+//   PackF16x2  2 frames per 32-bit word as two fp16 lanes holding the integer
+//              values exactly.  Every value is stored NEGATED (u = -x): then
+//              the reference's "bit 1" test x > 0 is exactly the sign bit of
+//              u (x = 0 gives u = +0, sign 0), so sign products are XORs of
+//              sign bits and conditional negations are sign-bit XORs; the
+//              saturations become clamps to [-127, 128].  -0 can appear only
+//              in messages, where x - (-0) = x keeps it harmless.
+//   PackI8     1 frame per thread lane: int8 in shared memory, int32 math.
+//              APP kept as x, messages kept negated (u = -m, |u| <= 127).
+//
+// Check magnitudes (c1 for the minimum edge, c2 for the others):
+//   MS   min(m, 31)                          decoder_ms/cuda/CUDA_MS_SIMD.cu:73-74
+//   OMS  min(max(m-1, 0), 31); no 31-clip on first-iteration rows of the second
+//        degree group                        decoder_oms/cuda/CUDA_OMS_SIMD.cu:73-74,115-116
+//   NMS  floor(0.75 m) for both              decoder_nms/cuda/CUDA_NMS_SIMD.cu:73-85
+//   2NMS floor(0.875 min2), floor(0.75 min1) decoder_2nms/cuda/CUDA_2NMS_SIMD.cu:76-83
+// (the reference's float multiply followed by the char conversion truncates a
+// non-negative exact product, i.e. floors it).
+#pragma once
+#include <cstdint>
+#include <cuda_fp16.h>
+
+namespace ldpc {
+
+enum { KIND_MS = 0, KIND_OMS = 1, KIND_NMS = 2, KIND_2NMS = 3, KIND_XMS = 4 };
+
+// ------------------------------------------------------------------------
+// 4 frames per word, per-byte saturating SIMD
+// ------------------------------------------------------------------------
+struct PackSIMD4 {
+    using S = uint32_t;  // shared-memory element
+    using R = uint32_t;  // register value
+    static constexpr int WPC = 1;  // storage words per 4-frame group
+    static constexpr int ID = 0;
+
+    __device__ __forceinline__ static R ld_app(const S* p) { return *p; }
+    __device__ __forceinline__ static R ld_msg(const S* p) { return *p; }
+    __device__ __forceinline__ static void st_app(S* p, R v) { *p = v; }
+    __device__ __forceinline__ static void st_msg(S* p, R v) { *p = v; }
+
+    template <int KIND>
+    __device__ __forceinline__ static void mags(R mn1, R mn2, bool noclip, R& c1, R& c2)
+    {
+        if (KIND == KIND_MS) {
+            c1 = __vminu4(mn2, 0x1f1f1f1fu);
+            c2 = __vminu4(mn1, 0x1f1f1f1fu);
+        } else if (KIND == KIND_OMS) {
+            c1 = __vsubus4(mn2, 0x01010101u);
+            c2 = __vsubus4(mn1, 0x01010101u);
+            if (!noclip) {
+                c1 = __vminu4(c1, 0x1f1f1f1fu);
+                c2 = __vminu4(c2, 0x1f1f1f1fu);
+            }
+        } else {
+            // floor(3m/4) = m - ceil(m/4); bytes <= 127 so no carry crosses a byte
+            c2 = mn1 - (((mn1 + 0x03030303u) >> 2) & 0x3f3f3f3fu);
+            if (KIND == KIND_NMS)
+                c1 = mn2 - (((mn2 + 0x03030303u) >> 2) & 0x3f3f3f3fu);
+            else  // floor(7m/8) = m - ceil(m/8)
+                c1 = mn2 - (((mn2 + 0x07070707u) >> 3) & 0x1f1f1f1fu);
+        }
+    }
+
+    // x[j]: APP in / APP out; m[j]: message in / out (all 4 byte lanes)
+    template <int KIND, int DT, bool EXACT>
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    {
+        R mn1 = 0x7f7f7f7fu, mn2 = 0x7f7f7f7fu, s = 0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                R t = __vsubss4(x[j], m[j]);
+                x[j] = t;
+                R a = __vabs4(t);
+                mn2 = __vminu4(mn2, __vmaxu4(a, mn1));
+                mn1 = __vminu4(mn1, a);
+                s ^= __vcmpgts4(t, 0u);
+            }
+        }
+        R c1, c2;
+        mags<KIND>(mn1, mn2, noclip, c1, c2);
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                R t = x[j];
+                R eq = __vcmpeq4(__vabs4(t), mn1);
+                R re = (eq & c1) | (~eq & c2);
+                R sg = s ^ __vcmpgts4(t, 0u);
+                R out = (re & sg) | (__vneg4(re) & ~sg);
+                m[j] = out;
+                x[j] = __vaddss4(t, out);
+            }
+        }
+        ov |= s;
+    }
+};
+
+// ------------------------------------------------------------------------
+// 2 frames per word, integer-valued fp16 lanes, negated values
+// ------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+__device__ __forceinline__ __half2 u2h(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+
+struct PackF16x2 {
+    using S = uint32_t;
+    using R = uint32_t;
+    static constexpr int WPC = 2;
+    static constexpr int ID = 1;
+
+    __device__ __forceinline__ static R ld_app(const S* p) { return *p; }
+    __device__ __forceinline__ static R ld_msg(const S* p) { return *p; }
+    __device__ __forceinline__ static void st_app(S* p, R v) { *p = v; }
+    __device__ __forceinline__ static void st_msg(S* p, R v) { *p = v; }
+
+    // floor(m * k) for integer m in [0,127] and k = 3/4 or 7/8: the product
+    // minus (1/2 - 1/2^(bits+1)) is exact in fp16 and lies within 1/2 of the
+    // floor (never on a tie), so adding 1024 rounds it to that integer.
+    __device__ __forceinline__ static __half2 floor_scale(__half2 mn, float k, float bias)
+    {
+        const __half2 big = __float2half2_rn(1024.f);
+        __half2 y = __hfma2_relu(mn, __float2half2_rn(k), __float2half2_rn(-bias));
+        return __hsub2(__hadd2(y, big), big);
+    }
+
+    template <int KIND>
+    __device__ __forceinline__ static void mags(__half2 mn1, __half2 mn2, bool noclip, __half2& c1, __half2& c2)
+    {
+        const __half2 c31 = __float2half2_rn(31.f);
+        if (KIND == KIND_MS) {
+            c1 = __hmin2(mn2, c31);
+            c2 = __hmin2(mn1, c31);
+        } else if (KIND == KIND_OMS) {
+            const __half2 one = __float2half2_rn(1.f), mone = __float2half2_rn(-1.f);
+            c1 = __hfma2_relu(mn2, one, mone);
+            c2 = __hfma2_relu(mn1, one, mone);
+            if (!noclip) {
+                c1 = __hmin2(c1, c31);
+                c2 = __hmin2(c2, c31);
+            }
+        } else {
+            c2 = floor_scale(mn1, 0.75f, 0.375f);
+            if (KIND == KIND_NMS)
+                c1 = floor_scale(mn2, 0.75f, 0.375f);
+            else
+                c1 = floor_scale(mn2, 0.875f, 0.4375f);
+        }
+    }
+
+    template <int KIND, int DT, bool EXACT>
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    {
+        const __half2 lo = __float2half2_rn(-127.f), hi = __float2half2_rn(128.f);
+        __half2 mn1 = __float2half2_rn(127.f), mn2 = mn1;
+        uint32_t s = 0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                __half2 t = __hmin2(__hmax2(__hsub2(u2h(x[j]), u2h(m[j])), lo), hi);
+                x[j] = h2u(t);
+                __half2 a = __habs2(t);
+                mn2 = __hmin2(mn2, __hmax2(a, mn1));
+                mn1 = __hmin2(mn1, a);
+                s ^= x[j];
+            }
+        }
+        __half2 c1, c2;
+        mags<KIND>(mn1, mn2, noclip, c1, c2);
+        s &= 0x80008000u;
+        const uint32_t c1s = h2u(c1) | s, c2s = h2u(c2) | s;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                __half2 t = u2h(x[j]);
+                uint32_t eq = __heq2_mask(__habs2(t), mn1);
+                uint32_t re = (eq & c1s) | (~eq & c2s);
+                uint32_t out = re ^ (x[j] & 0x80008000u);
+                m[j] = out;
+                x[j] = h2u(__hmin2(__hmax2(__hadd2(t, u2h(out)), lo), hi));
+            }
+        }
+        ov |= s;
+    }
+};
+
+// ------------------------------------------------------------------------
+// 1 frame per lane, int8 storage, int32 arithmetic
+// ------------------------------------------------------------------------
+struct PackI8 {
+    using S = int8_t;
+    using R = int;
+    static constexpr int WPC = 4;
+    static constexpr int ID = 2;
+
+    __device__ __forceinline__ static R ld_app(const S* p) { return *p; }
+    __device__ __forceinline__ static R ld_msg(const S* p) { return *p; }
+    __device__ __forceinline__ static void st_app(S* p, R v) { *p = (S)v; }
+    __device__ __forceinline__ static void st_msg(S* p, R v) { *p = (S)v; }
+
+    template <int KIND>
+    __device__ __forceinline__ static void mags(int mn1, int mn2, bool noclip, int& c1, int& c2)
+    {
+        if (KIND == KIND_MS) {
+            c1 = min(mn2, 31);
+            c2 = min(mn1, 31);
+        } else if (KIND == KIND_OMS) {
+            c1 = max(mn2 - 1, 0);
+            c2 = max(mn1 - 1, 0);
+            if (!noclip) {
+                c1 = min(c1, 31);
+                c2 = min(c2, 31);
+            }
+        } else {
+            c2 = (3 * mn1) >> 2;
+            c1 = (KIND == KIND_NMS) ? (3 * mn2) >> 2 : (7 * mn2) >> 3;
+        }
+    }
+
+    // x[j]: APP (as x) in/out; m[j]: message stored negated (u = -msg) in/out
+    template <int KIND, int DT, bool EXACT>
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    {
+        int mn1 = 127, mn2 = 127, s = 0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                int ut = min(max(-x[j] - m[j], -127), 128);  // u_t = -(sat8(app - msg))
+                x[j] = ut;
+                int a = abs(ut);
+                mn2 = min(mn2, max(a, mn1));
+                mn1 = min(mn1, a);
+                s ^= ut;
+            }
+        }
+        int c1, c2;
+        mags<KIND>(mn1, mn2, noclip, c1, c2);
+        const int sm = s >> 31;  // all ones when the parity of "x > 0" edges is odd
+        c1 = (c1 ^ sm) - sm;
+        c2 = (c2 ^ sm) - sm;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                int ut = x[j];
+                int re = (abs(ut) == mn1) ? c1 : c2;
+                int tm = ut >> 31;
+                int um = (re ^ tm) - tm;  // negated message: sign flips with this edge's bit
+                m[j] = um;
+                x[j] = min(max(-(ut + um), -128), 127);
+            }
+        }
+        ov |= s & (int)0x80000000;
+    }
+};
+
+}  // namespace ldpc

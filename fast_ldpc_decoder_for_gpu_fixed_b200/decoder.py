@@ -1,0 +1,206 @@
+"""Decoder objects over the C ABI, and Python mirrors of the reference's plugin classes.
+
+The reference's decoder plugins (``src/decoder_template/CGPUDecoder.h:19-35``)
+are C++ classes built against one compile-time H matrix:
+
+    CGPUDecoder(size_t nb_frames, size_t n, size_t k, size_t m);
+    virtual void initialize() = 0;
+    virtual void decode(float var_nodes[_N], int Rprime_fix[_N], int nombre_iterations) = 0;
+
+with subclasses CGPU_Decoder_MS_SIMD, _OMS_SIMD, _NMS_SIMD, _2NMS_SIMD and
+CGPU_Decoder_MS_SIMD_v2 (``-xMS``), chosen in ``src/main.cpp:213-228``.
+``nb_frames`` counts 32-bit lanes (4 codewords each); ``decode`` takes the
+frame-major int8 LLRs of 4*nb_frames codewords (typed float* in the reference)
+and writes frame-major 0/1 bytes (typed int*).  The classes below keep those
+names, arguments and meanings; the H matrix is the module's selected code
+(``select_code``, default "4000x2000" like ``src/matrix/code.h:1``), and
+errors raise ``LdpcError`` instead of the reference's exit(0).
+The C++ equivalents of these classes are in ``cpp/CGPUDecoder.h``.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .codes import Code, load_table
+
+
+class NativeCode:
+    """An ldpc_code handle (H matrix + level schedule) built from a ``Code``."""
+
+    def __init__(self, code):
+        self.code = code
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ldpc_code_create(
+            ctypes.byref(h), code.n, code.m, code.row_ptr.ctypes.data, code.cols.ctypes.data,
+            code.row_class.ctypes.data))
+        self.handle = h
+
+    def info(self):
+        a = (ctypes.c_int * 8)()
+        _lib.check(_lib.lib().ldpc_code_info(self.handle, a))
+        keys = ("n", "checks", "edges", "dmax", "levels", "widest_level", "n_info")
+        return dict(zip(keys, list(a)))
+
+    def close(self):
+        if self.handle:
+            _lib.lib().ldpc_code_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(x):
+    """Raw address of a numpy array, a torch tensor, an int or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError("cannot take the address of %r" % type(x))
+
+
+class Decoder:
+    """One ldpc_decoder: ``kind`` in MS/OMS/NMS/2NMS/XMS, ``nb_frames`` 32-bit lanes
+    (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8."""
+
+    def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO"):
+        if isinstance(code, str):
+            code = load_table(code)
+        self.code = code if isinstance(code, Code) else code.code
+        self.native = code if isinstance(code, NativeCode) else NativeCode(self.code)
+        self.kind = kind.upper()
+        self.nb_frames = int(nb_frames)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ldpc_decoder_create(
+            ctypes.byref(h), self.native.handle, _lib.KINDS[self.kind], self.nb_frames,
+            _lib.PACKS[pack.upper()], 0))
+        self.handle = h
+
+    def info(self):
+        a = (ctypes.c_int * 8)()
+        _lib.check(_lib.lib().ldpc_decoder_info(self.handle, a))
+        keys = ("kind", "pack", "nb_frames", "threads", "smem", "ctas_per_sm", "regs", "frames_per_cta")
+        return dict(zip(keys, list(a)))
+
+    def decode_host(self, llr, hard, iters):
+        """Synchronous host-buffer decode of all 4*nb_frames codewords (numpy arrays)."""
+        n_bytes = 4 * self.nb_frames * self.code.n
+        if llr.nbytes < n_bytes or hard.nbytes < n_bytes:
+            raise ValueError("buffers must hold %d bytes" % n_bytes)
+        if not (llr.flags.c_contiguous and hard.flags.c_contiguous and hard.flags.writeable):
+            raise ValueError("buffers must be C-contiguous (and hard writeable)")
+        _lib.check(_lib.lib().ldpc_decode_host(self.handle, _ptr(llr), _ptr(hard), int(iters)))
+        return hard
+
+    def decode_device(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None):
+        """Asynchronous device-buffer decode of 4*n_words codewords on ``stream`` (a raw
+        cudaStream_t value, a torch stream or None for the legacy default stream)."""
+        st = getattr(stream, "cuda_stream", stream)
+        _lib.check(_lib.lib().ldpc_decode_device(self.handle, _ptr(d_llr), _ptr(d_out), int(n_words), int(iters),
+                                                 int(out_format), _ptr(d_iters), st))
+
+    def decode_device_state(self, d_llr, d_hard, n_words, iters, d_iters=None, d_app=None, d_msg=None,
+                            stream=None):
+        st = getattr(stream, "cuda_stream", stream)
+        _lib.check(_lib.lib().ldpc_decode_device_state(self.handle, _ptr(d_llr), _ptr(d_hard), int(n_words),
+                                                       int(iters), _ptr(d_iters), _ptr(d_app), _ptr(d_msg), st))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.lib().ldpc_decoder_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# reference-compatible plugin classes
+# ---------------------------------------------------------------------------
+
+_selected = {"code": None, "name": "4000x2000"}
+
+
+def select_code(code):
+    """Selects the H matrix the plugin classes use (the reference's src/matrix/code.h)."""
+    if isinstance(code, str):
+        _selected["name"], _selected["code"] = code, None
+    else:
+        _selected["name"], _selected["code"] = code.name, code
+
+
+def selected_code():
+    if _selected["code"] is None:
+        _selected["code"] = load_table(_selected["name"])
+    return _selected["code"]
+
+
+class CGPUDecoder:
+    """Mirror of decoder_template/CGPUDecoder.h:19-35 (abstract; use a subclass)."""
+    KIND = None
+
+    def __init__(self, nb_frames, n, k, m, pack="AUTO"):
+        code = selected_code()
+        if (n, k, m) != (code.n, code.m, code.e):
+            raise ValueError("decoder built for (N,K,M)=(%d,%d,%d) but the selected code is (%d,%d,%d)"
+                             % (n, k, m, code.n, code.m, code.e))
+        if self.KIND is None:
+            raise TypeError("CGPUDecoder is abstract")
+        self.nb_frames = int(nb_frames)
+        self.sz_nodes = n * self.nb_frames
+        self.sz_checks = k * self.nb_frames
+        self.sz_msgs = m * self.nb_frames
+        self._dec = Decoder(code, self.KIND, self.nb_frames, pack)
+
+    def initialize(self):
+        pass
+
+    def decode(self, var_nodes, Rprime_fix, nombre_iterations):
+        """var_nodes: 4*nb_frames*N int8 LLRs (any dtype, read as bytes);
+        Rprime_fix: writable buffer of the same byte size receiving 0/1 bytes."""
+        llr = np.ascontiguousarray(var_nodes).view(np.int8).reshape(-1)
+        out = Rprime_fix.view(np.uint8).reshape(-1)
+        self._dec.decode_host(llr, out, nombre_iterations)
+
+    def close(self):
+        self._dec.close()
+
+
+class CGPU_Decoder_MS_SIMD(CGPUDecoder):
+    """-MS / -fMS (decoder_ms/CGPU_Decoder_MS_SIMD.cu)."""
+    KIND = "MS"
+
+
+class CGPU_Decoder_OMS_SIMD(CGPUDecoder):
+    """-OMS (decoder_oms/CGPU_Decoder_OMS_SIMD.cu)."""
+    KIND = "OMS"
+
+
+class CGPU_Decoder_NMS_SIMD(CGPUDecoder):
+    """-NMS (decoder_nms/CGPU_Decoder_NMS_SIMD.cu)."""
+    KIND = "NMS"
+
+
+class CGPU_Decoder_2NMS_SIMD(CGPUDecoder):
+    """-2NMS (decoder_2nms/CGPU_Decoder_2NMS_SIMD.cu)."""
+    KIND = "2NMS"
+
+
+class CGPU_Decoder_MS_SIMD_v2(CGPUDecoder):
+    """-xMS (decoder_oms_v2/CGPU_Decoder_MS_SIMD_v2.cu): input already word-interleaved."""
+    KIND = "XMS"
+
+
+PLUGINS = {"fMS": CGPU_Decoder_MS_SIMD, "MS": CGPU_Decoder_MS_SIMD, "OMS": CGPU_Decoder_OMS_SIMD,
+           "NMS": CGPU_Decoder_NMS_SIMD, "2NMS": CGPU_Decoder_2NMS_SIMD, "xMS": CGPU_Decoder_MS_SIMD_v2}

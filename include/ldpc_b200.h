@@ -1,0 +1,152 @@
+/*
+ * ldpc_b200.h - C ABI of the B200 (sm_100a) fixed-point LDPC decoding engine.
+ *
+ * Plain C types only (pointers, sizes, ints); no CUDA or torch types appear
+ * in the signatures, so cgo / JNI / ctypes / C++ callers bind it directly.
+ * Every entry point returns 0 on success or a negative LDPC_ERR_* code and
+ * never exits the process; ldpc_last_error_string() describes the last
+ * failure of the calling thread.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - the compile-time H matrix: src/matrix/code.h:1 (#define CODE),
+ *     src/matrix/<code>/constantes_gpu.h:6-16 (_N, _K, _M, NB_DEGRES, DEG_1,
+ *     DEG_2, DEG_1_COMPUTATIONS, DEG_2_COMPUTATIONS) and
+ *     src/matrix/<code>/constantes_decoder.h:3 (PosNoeudsVariable[_M])
+ *     -> ldpc_code_create_from_table / ldpc_code_create / ldpc_code_load;
+ *   - the plugin constructors CGPUDecoder::CGPUDecoder(nb_frames, n, k, m)
+ *     (src/decoder_template/CGPUDecoder.cpp:14-38) and
+ *     CGPU_Decoder_{MS,OMS,NMS,2NMS}_SIMD / CGPU_Decoder_MS_SIMD_v2
+ *     (src/decoder_oms/CGPU_Decoder_OMS_SIMD.cu:20-90 and the same lines of the
+ *     MS, NMS, 2NMS and oms_v2 plugins, selected in src/main.cpp:213-228)
+ *     -> ldpc_decoder_create;
+ *   - CGPU_Decoder_*::decode(float*, int*, int)
+ *     (src/decoder_oms/CGPU_Decoder_OMS_SIMD.cu:97-147 and siblings)
+ *     -> ldpc_decode_host;
+ *   - the destructor (src/decoder_template/CGPUDecoder.cpp:41-54)
+ *     -> ldpc_decoder_destroy;
+ *   - ERROR_CHECK's print-then-exit(0) (src/custom_api/custom_cuda.cu:5-17)
+ *     -> status codes + ldpc_last_error_string.
+ */
+#ifndef LDPC_B200_H
+#define LDPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LDPC_OK 0
+#define LDPC_ERR_ARG (-1)         /* bad argument: null pointer, size, range   */
+#define LDPC_ERR_CUDA (-2)        /* a CUDA runtime call failed                */
+#define LDPC_ERR_UNSUPPORTED (-3) /* valid request this build cannot serve     */
+#define LDPC_ERR_NOMEM (-4)       /* device or host allocation failed          */
+#define LDPC_ERR_SHAPE (-5)       /* batch shape not accepted                  */
+
+/* decoder kinds = the reference's plugins (src/main.cpp:166-182 flags) */
+#define LDPC_MS 0   /* -MS / -fMS : CGPU_Decoder_MS_SIMD                          */
+#define LDPC_OMS 1  /* -OMS       : CGPU_Decoder_OMS_SIMD (offset 1)              */
+#define LDPC_NMS 2  /* -NMS       : CGPU_Decoder_NMS_SIMD (x0.75)                 */
+#define LDPC_2NMS 3 /* -2NMS      : CGPU_Decoder_2NMS_SIMD (x0.75/x0.875, early term.) */
+#define LDPC_XMS 4  /* -xMS       : CGPU_Decoder_MS_SIMD_v2 (input already word-interleaved) */
+
+/* frame packing of the on-chip decoder state */
+#define LDPC_PACK_AUTO (-1)
+#define LDPC_PACK_SIMD4 0 /* 4 frames per 32-bit word, saturating byte lanes      */
+#define LDPC_PACK_F16X2 1 /* 2 frames per 32-bit word, integer-valued fp16 lanes  */
+#define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
+
+/* output formats of ldpc_decode_device */
+#define LDPC_OUT_BYTES 0  /* frame-major 0/1 bytes [frames][n] (the reference's)  */
+#define LDPC_OUT_PACKED 1 /* frame-major bits, LSB first, ceil(n/8) bytes/frame   */
+
+typedef struct ldpc_code ldpc_code;
+typedef struct ldpc_decoder ldpc_decoder;
+
+/* ---- codes ------------------------------------------------------------- */
+
+/* H in the reference's own form: PosNoeudsVariable[m_edges] listing, check
+ * by check in layer order, the variable index of every edge; the first
+ * deg1_rows rows have degree deg1, the next deg2_rows rows degree deg2
+ * (nb_degres = 1 or 2).  Replaces src/matrix/<code>/constantes_gpu.h:6-16
+ * and constantes_decoder.h:3. */
+int ldpc_code_create_from_table(ldpc_code** out, int n, int k_checks, int m_edges,
+                                int nb_degres, int deg1, int deg1_rows, int deg2,
+                                int deg2_rows, const uint32_t* pos_noeuds_variable);
+
+/* H as CSR rows in layer order.  row_class (nullable) marks rows of the
+ * reference's second degree group (1) - the offset-min-sum kernel skips the
+ * 31-clip on them in the first iteration (decoder_oms/cuda/CUDA_OMS_SIMD.cu:115-116). */
+int ldpc_code_create(ldpc_code** out, int n_vars, int n_checks, const int32_t* row_ptr,
+                     const int32_t* cols, const uint8_t* row_class);
+
+/* Loads a .ldpc table file (format: fast_ldpc_decoder_for_gpu_fixed_b200/codes.py). */
+int ldpc_code_load(ldpc_code** out, const char* path);
+
+/* info[0..7] = n, checks, edges, max row degree, schedule levels per
+ * iteration, widest level, n_info (= n - checks), 0 */
+int ldpc_code_info(const ldpc_code* code, int* info);
+
+void ldpc_code_destroy(ldpc_code* code);
+
+/* ---- decoders ---------------------------------------------------------- */
+
+/* nb_frames counts 32-bit lanes like the reference's constructor argument:
+ * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
+ * Unlike the reference (decoder_oms/CGPU_Decoder_OMS_SIMD.cu:101-105), any
+ * nb_frames >= 1 is accepted.  The decoder owns its device buffers; the code
+ * may be destroyed after this call.  pack = LDPC_PACK_*; flags = 0. */
+int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* code, int kind, size_t nb_frames,
+                        int pack, int flags);
+
+/* Synchronous decode of 4*nb_frames codewords between host buffers, exactly
+ * like CGPU_Decoder_*::decode(float* var_nodes, int* Rprime_fix, int iters):
+ * llr = frame-major int8 [4*nb_frames][n] (LDPC_XMS: the word-interleaved
+ * reading word[v*nb_frames+g], byte k = frame 4g+k, as CGPU_Decoder_MS_SIMD_v2
+ * receives it), hard = frame-major 0/1 bytes [4*nb_frames][n].  Host buffers
+ * may be pageable or pinned; copies are pipelined with the decoding. */
+int ldpc_decode_host(ldpc_decoder* dec, const int8_t* llr, uint8_t* hard, int iters);
+
+/* Asynchronous decode between device buffers on `stream` (a cudaStream_t,
+ * 0 = legacy default stream).  n_words <= nb_frames words (4*n_words
+ * codewords) starting at llr; out_format = LDPC_OUT_*.  iters_out (nullable,
+ * device, n_words int32) receives the iterations executed per word. */
+int ldpc_decode_device(ldpc_decoder* dec, const int8_t* d_llr, void* d_out, size_t n_words,
+                       int iters, int out_format, int32_t* d_iters_out, void* stream);
+
+/* Like ldpc_decode_device, plus the final decoder state in the reference's
+ * device layouts (nullable): d_app = device_V, n*n_words 32-bit words
+ * word[v*n_words+g]; d_msg = d_MSG_C_2_V, edges*n_words words word[e*n_words+g]
+ * with e the edge index in table order.  For parity checks. */
+int ldpc_decode_device_state(ldpc_decoder* dec, const int8_t* d_llr, uint8_t* d_hard,
+                             size_t n_words, int iters, int32_t* d_iters_out,
+                             int8_t* d_app, int8_t* d_msg, void* stream);
+
+/* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
+ * per CTA, CTAs per SM, registers per thread, frames per CTA */
+int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
+
+int ldpc_decoder_destroy(ldpc_decoder* dec);
+
+/* ---- misc -------------------------------------------------------------- */
+
+const char* ldpc_last_error_string(void);
+int ldpc_version(void);
+
+/* Exhaustive check helper: applies the device's per-byte SIMD operation `op`
+ * (ids as oracle_byte_op: 0 sat-sub, 1 sat-add, 2 abs, 3 minu, 4 maxu,
+ * 5 subus, 6 gt-mask, 7 eq-mask, 8 neg, 9 gt-0/1) to n word pairs on the GPU. */
+int ldpc_simd_selftest(int op, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_out,
+                       size_t n, void* stream);
+
+/* Measures this GPU's INT32 issue rate (lane operations per second, best of
+ * independent LOP3 / IADD3 / mixed chains over all SMs): the denominator of
+ * the integer decoder's roofline.  No reference counterpart. */
+int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
