@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--ebn0", type=float, default=2.0)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-qc", action="store_true", help="use the level-scheduled kernel even for the QC code")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
     return ap.parse_args()
 
@@ -174,6 +175,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     code, enc, cws, idx, llr, sigma = make_workload(args.frames, args.ebn0, args.seed, rank)
+    code.no_qc = args.no_qc
     words = args.frames // 4
     dec = Decoder(code, args.kind, nb_frames=words, pack=args.pack)
     info = dec.info()
@@ -210,10 +212,8 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import replicas
+    ms_max = replicas.max_over_ranks(ms, device="cuda")
     ms_step = ms_max / args.steps
     info_bits = args.frames * enc.k
     value = world * info_bits * args.steps / (ms_max * 1e-3) / 1e9
@@ -245,7 +245,8 @@ def main():
                        "iterations": args.iters, "ebn0_db": args.ebn0, "fer": fer, "ber": ber,
                        "l2": "inputs (268 MB) larger than L2; no flush", "parallelism": "replicas" if world > 1 else "1gpu",
                        "threads_per_cta": info["threads"], "smem_per_cta": info["smem"],
-                       "ctas_per_sm": info["ctas_per_sm"], "regs": info["regs"]},
+                       "ctas_per_sm": info["ctas_per_sm"], "regs": info["regs"],
+                       "kernel": "qc_register_messages" if info["path"] == 1 else "level_scheduled"},
             "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
                          "frac": achieved / int_peak, "traffic": None,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,

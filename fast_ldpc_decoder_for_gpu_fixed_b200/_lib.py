@@ -24,6 +24,7 @@ SIGNATURES = {
     "ldpc_code_create_from_table": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I, _I, _I, _I, _I, _P]),
     "ldpc_code_create": (_I, [ctypes.POINTER(_P), _I, _I, _P, _P, _P]),
     "ldpc_code_load": (_I, [ctypes.POINTER(_P), ctypes.c_char_p]),
+    "ldpc_code_create_qc": (_I, [ctypes.POINTER(_P), _I, _I, _I, _P]),
     "ldpc_code_info": (_I, [_P, _P]),
     "ldpc_code_destroy": (None, [_P]),
     "ldpc_decoder_create": (_I, [ctypes.POINTER(_P), _P, _I, _SZ, _I, _I]),
@@ -36,6 +37,11 @@ SIGNATURES = {
     "ldpc_version": (_I, []),
     "ldpc_simd_selftest": (_I, [_I, _P, _P, _P, _SZ, _P]),
     "ldpc_probe_int_peak": (_I, [ctypes.POINTER(ctypes.c_double), _P]),
+    "ldpc_sigma": (ctypes.c_double, [ctypes.c_double, ctypes.c_double, _I]),
+    "ldpc_channel_awgn": (_I, [_P, _SZ, _I, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64, _P, _SZ, _P]),
+    "ldpc_philox": (_I, [_P, _SZ, ctypes.c_uint64, ctypes.c_uint64, _P]),
+    "ldpc_count_errors": (_I, [_P, _SZ, _I, _I, _P, _SZ, _P, _P]),
+    "ldpc_simulate": (_I, [_P, _SZ, _I, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64, _P, _SZ, _I, _P, _P, _P]),
 }
 
 

@@ -23,6 +23,7 @@
 // the CTA with __syncthreads_or.
 #pragma once
 #include <cstdint>
+#include "channel.cuh"
 #include "packs.cuh"
 
 namespace ldpc {
@@ -52,6 +53,16 @@ struct Job {
     int32_t* iters_out;   // [words] or null
     int8_t* app_out;      // state dumps (reference device layouts) or null
     int8_t* msg_out;
+    // fused simulation (llr == null): the channel generates the LLRs in the
+    // prologue and the epilogue counts errors instead of (or as well as) writing
+    // hard decisions
+    int gen;              // 1: generate LLRs (AWGN channel) instead of reading llr
+    float sigma;
+    unsigned long long seed, offset;
+    const uint8_t* cw;    // transmitted codewords (frame-major 0/1), null = all-zero
+    long long n_cw;
+    unsigned long long* counts;  // [3] frames, bit errors, frame errors (or null)
+    int n_vars;           // bits counted per frame
 };
 
 // ---- prologue / epilogue: frame-major global <-> packed shared memory ----
@@ -72,6 +83,47 @@ template <class F>
 __device__ __forceinline__ void read_group(const Plan& P, const Job& J, long long g, F put)
 {
     const int n = P.n;
+    if (J.gen) {
+        // frames 4g..4g+3 of the channel stream: sample s = frame * n + v
+        if ((n & 3) == 0) {
+            // 4 consecutive samples of a frame share one Philox call (counter s / 4)
+            for (int q = threadIdx.x; q < (n >> 2); q += blockDim.x) {
+                uint32_t a[4], w[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const unsigned long long f = 4ull * g + k;
+                    const unsigned long long s0 = f * (unsigned long long)n + 4 * q;
+                    float u[4], gs[4];
+                    uniforms4(s0 >> 2, J.seed, J.offset, u);
+                    box_muller4(u, gs);
+                    uint32_t x = 0;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        float mean = -1.0f;
+                        if (J.cw) mean = J.cw[(f % (unsigned long long)J.n_cw) * n + 4 * q + i] ? 1.0f : -1.0f;
+                        x |= (uint32_t)(uint8_t)quantise(mean + J.sigma * gs[i]) << (8 * i);
+                    }
+                    a[k] = x;
+                }
+                transpose4x4(a, w);
+#pragma unroll
+                for (int j = 0; j < 4; j++) put(4 * q + j, w[j]);
+            }
+        } else {
+            for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                uint32_t w = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const unsigned long long f = 4ull * g + k, s = f * (unsigned long long)n + v;
+                    float mean = -1.0f;
+                    if (J.cw) mean = J.cw[(f % (unsigned long long)J.n_cw) * n + v] ? 1.0f : -1.0f;
+                    w |= (uint32_t)(uint8_t)awgn_sample(s, J.seed, J.offset, J.sigma, mean) << (8 * k);
+                }
+                put(v, w);
+            }
+        }
+        return;
+    }
     if (J.interleaved) {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(J.llr);
         for (int v = threadIdx.x; v < n; v += blockDim.x) put(v, __ldg(src + (long long)v * J.total_words + g));
@@ -97,12 +149,54 @@ __device__ __forceinline__ void read_group(const Plan& P, const Job& J, long lon
     }
 }
 
+// Error counting of the group's 4 frames against the transmitted codewords
+// (ber_analyzer/CErrorAnalyzer.cpp:142-158): bits among the first n_vars whose
+// decision (x > 0) differs from the codeword bit.  Every thread of the CTA calls it.
+template <class F>
+__device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, long long g, F get)
+{
+    __shared__ int part[4][32];
+    int e[4] = {0, 0, 0, 0};
+    for (int v = threadIdx.x; v < J.n_vars; v += blockDim.x) {
+        uint32_t h = __vsetgts4(get(v), 0u);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            int bit = (h >> (8 * k)) & 1;
+            int ref = J.cw ? (J.cw[((4ull * g + k) % (unsigned long long)J.n_cw) * P.n + v] != 0) : 0;
+            e[k] += bit != ref;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) e[k] += __shfl_xor_sync(0xffffffffu, e[k], o);
+    }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; k++) part[k][threadIdx.x >> 5] = e[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long be = 0, fe = 0;
+        for (int k = 0; k < 4; k++) {
+            int t = 0;
+            for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) t += part[k][w];
+            be += t;
+            fe += t != 0;
+        }
+        atomicAdd(J.counts + 0, 4ull);
+        atomicAdd(J.counts + 1, be);
+        atomicAdd(J.counts + 2, fe);
+    }
+}
+
 // Writes hard decisions; get(v) returns the 4-frame byte word (values as x) of variable v.
 template <class F>
 __device__ __forceinline__ void write_group(const Plan& P, const Job& J, long long g, F get)
 {
     const int n = P.n;
     const long long lg = g - J.word0;
+    if (J.counts) count_group_errors(P, J, g, get);
+    if (!J.out) return;
     if (!J.out_packed) {
         uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + 4 * lg * n;
         if ((n & 3) == 0) {
@@ -149,17 +243,11 @@ template <> struct Access<PackSIMD4> {
     __device__ __forceinline__ static uint32_t get_msg(const uint32_t* msg, int stride, int idx) { return msg[idx]; }
 };
 
-__device__ __forceinline__ uint32_t neg_half_to_byte(uint16_t h)
-{
-    // integer-valued fp16 u in [-127,128] -> byte of x = -u (x in [-128,127])
-    int u = __half2int_rn(__ushort_as_half(h));
-    return (uint32_t)(uint8_t)(int8_t)(-u);
-}
-
 template <> struct Access<PackF16x2> {
+    // x bytes of frames k0, k0+1 -> biased negated pair b = 127 - x
     __device__ __forceinline__ static uint32_t pair(uint32_t w, int k0)
     {
-        int a = -(int)(int8_t)(w >> (8 * k0)), b = -(int)(int8_t)(w >> (8 * k0 + 8));
+        int a = 127 - (int)(int8_t)(w >> (8 * k0)), b = 127 - (int)(int8_t)(w >> (8 * k0 + 8));
         __half2 h = __halves2half2(__int2half_rn(a), __int2half_rn(b));
         return h2u(h);
     }
@@ -168,18 +256,20 @@ template <> struct Access<PackF16x2> {
         app[v] = pair(w, 0);
         app[npad + v] = pair(w, 2);
     }
-    __device__ __forceinline__ static uint32_t unpair(uint32_t lo, uint32_t hi)
+    __device__ __forceinline__ static uint32_t unbias(uint32_t lo, uint32_t hi)
     {
-        return neg_half_to_byte(lo & 0xffff) | (neg_half_to_byte(lo >> 16) << 8) |
-               (neg_half_to_byte(hi & 0xffff) << 16) | (neg_half_to_byte(hi >> 16) << 24);
+        auto x = [](uint16_t h) { return (uint32_t)(uint8_t)(int8_t)(127 - __half2int_rn(__ushort_as_half(h))); };
+        return x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
     }
     __device__ __forceinline__ static uint32_t get(const uint32_t* app, int npad, int v)
     {
-        return unpair(app[v], app[npad + v]);
+        return unbias(app[v], app[npad + v]);
     }
     __device__ __forceinline__ static uint32_t get_msg(const uint32_t* msg, int stride, int idx)
     {
-        return unpair(msg[idx], msg[stride + idx]);
+        auto x = [](uint16_t h) { return (uint32_t)(uint8_t)(int8_t)(-__half2int_rn(__ushort_as_half(h))); };
+        uint32_t lo = msg[idx], hi = msg[stride + idx];
+        return x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
     }
 };
 

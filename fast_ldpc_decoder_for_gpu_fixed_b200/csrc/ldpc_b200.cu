@@ -25,7 +25,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ldpc_b200.h"
-#include "decode_kernel.cuh"
+#include "qc_kernel.cuh"
 
 using namespace ldpc;
 
@@ -41,6 +41,8 @@ static int fail(int code, const char* fmt, ...)
     g_err = buf;
     return code;
 }
+
+int ldpc_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
 #define CUDA_TRY(x)                                                                          \
     do {                                                                                     \
@@ -60,6 +62,10 @@ struct ldpc_code {
     std::vector<int32_t> order;   // order[r'] = row in table order
     std::vector<int2> levels;     // (first r', count)
     int widest = 0;
+    // quasi-cyclic description, when the code was built from one
+    bool qc = false;
+    int z = 0, mb = 0, nb = 0;
+    std::vector<int32_t> shifts;  // [mb][nb], -1 = zero block
 };
 
 struct ldpc_decoder {
@@ -77,6 +83,8 @@ struct ldpc_decoder {
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
+    int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel
+    QCParams qcp{};
 };
 
 // ------------------------------------------------------------------------
@@ -177,6 +185,33 @@ extern "C" int ldpc_code_create_from_table(ldpc_code** out, int n, int k_checks,
     return ldpc_code_create(out, n, k_checks, rp.data(), cols.data(), cls.data());
 }
 
+extern "C" int ldpc_code_create_qc(ldpc_code** out, int z, int mb, int nb, const int32_t* shifts)
+{
+    if (!out || !shifts || z < 1 || mb < 1 || nb < 1) return fail(LDPC_ERR_ARG, "ldpc_code_create_qc: bad argument");
+    if ((long long)z * nb > 65535) return fail(LDPC_ERR_UNSUPPORTED, "ldpc_code_create_qc: n = %d > 65535", z * nb);
+    std::vector<int32_t> rp(1, 0), cols;
+    for (int i = 0; i < mb; i++) {
+        for (int k = 0; k < z; k++) {
+            for (int j = 0; j < nb; j++) {
+                int s = shifts[i * nb + j];
+                if (s < -1 || s >= z) return fail(LDPC_ERR_ARG, "shift %d of block (%d,%d) outside [-1,%d)", s, i, j, z);
+                if (s >= 0) cols.push_back(j * z + (k + s) % z);
+            }
+            rp.push_back((int32_t)cols.size());
+        }
+    }
+    ldpc_code* c = nullptr;
+    int rc = ldpc_code_create(&c, z * nb, z * mb, rp.data(), cols.data(), nullptr);
+    if (rc) return rc;
+    c->qc = true;
+    c->z = z;
+    c->mb = mb;
+    c->nb = nb;
+    c->shifts.assign(shifts, shifts + mb * nb);
+    *out = c;
+    return LDPC_OK;
+}
+
 extern "C" int ldpc_code_load(ldpc_code** out, const char* path)
 {
     if (!out || !path) return fail(LDPC_ERR_ARG, "ldpc_code_load: null pointer");
@@ -243,6 +278,40 @@ namespace ldpc {
 const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
+const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2);
+}
+
+// QC register-message kernel, when the code is QC and a matching instantiation exists
+static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
+{
+    if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256) return nullptr;
+    memset(&q, 0, sizeof q);
+    q.z = c->z;
+    q.n = c->n;
+    q.layers = c->mb;
+    int dt = 0;
+    bool exact = true;
+    for (int i = 0; i < c->mb; i++) {
+        int d = 0;
+        for (int j = 0; j < c->nb; j++) {
+            int s = c->shifts[i * c->nb + j];
+            if (s < 0) continue;
+            if (d >= QC_MAX_DEG) return nullptr;
+            q.cz4[i * QC_MAX_DEG + d] = j * c->z * 8;
+            q.s[i * QC_MAX_DEG + d] = s;
+            d++;
+        }
+        if (d == 0) return nullptr;
+        q.deg[i] = d;
+        q.cls[i] = c->row_class[i * c->z];
+        for (int k = 1; k < c->z; k++)
+            if (c->row_class[i * c->z + k] != q.cls[i]) return nullptr;
+        if (i > 0 && d != dt) exact = false;
+        dt = std::max(dt, d);
+    }
+    bool pow2 = (c->z & (c->z - 1)) == 0;
+    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;
+    return kernel_table_qc(k, dt, exact, c->mb, pow2);
 }
 
 // variant: 0/1 = every row has degree 6/7 (fully unrolled), 2/3/4 = rows of
@@ -343,6 +412,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (kind < LDPC_MS || kind > LDPC_XMS) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
     if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
     if (flags != 0) return fail(LDPC_ERR_ARG, "flags must be 0");
+    const int pack_req = pack;
     if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
     if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
     if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
@@ -352,7 +422,10 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     CUDA_TRY(cudaGetDevice(&dev));
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > (size_t)smem_max)
+    QCParams probe;
+    bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
+    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && (size_t)c->n * 8 <= (size_t)smem_max;
+    if (smem > (size_t)smem_max && !qc_ok)
         return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
                     smem, smem_max);
     ldpc_decoder* d = new ldpc_decoder();
@@ -368,9 +441,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         decoder_free(d);
         return rc;
     }
-    d->kfn = kernel_for(pack, kind, degree_variant(c));
-    d->smem = (int)smem;
-    d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    const void* qk = (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2) ? qc_kernel_for(c, kind, d->qcp) : nullptr;
+    if (qk && (size_t)c->n * 8 <= (size_t)smem_max) {
+        d->kfn = qk;
+        d->path = 1;
+        d->pack = LDPC_PACK_F16X2;
+        d->smem = c->n * 8;
+        d->threads = c->z;
+    } else {
+        d->kfn = kernel_for(pack, kind, degree_variant(c));
+        d->smem = (int)smem;
+        d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    }
     cudaError_t e1 = cudaFuncSetAttribute(d->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
     cudaFuncAttributes fa;
     cudaError_t e2 = cudaFuncGetAttributes(&fa, d->kfn);
@@ -406,7 +488,7 @@ extern "C" int ldpc_decoder_info(const ldpc_decoder* d, int* info)
     info[4] = d->smem;
     info[5] = d->ctas_per_sm;
     info[6] = d->regs;
-    info[7] = 4;
+    info[7] = d->path;
     return LDPC_OK;
 }
 
@@ -421,9 +503,10 @@ extern "C" int ldpc_decoder_destroy(ldpc_decoder* d)
 
 static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed, long long word0, long long words,
                   long long total_words, int iters, int32_t* iters_out, int8_t* app_out, int8_t* msg_out,
-                  cudaStream_t st)
+                  cudaStream_t st, const Job* sim = nullptr)
 {
-    Job J;
+    Job J{};
+    if (sim) J = *sim;
     J.llr = llr;
     J.out = out;
     J.out_packed = out_packed;
@@ -435,7 +518,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.iters_out = iters_out;
     J.app_out = app_out;
     J.msg_out = msg_out;
-    void* args[] = {(void*)&d->plan, (void*)&J};
+    void* args[] = {d->path == 1 ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
     CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)words), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
 }
@@ -469,6 +552,31 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
                   (cudaStream_t)stream);
+}
+
+extern "C" int ldpc_simulate(ldpc_decoder* d, size_t n_words, int iters, float sigma, uint64_t seed, uint64_t offset,
+                             const uint8_t* d_codewords, size_t n_codewords, int n_vars, int64_t* d_counts,
+                             uint8_t* d_hard, void* stream)
+{
+    if (!d || !d_counts) return fail(LDPC_ERR_ARG, "simulate: null pointer");
+    if (d->kind == LDPC_XMS) return fail(LDPC_ERR_UNSUPPORTED, "simulate: xMS reads word-interleaved input; use OMS");
+    if (iters < 1) return fail(LDPC_ERR_ARG, "simulate: iterations must be >= 1 (got %d)", iters);
+    if (n_words < 1 || n_words > d->nb_words)
+        return fail(LDPC_ERR_SHAPE, "simulate: %zu words requested, decoder holds %zu", n_words, d->nb_words);
+    if (n_vars < 0 || n_vars > d->n || sigma < 0 || (d_codewords && n_codewords == 0))
+        return fail(LDPC_ERR_ARG, "simulate: bad n_vars / sigma / codewords");
+    CUDA_TRY(cudaSetDevice(d->device));
+    Job J{};
+    J.gen = 1;
+    J.sigma = sigma;
+    J.seed = seed;
+    J.offset = offset;
+    J.cw = d_codewords;
+    J.n_cw = (long long)n_codewords;
+    J.counts = reinterpret_cast<unsigned long long*>(d_counts);
+    J.n_vars = n_vars;
+    return launch(d, nullptr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, nullptr, nullptr, nullptr,
+                  (cudaStream_t)stream, &J);
 }
 
 extern "C" int ldpc_decode_host(ldpc_decoder* d, const int8_t* llr, uint8_t* hard, int iters)
@@ -567,10 +675,11 @@ __global__ void __launch_bounds__(256) int_peak_kernel(uint32_t* out, uint32_t s
     for (int it = 0; it < iters; it++) {
 #pragma unroll
         for (int i = 0; i < 8; i++) {
+            // chains read their neighbour so that no closed form exists
             if (MIX == 0 || (MIX == 2 && (i & 1)))
-                v[i] = (v[i] ^ k) & (v[i] | 0x0f0f0f0fu);  // one LOP3
+                v[i] = (v[i] ^ v[(i + 1) & 7]) & (v[i] | k);  // one LOP3
             else
-                v[i] = v[i] + k + 0x1234567u;               // one IADD3
+                v[i] = v[i] + v[(i + 1) & 7] + k;             // one IADD3
         }
     }
     uint32_t x = 0;

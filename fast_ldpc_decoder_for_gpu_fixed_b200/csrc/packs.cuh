@@ -11,12 +11,13 @@
 //              SIMD intrinsics (__vsubss4, __vabs4, __vminu4, ...).  Same
 //              packing as the reference; word g holds frames 4g..4g+3.
 //   PackF16x2  2 frames per 32-bit word as two fp16 lanes holding the integer
-//              values exactly.  Every value is stored NEGATED (u = -x): then
-//              the reference's "bit 1" test x > 0 is exactly the sign bit of
-//              u (x = 0 gives u = +0, sign 0), so sign products are XORs of
-//              sign bits and conditional negations are sign-bit XORs; the
+//              values exactly.  Every value is NEGATED (u = -x): then the
+//              reference's "bit 1" test x > 0 is exactly the sign bit of u
+//              (x = 0 gives u = +0, sign 0), so sign products are XORs of sign
+//              bits and conditional negations are sign-bit XORs; the
 //              saturations become clamps to [-127, 128].  -0 can appear only
-//              in messages, where x - (-0) = x keeps it harmless.
+//              in messages, where x - (-0) = x keeps it harmless.  APP is
+//              stored biased by +127 (see namespace h2).
 //   PackI8     1 frame per thread lane: int8 in shared memory, int32 math.
 //              APP kept as x, messages kept negated (u = -m, |u| <= 127).
 //
@@ -110,8 +111,130 @@ struct PackSIMD4 {
 // ------------------------------------------------------------------------
 // 2 frames per word, integer-valued fp16 lanes, negated values
 // ------------------------------------------------------------------------
+//
+// Values: u = -x (so the sign bit of u is the reference's "x > 0" test), every
+// integer in [-128, 256] is exact in fp16.  APP is kept biased, b = u + 127 in
+// [0, 255], so the saturation of the extrinsic and of the new APP is one
+// fma.relu (lower bound, FMA pipe) plus one min (upper bound, ALU pipe).
+// min.xorsign.abs folds the running min1 and the XOR of the sign bits of the
+// row into one instruction: its result has magnitude min(|a|,|b|) and sign
+// sign(a) ^ sign(b).
 __device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
-__device__ __forceinline__ __half2 u2h(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+
+namespace h2 {
+constexpr uint32_t SIGN = 0x80008000u, MAG = 0x7fff7fffu;
+constexpr uint32_t ONE = 0x3c003c00u, NEG1 = 0xbc00bc00u, C127 = 0x57f057f0u, CNEG127 = 0xd7f0d7f0u,
+                   C255 = 0x5bf85bf8u, C31 = 0x4fc04fc0u, C1024 = 0x64006400u, CNEG1024 = 0xe400e400u,
+                   C075 = 0x3a003a00u, CNEG0375 = 0xb600b600u, C0875 = 0x3b003b00u, CNEG04375 = 0xb700b700u;
+__device__ __forceinline__ uint32_t fma_relu(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("fma.rn.relu.f16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+__device__ __forceinline__ uint32_t fma(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+__device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t hmin(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("min.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t min_xs(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t max_xs(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("max.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t eq01(uint32_t a, uint32_t b)  // 1.0 where equal, else 0.0
+{
+    uint32_t d;
+    asm("set.eq.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+// floor(m * k) for integer m in [0,127], k = 3/4 or 7/8: m*k - (1/2 - 2^-(bits+1)) is
+// exact, within 1/2 of the floor and never on a tie, so adding 1024 rounds it there.
+__device__ __forceinline__ uint32_t floor_scale(uint32_t m, uint32_t k, uint32_t bias)
+{
+    return add(add(fma_relu(m, k, bias), C1024), CNEG1024);
+}
+
+// row magnitudes from |min1| (a1) and |min2| (a2)
+template <int KIND>
+__device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2)
+{
+    if (KIND == KIND_MS) {
+        c1 = hmin(a2, C31);
+        c2 = hmin(a1, C31);
+    } else if (KIND == KIND_OMS) {
+        c1 = fma_relu(a2, ONE, NEG1);
+        c2 = fma_relu(a1, ONE, NEG1);
+        if (!noclip) {
+            c1 = hmin(c1, C31);
+            c2 = hmin(c2, C31);
+        }
+    } else {
+        c2 = floor_scale(a1, C075, CNEG0375);
+        c1 = (KIND == KIND_NMS) ? floor_scale(a2, C075, CNEG0375) : floor_scale(a2, C0875, CNEG04375);
+    }
+}
+
+// one row over one pair-word: b[j] biased APP in/out, m[j] negated message in/out
+template <int KIND, int DT, bool EXACT>
+__device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov)
+{
+    uint32_t ut[DT];
+    uint32_t mn1 = C127, mn2 = C127;
+#pragma unroll
+    for (int j = 0; j < DT; j++) {
+        if (EXACT || j < d) {
+            uint32_t bt = hmin(fma_relu(m[j], NEG1, b[j]), C255);  // clamp(b - m, 0, 255)
+            b[j] = bt;
+            ut[j] = add(bt, CNEG127);
+            uint32_t mx = max_xs(ut[j], mn1);
+            mn1 = min_xs(mn1, ut[j]);
+            mn2 = min_xs(mn2, mx);
+        }
+    }
+    const uint32_t a1 = mn1 & MAG, a2 = mn2 & MAG;
+    uint32_t c1, c2;
+    mags<KIND>(a1, a2, noclip, c1, c2);
+    const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
+    const uint32_t dcs = sub(c1s, c2s);
+#pragma unroll
+    for (int j = 0; j < DT; j++) {
+        if (EXACT || j < d) {
+            uint32_t r = fma(eq01(ut[j] & MAG, a1), dcs, c2s);  // c1s on the minimum edge, else c2s
+            uint32_t mo = r ^ (ut[j] & SIGN);                   // flip by this edge's own sign
+            m[j] = mo;
+            b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)
+        }
+    }
+    ov |= mn1 & SIGN;
+}
+}  // namespace h2
 
 struct PackF16x2 {
     using S = uint32_t;
@@ -124,73 +247,10 @@ struct PackF16x2 {
     __device__ __forceinline__ static void st_app(S* p, R v) { *p = v; }
     __device__ __forceinline__ static void st_msg(S* p, R v) { *p = v; }
 
-    // floor(m * k) for integer m in [0,127] and k = 3/4 or 7/8: the product
-    // minus (1/2 - 1/2^(bits+1)) is exact in fp16 and lies within 1/2 of the
-    // floor (never on a tie), so adding 1024 rounds it to that integer.
-    __device__ __forceinline__ static __half2 floor_scale(__half2 mn, float k, float bias)
-    {
-        const __half2 big = __float2half2_rn(1024.f);
-        __half2 y = __hfma2_relu(mn, __float2half2_rn(k), __float2half2_rn(-bias));
-        return __hsub2(__hadd2(y, big), big);
-    }
-
-    template <int KIND>
-    __device__ __forceinline__ static void mags(__half2 mn1, __half2 mn2, bool noclip, __half2& c1, __half2& c2)
-    {
-        const __half2 c31 = __float2half2_rn(31.f);
-        if (KIND == KIND_MS) {
-            c1 = __hmin2(mn2, c31);
-            c2 = __hmin2(mn1, c31);
-        } else if (KIND == KIND_OMS) {
-            const __half2 one = __float2half2_rn(1.f), mone = __float2half2_rn(-1.f);
-            c1 = __hfma2_relu(mn2, one, mone);
-            c2 = __hfma2_relu(mn1, one, mone);
-            if (!noclip) {
-                c1 = __hmin2(c1, c31);
-                c2 = __hmin2(c2, c31);
-            }
-        } else {
-            c2 = floor_scale(mn1, 0.75f, 0.375f);
-            if (KIND == KIND_NMS)
-                c1 = floor_scale(mn2, 0.75f, 0.375f);
-            else
-                c1 = floor_scale(mn2, 0.875f, 0.4375f);
-        }
-    }
-
     template <int KIND, int DT, bool EXACT>
     __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
     {
-        const __half2 lo = __float2half2_rn(-127.f), hi = __float2half2_rn(128.f);
-        __half2 mn1 = __float2half2_rn(127.f), mn2 = mn1;
-        uint32_t s = 0;
-#pragma unroll
-        for (int j = 0; j < DT; j++) {
-            if (EXACT || j < d) {
-                __half2 t = __hmin2(__hmax2(__hsub2(u2h(x[j]), u2h(m[j])), lo), hi);
-                x[j] = h2u(t);
-                __half2 a = __habs2(t);
-                mn2 = __hmin2(mn2, __hmax2(a, mn1));
-                mn1 = __hmin2(mn1, a);
-                s ^= x[j];
-            }
-        }
-        __half2 c1, c2;
-        mags<KIND>(mn1, mn2, noclip, c1, c2);
-        s &= 0x80008000u;
-        const uint32_t c1s = h2u(c1) | s, c2s = h2u(c2) | s;
-#pragma unroll
-        for (int j = 0; j < DT; j++) {
-            if (EXACT || j < d) {
-                __half2 t = u2h(x[j]);
-                uint32_t eq = __heq2_mask(__habs2(t), mn1);
-                uint32_t re = (eq & c1s) | (~eq & c2s);
-                uint32_t out = re ^ (x[j] & 0x80008000u);
-                m[j] = out;
-                x[j] = h2u(__hmin2(__hmax2(__hadd2(t, u2h(out)), lo), hi));
-            }
-        }
-        ov |= s;
+        h2::row<KIND, DT, EXACT>(x, m, d, noclip, ov);
     }
 };
 

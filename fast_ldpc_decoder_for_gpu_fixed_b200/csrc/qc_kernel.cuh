@@ -1,0 +1,137 @@
+// Layered decoder for quasi-cyclic codes with every c->v message in registers.
+//
+// A QC code is a base matrix of L block rows ("layers") whose nonzero entries
+// are Z x Z circulant permutations: row k of layer l connects variable
+// c*Z + (k + s) mod Z for every nonzero (c, s) of the layer.  The Z rows of a
+// layer touch disjoint variables, so the reference's serial row order
+// (decoder_oms/cuda/CUDA_OMS_SIMD.cu:138-246) is reproduced exactly by
+// updating a whole layer at once and ordering the layers.
+//
+// Mapping: CTA = Z threads = 4 frames (two fp16x2 pair-words, PackF16x2
+// arithmetic); thread k owns row k of every layer for both pair-words, so its
+// L*D*2 messages never leave registers, and the APP of the 4 frames (biased
+// fp16 pairs, 8 bytes per variable) is the only shared-memory state.  One
+// barrier per layer.  The 4 frames of a CTA are the 4 frames of reference word
+// g, so 2NMS early termination (per 32-bit word) is a __syncthreads_or.
+#pragma once
+#include "decode_kernel.cuh"
+
+namespace ldpc {
+
+constexpr int QC_MAX_LAYERS = 16;
+constexpr int QC_MAX_DEG = 16;
+
+struct QCParams {
+    int z;                   // circulant size = threads per CTA
+    int n;                   // variables = nb * z
+    int layers;
+    int deg[QC_MAX_LAYERS];  // row degree of each layer
+    int cls[QC_MAX_LAYERS];  // reference degree group of each layer (OMS quirk)
+    // per (layer, edge): byte offset of the block column in the APP array and the shift
+    int cz4[QC_MAX_LAYERS * QC_MAX_DEG];
+    int s[QC_MAX_LAYERS * QC_MAX_DEG];
+};
+
+// byte offset (8 bytes per variable) of the variable of edge j of row k in layer l
+template <bool POW2>
+__device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int k)
+{
+    int u = k + Q.s[idx];
+    if (POW2)
+        u &= Q.z - 1;
+    else
+        u = min((unsigned)u, (unsigned)(u - Q.z));
+    return Q.cz4[idx] + u * 8;
+}
+
+template <int KIND, int DT, bool EXACT, int L, bool POW2>
+__global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, const Job J)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint2* app = reinterpret_cast<uint2*>(smem_raw);  // [n] (pair-word 0, pair-word 1)
+    char* appb = reinterpret_cast<char*>(smem_raw);
+    const long long g = J.word0 + blockIdx.x;
+    const int k = threadIdx.x;
+
+    Plan P;  // only n is used by the shared prologue / epilogue helpers
+    P.n = Q.n;
+    read_group(P, J, g, [&](int v, uint32_t w) {
+        app[v] = make_uint2(Access<PackF16x2>::pair(w, 0), Access<PackF16x2>::pair(w, 2));
+    });
+    __syncthreads();
+
+    uint32_t msg[2][L][DT];
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int j = 0; j < DT; j++) msg[w][l][j] = 0;
+
+    int executed = 0;
+    for (int it = 0; it < J.iters; it++) {
+        uint32_t ov = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+            const bool noclip = J.quirk && it == 0 && Q.cls[l];
+            // recompute the 2-instruction addresses each layer instead of pinning
+            // L*D of them in registers across iterations
+            int kk = k;
+            asm volatile("" : "+r"(kk));
+            int off[DT];
+            uint32_t b0[DT], b1[DT];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    off[j] = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk);
+                    uint2 v = *reinterpret_cast<const uint2*>(appb + off[j]);
+                    b0[j] = v.x;
+                    b1[j] = v.y;
+                }
+            }
+            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov);
+            h2::row<KIND, DT, EXACT>(b1, msg[1][l], d, noclip, ov);
+#pragma unroll
+            for (int j = 0; j < DT; j++)
+                if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
+            __syncthreads();
+        }
+        executed = it + 1;
+        if (KIND == KIND_2NMS && it >= 1) {
+            if (!__syncthreads_or(ov != 0)) break;
+        }
+    }
+
+    write_group(P, J, g, [&](int v) { uint2 a = app[v]; return Access<PackF16x2>::unbias(a.x, a.y); });
+    if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
+    if (J.app_out) {
+        uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
+        for (int v = threadIdx.x; v < Q.n; v += blockDim.x) {
+            uint2 a = app[v];
+            ao[(long long)v * J.total_words + g] = Access<PackF16x2>::unbias(a.x, a.y);
+        }
+    }
+    if (J.msg_out) {
+        // edge index in table order: rows are layer-major (row = l*z + k), each row's
+        // edges in the order of the layer's entries; e = first edge of the layer + k*d + j
+        uint32_t* mo = reinterpret_cast<uint32_t*>(J.msg_out);
+        long long e0 = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    auto x = [](uint32_t h) { return (uint32_t)(uint8_t)(int8_t)(-__half2int_rn(__ushort_as_half((uint16_t)h))); };
+                    uint32_t lo = msg[0][l][j], hi = msg[1][l][j];
+                    uint32_t wv = x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
+                    mo[(e0 + (long long)k * d + j) * J.total_words + g] = wv;
+                }
+            }
+            e0 += (long long)Q.z * d;
+        }
+    }
+}
+
+}  // namespace ldpc

@@ -31,9 +31,14 @@ class NativeCode:
     def __init__(self, code):
         self.code = code
         h = ctypes.c_void_p()
-        _lib.check(_lib.lib().ldpc_code_create(
-            ctypes.byref(h), code.n, code.m, code.row_ptr.ctypes.data, code.cols.ctypes.data,
-            code.row_class.ctypes.data))
+        if getattr(code, "shifts", None) is not None and not getattr(code, "no_qc", False):
+            sh = np.where(code.base > 0, code.shifts, -1).astype(np.int32)
+            _lib.check(_lib.lib().ldpc_code_create_qc(ctypes.byref(h), int(code.z), sh.shape[0], sh.shape[1],
+                                                      sh.ctypes.data))
+        else:
+            _lib.check(_lib.lib().ldpc_code_create(
+                ctypes.byref(h), code.n, code.m, code.row_ptr.ctypes.data, code.cols.ctypes.data,
+                code.row_class.ctypes.data))
         self.handle = h
 
     def info(self):
@@ -87,7 +92,7 @@ class Decoder:
     def info(self):
         a = (ctypes.c_int * 8)()
         _lib.check(_lib.lib().ldpc_decoder_info(self.handle, a))
-        keys = ("kind", "pack", "nb_frames", "threads", "smem", "ctas_per_sm", "regs", "frames_per_cta")
+        keys = ("kind", "pack", "nb_frames", "threads", "smem", "ctas_per_sm", "regs", "path")
         return dict(zip(keys, list(a)))
 
     def decode_host(self, llr, hard, iters):
@@ -112,6 +117,15 @@ class Decoder:
         st = getattr(stream, "cuda_stream", stream)
         _lib.check(_lib.lib().ldpc_decode_device_state(self.handle, _ptr(d_llr), _ptr(d_hard), int(n_words),
                                                        int(iters), _ptr(d_iters), _ptr(d_app), _ptr(d_msg), st))
+
+    def simulate(self, n_words, iters, sigma, seed, offset, d_counts, d_codewords=None, n_codewords=0,
+                 n_vars=None, d_hard=None, stream=None):
+        """Fused channel + decode + error count of 4*n_words frames (device buffers)."""
+        st = getattr(stream, "cuda_stream", stream)
+        nv = self.code.n_info if n_vars is None else n_vars
+        _lib.check(_lib.lib().ldpc_simulate(self.handle, int(n_words), int(iters), float(sigma), int(seed),
+                                            int(offset), _ptr(d_codewords), int(n_codewords), int(nv),
+                                            _ptr(d_counts), _ptr(d_hard), st))
 
     def close(self):
         if getattr(self, "handle", None):

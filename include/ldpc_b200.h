@@ -82,6 +82,14 @@ int ldpc_code_create_from_table(ldpc_code** out, int n, int k_checks, int m_edge
 int ldpc_code_create(ldpc_code** out, int n_vars, int n_checks, const int32_t* row_ptr,
                      const int32_t* cols, const uint8_t* row_class);
 
+/* Quasi-cyclic H from a base matrix: shifts[i*nb+j] is the circulant shift of
+ * block (i, j) (row k of block row i meets variable j*z + (k+s) mod z), or -1
+ * for a zero block.  Rows are block-row major (row i*z+k), a row's edges in
+ * ascending block column.  Decoders of such codes may use the QC kernel that
+ * keeps every message in registers.  No reference counterpart (the reference
+ * only ships fixed tables). */
+int ldpc_code_create_qc(ldpc_code** out, int z, int mb, int nb, const int32_t* shifts);
+
 /* Loads a .ldpc table file (format: fast_ldpc_decoder_for_gpu_fixed_b200/codes.py). */
 int ldpc_code_load(ldpc_code** out, const char* path);
 
@@ -124,11 +132,53 @@ int ldpc_decode_device_state(ldpc_decoder* dec, const int8_t* d_llr, uint8_t* d_
                              size_t n_words, int iters, int32_t* d_iters_out,
                              int8_t* d_app, int8_t* d_msg, void* stream);
 
+/* Fused Monte-Carlo step on `stream`: the decoder's prologue draws the LLRs of
+ * 4*n_words frames from the AWGN channel itself (bit-identical to
+ * ldpc_channel_awgn with the same sigma, seed, offset and codewords), decodes
+ * them, and its epilogue adds frames / bit errors / frame errors over the first
+ * n_vars bits to d_counts[0..2] (as ldpc_count_errors).  d_hard (nullable)
+ * also receives the 0/1 decisions.  Replaces the channel -> decode ->
+ * analyser round trip through host memory of src/main.cpp:258-286.  Not for
+ * LDPC_XMS (its input is the word-interleaved layout). */
+int ldpc_simulate(ldpc_decoder* dec, size_t n_words, int iters, float sigma, uint64_t seed,
+                  uint64_t offset, const uint8_t* d_codewords, size_t n_codewords, int n_vars,
+                  int64_t* d_counts, uint8_t* d_hard, void* stream);
+
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
- * per CTA, CTAs per SM, registers per thread, frames per CTA */
+ * per CTA, CTAs per SM, registers per thread, kernel path (0 = level
+ * scheduled, 1 = QC register-message) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
+
+/* ---- channel and error counting (the simulation stages around the decoder) */
+
+/* Noise deviation for an Eb/N0 (or Es/N0 when es_n0) in dB at code rate `rate`,
+ * as CChanel_AWGN_SIMD::configure (src/awgn_channel/CChanel_AWGN_SIMD.cu:63-73). */
+double ldpc_sigma(double ebn0, double rate, int es_n0);
+
+/* AWGN channel on the GPU, replacing CChanel_AWGN_SIMD::generate
+ * (src/awgn_channel/CChanel_AWGN_SIMD.cu:88-112): frames*n int8 LLRs,
+ * frame-major, q = trunc(clamp(8*((2b-1) + sigma*g), -31, 31)) with g a
+ * Box-Muller Gaussian from a Philox4x32-10 stream (seed, offset) indexed by
+ * sample, b the codeword bit (d_codewords: n_codewords frame-major 0/1
+ * codewords used cyclically, or null for the all-zero codeword). */
+int ldpc_channel_awgn(int8_t* d_llr, size_t frames, int n, float sigma, uint64_t seed,
+                      uint64_t offset, const uint8_t* d_codewords, size_t n_codewords,
+                      void* stream);
+
+/* Raw Philox4x32-10 words of stream (seed, offset), count of them (the
+ * channel's uniforms are (word + 0.5) / 2^32).  No reference counterpart. */
+int ldpc_philox(uint32_t* d_out, size_t count, uint64_t seed, uint64_t offset, void* stream);
+
+/* Error counting on the GPU, replacing CErrorAnalyzer::generate
+ * (src/ber_analyzer/CErrorAnalyzer.cpp:119-159): for each of `frames` decided
+ * frames (0/1 bytes, frame-major, n per frame) the bits among the first n_vars
+ * that differ from the transmitted codeword (null: all-zero) are counted;
+ * d_counts[0] += frames, d_counts[1] += bit errors, d_counts[2] += frame errors. */
+int ldpc_count_errors(const uint8_t* d_hard, size_t frames, int n, int n_vars,
+                      const uint8_t* d_codewords, size_t n_codewords, int64_t* d_counts,
+                      void* stream);
 
 /* ---- misc -------------------------------------------------------------- */
 

@@ -40,7 +40,7 @@
  *
  * Parity pin: this restatement is checked against outputs of the reference
  * kernels themselves (compiled from the reference sources by
- * oracle/build_ref.sh and run on a B200 by oracle/make_golden.py); the
+ * oracle/build_ref.sh and run on a B200 by tests/golden/make_golden.py); the
  * resulting fixtures live in tests/golden/.
  */
 #include <stdint.h>
@@ -281,4 +281,64 @@ double oracle_sigma(double ebn0, double rate, int es_n0)
     double interm = 10.0 * log10(rate);
     interm = -0.1 * (eb + interm);
     return sqrt(pow(10.0, interm) / 2);
+}
+
+/* ---- channel restatement in double precision ----------------------------
+ * Philox4x32-10 (Salmon et al., SC'11, the counter-based generator the
+ * project's GPU channel uses in place of the reference's cuRAND XORWOW), then
+ * Box-Muller and the reference quantiser
+ * q = (char) clamp(8 * (mean + sigma * g), -31, 31)
+ * (awgn_channel/CChanel_AWGN_SIMD.cu:17-24) evaluated in double. */
+static void philox10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[1] = (uint32_t)p1;
+        c[3] = (uint32_t)p0;
+        c[0] = n0;
+        c[2] = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+void oracle_philox(uint32_t* out, size_t count, uint64_t seed, uint64_t offset)
+{
+    for (size_t q = 0; 4 * q < count; q++) {
+        uint32_t c[4] = {(uint32_t)q, (uint32_t)(q >> 32), (uint32_t)offset, (uint32_t)(offset >> 32)};
+        philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        for (int i = 0; i < 4 && 4 * q + i < count; i++) out[4 * q + i] = c[i];
+    }
+}
+
+/* also returns, per sample, the pre-quantisation value 8y in y8 (nullable) */
+void oracle_awgn(int8_t* out, double* y8, size_t frames, int n, double sigma, uint64_t seed,
+                 uint64_t offset, const uint8_t* cw, size_t n_cw)
+{
+    const double PI = 3.14159265358979323846;
+    size_t total = frames * (size_t)n;
+    for (size_t q = 0; 4 * q < total; q++) {
+        uint32_t c[4] = {(uint32_t)q, (uint32_t)(q >> 32), (uint32_t)offset, (uint32_t)(offset >> 32)};
+        philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        double u[4], g[4];
+        for (int i = 0; i < 4; i++) u[i] = ((double)c[i] + 0.5) / 4294967296.0;
+        for (int p = 0; p < 2; p++) {
+            double r = sqrt(-2.0 * log(u[2 * p]));
+            g[2 * p] = r * cos(2.0 * PI * u[2 * p + 1]);
+            g[2 * p + 1] = r * sin(2.0 * PI * u[2 * p + 1]);
+        }
+        for (int i = 0; i < 4 && 4 * q + i < total; i++) {
+            size_t s = 4 * q + i;
+            double mean = -1.0;
+            if (cw) {
+                size_t f = s / n, v = s % n;
+                mean = cw[(f % n_cw) * n + v] ? 1.0 : -1.0;
+            }
+            double y = 8.0 * (mean + sigma * g[i]);
+            if (y8) y8[s] = y;
+            out[s] = (int8_t)trunc(fmin(fmax(y, -31.0), 31.0));
+        }
+    }
 }

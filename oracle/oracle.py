@@ -52,6 +52,9 @@ def lib():
         L.oracle_quantize.restype = i
         L.oracle_sigma.argtypes = [ctypes.c_double, ctypes.c_double, i]
         L.oracle_sigma.restype = ctypes.c_double
+        L.oracle_philox.argtypes = [P, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
+        L.oracle_awgn.argtypes = [P, P, ctypes.c_size_t, i, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, P,
+                                  ctypes.c_size_t]
         _lib = L
     return _lib
 
@@ -140,3 +143,19 @@ def count_errors(n, n_vars, hard):
 
 def sigma(ebn0, rate, es_n0=False):
     return lib().oracle_sigma(float(ebn0), float(rate), int(es_n0))
+
+
+def philox(count, seed, offset=0):
+    out = np.zeros(count, dtype=np.uint32)
+    lib().oracle_philox(_p(out), count, seed, offset)
+    return out
+
+
+def awgn(frames, n, sigma, seed, offset=0, codewords=None):
+    """Returns (int8 LLRs [frames, n], pre-quantisation 8y in double)."""
+    out = np.zeros(frames * n, dtype=np.int8)
+    y8 = np.zeros(frames * n, dtype=np.float64)
+    cw = None if codewords is None else np.ascontiguousarray(codewords, dtype=np.uint8)
+    lib().oracle_awgn(_p(out), _p(y8), frames, n, float(sigma), seed, offset, _p(cw),
+                      0 if cw is None else cw.shape[0])
+    return out.reshape(frames, n), y8.reshape(frames, n)

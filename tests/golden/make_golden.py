@@ -103,25 +103,35 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(HERE, "reference_decoder.json"))
     ap.add_argument("--time", default=None, help="only time the reference kernels (config-1 size)")
+    ap.add_argument("--limit", type=int, default=0, help="stop after this many cases (0 = all)")
+    ap.add_argument("--codes", default="", help="comma-separated subset of codes")
     args = ap.parse_args()
     refs = {cid: RefLib(cid) for cid in CODES}
     if args.time:
         return time_kernels(refs, args.time)
     results = []
     mism = 0
-    for case in cases():
+    t_start = time.time()
+    todo = [c for c in cases() if not args.codes or c["code"] in args.codes.split(",")]
+    if args.limit:
+        todo = todo[:args.limit]
+    for case in todo:
         ref = refs[case["lib"]]
         if case["kind"] == "XMS" and not xms_supported(ref):
             continue
         code = load_table(case["code"])
         llr = make_input(case, code.n)
-        hard, app, msg, _ = ref.decode(case["kind"], llr, case["W"], case["iters"])
+        t0 = time.time()
+        hard, app, msg, us = ref.decode(case["kind"], llr, case["W"], case["iters"])
+        t1 = time.time()
         o = oracle.decode(code, case["kind"], llr, case["iters"], want_state=True)
+        t2 = time.time()
         ok = (sha(o["hard"]) == sha(hard) and sha(o["app"]) == sha(app) and sha(o["msg"]) == sha(msg))
         mism += (not ok)
         results.append(dict(case, sha256={"hard": sha(hard), "app": sha(app), "msg": sha(msg)},
                             oracle_agreed=bool(ok)))
         print(case["code"], case["kind"], case["iters"], case["input"]["type"], "oracle", "OK" if ok else "MISMATCH",
+              "ref %.2fs (kernel %.0f us) oracle %.2fs total %.0fs" % (t1 - t0, us, t2 - t1, time.time() - t_start),
               flush=True)
     doc = {"generator": "tests/golden/make_golden.py", "source": "reference kernels built by oracle/build_ref.sh",
            "cases": results}

@@ -37,12 +37,17 @@ def _llr(case, n):
 @pytest.mark.parametrize("pack", ["SIMD4", "F16X2", "I8"])
 def test_gpu_matches_reference_kernels(cuda, pack):
     assert CASES, "golden fixture missing"
-    bad = []
+    bad, done = [], 0
     for case in CASES:
         code = table(case["code"])
-        out = gpu_decode(code, case["kind"], _llr(case, code.n), case["iters"], case["W"], pack=pack)
+        try:
+            out = gpu_decode(code, case["kind"], _llr(case, code.n), case["iters"], case["W"], pack=pack)
+        except pytest.skip.Exception:
+            continue  # state too large for one CTA with this packing (LDPC_ERR_UNSUPPORTED)
+        done += 1
         got = {"hard": sha(out["hard"]), "app": sha(out["app"]), "msg": sha(out["msg"])}
         if got != case["sha256"]:
             bad.append((case["code"], case["kind"], case["iters"], case["input"]["type"],
                         [k for k in got if got[k] != case["sha256"][k]]))
-    assert not bad, "%d of %d cases differ from the reference: %s" % (len(bad), len(CASES), bad[:10])
+    assert not bad, "%d of %d cases differ from the reference: %s" % (len(bad), done, bad[:10])
+    assert done >= len(CASES) * 3 // 4
