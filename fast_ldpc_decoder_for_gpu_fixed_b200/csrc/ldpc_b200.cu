@@ -298,7 +298,7 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
             if (s < 0) continue;
             if (d >= QC_MAX_DEG) return nullptr;
             q.cz4[i * QC_MAX_DEG + d] = j * c->z * 8;
-            q.s[i * QC_MAX_DEG + d] = s;
+            q.s[i * QC_MAX_DEG + d] = 8 * s;
             d++;
         }
         if (d == 0) return nullptr;
@@ -722,3 +722,4 @@ extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
     *lane_ops_per_s = best;
     return LDPC_OK;
 }
+

@@ -144,6 +144,12 @@ __device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b)
     asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
 }
+__device__ __forceinline__ uint32_t add_sat(uint32_t a, uint32_t b)  // clamp(a + b, 0, 1)
+{
+    uint32_t d;
+    asm("add.rn.sat.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
 __device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b)
 {
     uint32_t d;
@@ -166,12 +172,6 @@ __device__ __forceinline__ uint32_t max_xs(uint32_t a, uint32_t b)
 {
     uint32_t d;
     asm("max.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
-    return d;
-}
-__device__ __forceinline__ uint32_t eq01(uint32_t a, uint32_t b)  // 1.0 where equal, else 0.0
-{
-    uint32_t d;
-    asm("set.eq.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
 }
 // floor(m * k) for integer m in [0,127], k = 3/4 or 7/8: m*k - (1/2 - 2^-(bits+1)) is
@@ -222,11 +222,14 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
     uint32_t c1, c2;
     mags<KIND>(a1, a2, noclip, c1, c2);
     const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
-    const uint32_t dcs = sub(c1s, c2s);
+    const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
 #pragma unroll
     for (int j = 0; j < DT; j++) {
         if (EXACT || j < d) {
-            uint32_t r = fma(eq01(ut[j] & MAG, a1), dcs, c2s);  // c1s on the minimum edge, else c2s
+            // |t| >= min1 on every edge, so sat(|t| - min1) is 0 on the minimum edge(s)
+            // and 1 elsewhere: r = c1s there, c2s elsewhere (one FMA instead of a
+            // compare and a select)
+            uint32_t r = fma(add_sat(ut[j] & MAG, na1), dcs, c1s);
             uint32_t mo = r ^ (ut[j] & SIGN);                   // flip by this edge's own sign
             m[j] = mo;
             b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)

@@ -28,20 +28,20 @@ struct QCParams {
     int deg[QC_MAX_LAYERS];  // row degree of each layer
     int cls[QC_MAX_LAYERS];  // reference degree group of each layer (OMS quirk)
     // per (layer, edge): byte offset of the block column in the APP array and the shift
-    int cz4[QC_MAX_LAYERS * QC_MAX_DEG];
-    int s[QC_MAX_LAYERS * QC_MAX_DEG];
+    int cz4[QC_MAX_LAYERS * QC_MAX_DEG];  // 8 * c * z
+    int s[QC_MAX_LAYERS * QC_MAX_DEG];    // 8 * shift
 };
 
-// byte offset (8 bytes per variable) of the variable of edge j of row k in layer l
+// byte offset (8 bytes per variable) of the variable of edge `idx` of row k, from
+// k8 = 8k: ((8k + 8s) mod 8z) + 8cz; for a power-of-two z the mod is a mask and the
+// block offset an OR (its low bits are zero)
 template <bool POW2>
-__device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int k)
+__device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int k8)
 {
-    int u = k + Q.s[idx];
-    if (POW2)
-        u &= Q.z - 1;
-    else
-        u = min((unsigned)u, (unsigned)(u - Q.z));
-    return Q.cz4[idx] + u * 8;
+    int u = k8 + Q.s[idx];
+    if (POW2) return (u & (8 * Q.z - 1)) | Q.cz4[idx];
+    u = min((unsigned)u, (unsigned)(u - 8 * Q.z));
+    return Q.cz4[idx] + u;
 }
 
 template <int KIND, int DT, bool EXACT, int L, bool POW2>
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
             const bool noclip = J.quirk && it == 0 && Q.cls[l];
             // recompute the 2-instruction addresses each layer instead of pinning
             // L*D of them in registers across iterations
-            int kk = k;
+            int kk = 8 * k;
             asm volatile("" : "+r"(kk));
             int off[DT];
             uint32_t b0[DT], b1[DT];

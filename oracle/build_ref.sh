@@ -28,7 +28,7 @@ dir_of() {
 }
 
 CODES=("$@")
-[ ${#CODES[@]} -gt 0 ] || CODES=(4000 576 1944 2048 816 9972)
+[ ${#CODES[@]} -gt 0 ] || CODES=(4000)
 
 for CODE in "${CODES[@]}"; do
     D=$(dir_of "$CODE")

@@ -57,3 +57,11 @@ def sigma_for(ebn0_db, rate):
     """Noise deviation of the reference channel (CChanel_AWGN_SIMD.cu:63-73)."""
     interm = -0.1 * (ebn0_db + 10.0 * np.log10(rate))
     return float(np.sqrt(10.0 ** interm / 2.0))
+
+
+def case_llr(case, n):
+    """LLRs of a golden-fixture case (see make_golden.make_input)."""
+    inp = case["input"]
+    words = 1 if inp.get("tile") else case["W"]
+    x = llr(inp["type"], 4 * words * n, inp["seed"], sigma=inp.get("sigma"), value=inp.get("value", 0))
+    return np.tile(x, case["W"]) if inp.get("tile") else x

@@ -31,8 +31,12 @@ from oracle import oracle  # noqa: E402
 from fast_ldpc_decoder_for_gpu_fixed_b200.codes import load_table  # noqa: E402
 
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
-CODES = {4000: "4000x2000", 576: "576x288", 1944: "1944x972", 2048: "2048x384",
-         816: "816x408", 9972: "9972x4986"}
+# Only the reference's default table (src/matrix/code.h: CODE 4000).  Its build for the
+# two-degree 576x288 table stopped with cudaErrorInvalidAddressSpace (717) inside the
+# reference decoder kernel on a B200, on inputs checked in bounds, so the reference's
+# kernels are not run on the other tables; those are covered by the CPU oracle, which
+# these 4000x2000 cases pin.
+CODES = {4000: "4000x2000"}
 KINDS = ["MS", "OMS", "NMS", "2NMS", "XMS"]
 
 
@@ -80,8 +84,15 @@ def cases():
         for kind in KINDS:
             for inp in inputs:
                 seed += 1
+                # The reference 2NMS kernel (EARLY_TERM 1) leaves its iteration loop per
+                # thread while the other threads of the CTA keep executing the row loops'
+                # __syncthreads(); words of one CTA that stop at different iterations
+                # leave those barriers divergent and the kernel hangs (seen on a B200 with
+                # the 4000x2000 code at Eb/N0 2.5 dB).  Its cases therefore repeat one
+                # word across the batch, so that every thread stops at the same iteration.
+                tile = {"tile": True} if kind == "2NMS" else {}
                 out.append({"code": name, "lib": cid, "kind": kind, "iters": 20, "W": 32,
-                            "input": dict(inp, seed=seed)})
+                            "input": dict(inp, seed=seed, **tile)})
         for iters in (1, 2, 3):
             seed += 1
             out.append({"code": name, "lib": cid, "kind": "OMS", "iters": iters, "W": 32,
@@ -89,14 +100,14 @@ def cases():
         seed += 1
         out.append({"code": name, "lib": cid, "kind": "2NMS", "iters": 30, "W": 32,
                     "input": {"type": "awgn", "ebn0": 3.5, "sigma": llr_gen.sigma_for(3.5, rate),
-                              "seed": seed}})
+                              "seed": seed, "tile": True}})
     return out
 
 
 def make_input(case, n):
-    inp = case["input"]
-    count = 4 * case["W"] * n
-    return llr_gen.llr(inp["type"], count, inp["seed"], sigma=inp.get("sigma"), value=inp.get("value", 0))
+    """Deterministic LLRs of a case.  With "tile", one 4-frame word is generated
+    and repeated in every word of the batch (used for every 2NMS case, see cases())."""
+    return llr_gen.case_llr(case, n)
 
 
 def main():
@@ -138,7 +149,7 @@ def main():
     with open(args.out, "w") as f:
         json.dump(doc, f, indent=1)
     print("cases", len(results), "oracle mismatches", mism)
-    return 0
+    return 0 if mism == 0 else 1
 
 
 def time_kernels(refs, path):
@@ -150,6 +161,8 @@ def time_kernels(refs, path):
     for W in (1024, 8192):
         llr = llr_gen.llr("awgn", 4 * W * code.n, 7, sigma=llr_gen.sigma_for(2.0, rate))
         for kind in KINDS:
+            if kind == "2NMS":
+                continue  # its early termination hangs on divergent barriers (see cases())
             ts = []
             for _ in range(4):
                 _, _, _, us = ref.decode(kind, llr, W, 20, block=128, want_state=False)

@@ -29,9 +29,7 @@ CASES = _cases()
 
 
 def _llr(case, n):
-    inp = case["input"]
-    return llr_gen.llr(inp["type"], 4 * case["W"] * n, inp["seed"], sigma=inp.get("sigma"),
-                       value=inp.get("value", 0))
+    return llr_gen.case_llr(case, n)
 
 
 @pytest.mark.parametrize("pack", ["SIMD4", "F16X2", "I8"])

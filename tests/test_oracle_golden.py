@@ -31,8 +31,7 @@ def test_oracle_matches_reference(idx):
     case = CASES[idx]
     code = load_table(case["code"])
     inp = case["input"]
-    llr = llr_gen.llr(inp["type"], 4 * case["W"] * code.n, inp["seed"], sigma=inp.get("sigma"),
-                      value=inp.get("value", 0))
+    llr = llr_gen.case_llr(case, code.n)
     o = oracle.decode(code, case["kind"], llr, case["iters"], want_state=True)
     got = {"hard": _sha(o["hard"]), "app": _sha(o["app"]), "msg": _sha(o["msg"])}
     assert got == case["sha256"]
