@@ -41,6 +41,7 @@ SIGNATURES = {
     "ldpc_channel_awgn": (_I, [_P, _SZ, _I, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64, _P, _SZ, _P]),
     "ldpc_philox": (_I, [_P, _SZ, ctypes.c_uint64, ctypes.c_uint64, _P]),
     "ldpc_count_errors": (_I, [_P, _SZ, _I, _I, _P, _SZ, _P, _P]),
+    "ldpc_decode_noalloc": (_I, [_P, _I, _I, _P, _P, _SZ, _I, _P]),
     "ldpc_simulate": (_I, [_P, _SZ, _I, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64, _P, _SZ, _I, _P, _P, _P]),
 }
 

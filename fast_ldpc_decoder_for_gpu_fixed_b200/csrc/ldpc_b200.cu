@@ -19,6 +19,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -723,3 +724,105 @@ extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
     return LDPC_OK;
 }
 
+// ------------------------------------------------------------------------
+// Decoding without any allocation
+// ------------------------------------------------------------------------
+//
+// Some callers may not allocate device memory once they are running: real-time
+// receive chains and plugin hosts that reserve all GPU memory at start-up, where
+// cudaMalloc can stall for milliseconds, cudaFree synchronises the whole device,
+// and a framework-owned memory pool may refuse the request outright.  For them,
+// ldpc_decode_noalloc decodes with the level-scheduled kernel and no allocation:
+// the per-code tables that ldpc_decoder_create puts in its own device buffers
+// (column table, row degrees, row groups, level list) go instead into the
+// fixed array below, which every GPU that loads this library holds until exit.
+
+#define LDPC_NOALLOC_SCRATCH_BYTES (256 * 1024)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LDPC_NOALLOC_SCRATCH_BYTES];
+
+// host image of the tables, filled per call, copied into the device array
+static unsigned char g_noalloc_host[LDPC_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mutex;
+static const int kNoallocMaxDevices = 64;
+static void* g_noalloc_dev_ptr[kNoallocMaxDevices];
+
+extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const int8_t* d_llr, uint8_t* d_hard,
+                                   size_t n_words, int iters, void* stream)
+{
+    if (!c || !d_llr || !d_hard) return fail(LDPC_ERR_ARG, "ldpc_decode_noalloc: null pointer");
+    if (kind < LDPC_MS || kind > LDPC_XMS) return fail(LDPC_ERR_ARG, "ldpc_decode_noalloc: unknown kind %d", kind);
+    if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
+    if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "ldpc_decode_noalloc: unknown pack");
+    if (iters < 1) return fail(LDPC_ERR_ARG, "ldpc_decode_noalloc: iterations must be >= 1 (got %d)", iters);
+    if (n_words < 1) return fail(LDPC_ERR_SHAPE, "ldpc_decode_noalloc: n_words must be >= 1");
+    if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
+    const int m = c->m, dmax = c->dmax, nlev = (int)c->levels.size();
+    // layout: cols u16 [dmax][m] | rowdeg u8 [m] | rowcls u8 [m] | pad to 8 | levels int2 [nlev]
+    const size_t off_deg = (size_t)dmax * m * 2, off_cls = off_deg + m, off_lev = (off_cls + m + 7) / 8 * 8;
+    const size_t bytes = off_lev + (size_t)nlev * sizeof(int2);
+    if (bytes > LDPC_NOALLOC_SCRATCH_BYTES)
+        return fail(LDPC_ERR_UNSUPPORTED,
+                    "ldpc_decode_noalloc: the code's tables need %zu bytes, more than the %d-byte static array",
+                    bytes, LDPC_NOALLOC_SCRATCH_BYTES);
+    const int npad = (c->n + 15) / 16 * 16;
+    const size_t smem = smem_bytes(pack, npad, dmax, m);
+    int dev = 0, smem_max = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) return fail(LDPC_ERR_UNSUPPORTED, "device %d out of range", dev);
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)smem_max)
+        return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)", smem,
+                    smem_max);
+    const void* kfn = kernel_for(pack, kind, degree_variant(c));
+    if (!kfn) return fail(LDPC_ERR_UNSUPPORTED, "ldpc_decode_noalloc: no kernel for this pack/kind");
+
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    // first call on this device: the device address of the static array
+    if (!g_noalloc_dev_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_dev_ptr[dev] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(g_noalloc_dev_ptr[dev]);
+    // every byte the kernel reads is rewritten for this call
+    uint16_t* hcols = reinterpret_cast<uint16_t*>(g_noalloc_host);
+    uint8_t* hdeg = g_noalloc_host + off_deg;
+    uint8_t* hcls = g_noalloc_host + off_cls;
+    int2* hlev = reinterpret_cast<int2*>(g_noalloc_host + off_lev);
+    memset(g_noalloc_host, 0, bytes);
+    for (int rp = 0; rp < m; rp++) {
+        const int r = c->order[rp], b = c->row_ptr[r], dg = c->row_ptr[r + 1] - b;
+        hdeg[rp] = (uint8_t)dg;
+        hcls[rp] = c->row_class[r];
+        for (int j = 0; j < dg; j++) hcols[(size_t)j * m + rp] = (uint16_t)c->cols[b + j];
+    }
+    for (int l = 0; l < nlev; l++) hlev[l] = c->levels[l];
+    cudaStream_t st = (cudaStream_t)stream;
+    // pageable source: the call returns once the host image has been consumed
+    CUDA_TRY(cudaMemcpyAsync(base, g_noalloc_host, bytes, cudaMemcpyHostToDevice, st));
+
+    Plan P{};
+    P.n = c->n;
+    P.npad = npad;
+    P.m = m;
+    P.dmax = dmax;
+    P.nlevels = nlev;
+    P.cols = reinterpret_cast<const uint16_t*>(base);
+    P.rowdeg = base + off_deg;
+    P.rowcls = base + off_cls;
+    P.levels = reinterpret_cast<const int2*>(base + off_lev);
+    P.edge_orig = nullptr;
+    Job J{};
+    J.llr = d_llr;
+    J.out = d_hard;
+    J.interleaved = kind == LDPC_XMS;
+    J.total_words = (long long)n_words;
+    J.iters = iters;
+    J.quirk = kind == LDPC_OMS;
+    const int threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* args[] = {(void*)&P, (void*)&J};
+    CUDA_TRY(cudaLaunchKernel(kfn, dim3((unsigned)n_words), dim3(threads), args, smem, st));
+    return LDPC_OK;
+}

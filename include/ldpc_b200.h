@@ -144,6 +144,21 @@ int ldpc_simulate(ldpc_decoder* dec, size_t n_words, int iters, float sigma, uin
                   uint64_t offset, const uint8_t* d_codewords, size_t n_codewords, int n_vars,
                   int64_t* d_counts, uint8_t* d_hard, void* stream);
 
+/* Decode with no allocation at all, for callers that may not call cudaMalloc
+ * once running (real-time receive chains, plugin hosts whose memory pool owns
+ * the GPU: an allocation can stall, cudaFree synchronises the device, a pool
+ * may refuse).  No counterpart in the reference.  Same arguments and results
+ * as ldpc_decode_device with LDPC_OUT_BYTES for a decoder of `kind` and `pack`
+ * on `code` (level-scheduled kernel), but nothing is allocated: the code's
+ * device tables go into a static 256 KiB array inside the library that every
+ * GPU loading it keeps until exit.  Codes whose tables exceed it return
+ * LDPC_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture.  Every call rewrites
+ * the array: calls that overlap on the GPU (different streams, no ordering)
+ * race; issue them on one stream or synchronise between them. */
+int ldpc_decode_noalloc(const ldpc_code* code, int kind, int pack, const int8_t* d_llr,
+                        uint8_t* d_hard, size_t n_words, int iters, void* stream);
+
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level
  * scheduled, 1 = QC register-message) */
