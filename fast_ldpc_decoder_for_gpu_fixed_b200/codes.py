@@ -190,6 +190,107 @@ def qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name=None):
     return code
 
 
+def ira(n=64800, k=32400, group=360, frac_high=0.2, deg_high=8, deg_low=3, seed=2025, name=None):
+    """Seeded IRA code (DVB-S2-like structure): information columns in groups of
+    `group`; a fraction `frac_high` of the groups have degree `deg_high`, the rest
+    `deg_low`; each group's first column draws its check rows uniformly from the
+    seed and the other columns of the group follow with a cyclic step of
+    (n - k) / group, as in DVB-S2.  The parity part is the dual-diagonal staircase
+    (parity j in checks j and j+1).  Defaults: N=64800, K=32400, 1/5 of the groups
+    of degree 8, the rest of degree 3 (check degree about 6)."""
+    m = n - k
+    if k % group or m % group:
+        raise ValueError("k and n-k must be multiples of the group size")
+    q = m // group
+    rng = np.random.default_rng(seed)
+    ngroups = k // group
+    n_high = int(round(frac_high * ngroups))
+    rows = [[] for _ in range(m)]
+    for gi in range(ngroups):
+        deg = deg_high if gi < n_high else deg_low
+        base = rng.choice(m, size=deg, replace=False)
+        for c in range(group):
+            col = gi * group + c
+            for b in base:
+                rows[(int(b) + c * q) % m].append(col)
+    for j in range(m):
+        rows[j].append(k + j)
+        if j > 0:
+            rows[j].append(k + j - 1)
+    rows = [sorted(set(r)) for r in rows]
+    code = Code.from_rows(name or "ira%dx%d_s%d" % (n, m, seed), n, rows)
+    code.ira_k = k
+    return code
+
+
+class IRAEncoder:
+    """Linear-time systematic encoder of an `ira` code: p_j = p_{j-1} + (sum of the
+    information bits of check j), i.e. a cumulative XOR down the staircase."""
+
+    def __init__(self, code):
+        self.n, self.k = code.n, code.ira_k
+        m = code.m
+        h = np.zeros((m, self.k), dtype=np.uint8)
+        for r, cols in enumerate(code.rows()):
+            info = cols[cols < self.k]
+            h[r, info] ^= 1
+        self.hi = h.astype(np.float32)
+
+    def encode(self, info):
+        info = np.asarray(info, dtype=np.uint8)
+        s = np.mod(info.astype(np.float32) @ self.hi.T, 2).astype(np.uint8)
+        par = np.bitwise_xor.accumulate(s, axis=1)
+        return np.concatenate([info, par], axis=1)
+
+
+def qc_irregular(z=27, rate=(1, 2), seed=2026, nb=24, degrees=(2, 3, 4, 11), name=None):
+    """Seeded irregular QC code with a 24-column base and a dual-diagonal parity part
+    (802.11n-like layout): mb = nb*(1-rate) block rows, information block columns of
+    degrees drawn from `degrees` (at least one of the largest), a first parity column
+    of weight 3 (shifts s, 0, s at the top, middle and bottom rows) and a staircase of
+    identity blocks; shifts uniform in [0, z) with 4-cycles rejected."""
+    num, den = rate
+    mb = nb * (den - num) // den
+    kb = nb - mb
+    for attempt in range(100):
+        rng = np.random.default_rng(seed + 7717 * attempt)
+        base = np.zeros((mb, nb), dtype=np.uint8)
+        shifts = np.zeros((mb, nb), dtype=np.int64)
+        top = min(max(degrees), mb)
+        degs = [top] + [min(int(rng.choice(degrees)), mb) for _ in range(kb - 1)]
+        for j, d in enumerate(degs):
+            base[rng.choice(mb, size=d, replace=False), j] = 1
+        # parity part: column kb weight 3 (rows 0, mb//2, mb-1), then the identity staircase;
+        # its shifts are fixed first so that the information shifts are checked against them
+        for i in (0, mb // 2, mb - 1):
+            base[i, kb] = 1
+        for j in range(1, mb):
+            base[j - 1, kb + j] = 1
+            base[j, kb + j] = 1
+        s0 = int(rng.integers(1, z))
+        for i in (0, mb - 1):
+            shifts[i, kb] = s0
+        ok = True
+        for j in range(kb):
+            for i in np.flatnonzero(base[:, j]):
+                for _ in range(2000):
+                    shifts[i, j] = rng.integers(0, z)
+                    if not _qc_has_4cycle(base, shifts, z, i, j):
+                        break
+                else:
+                    ok = False
+                    break
+            if not ok:
+                break
+        if ok:
+            break
+    else:
+        raise RuntimeError("no 4-cycle-free base found for z=%d rate %d/%d" % (z, num, den))
+    code = qc_from_base(name or "qcirr_z%d_r%d%d_s%d" % (z, num, den, seed), base, shifts, z)
+    code.base, code.shifts, code.z = base, shifts, z
+    return code
+
+
 class Encoder:
     """Systematic encoder for any H: Gaussian elimination over GF(2) gives pivot
     (parity) columns P and free (information) columns I with H_P^-1 H_I = A, so a

@@ -153,7 +153,7 @@ __device__ __forceinline__ void read_group(const Plan& P, const Job& J, long lon
 // (ber_analyzer/CErrorAnalyzer.cpp:142-158): bits among the first n_vars whose
 // decision (x > 0) differs from the codeword bit.  Every thread of the CTA calls it.
 template <class F>
-__device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, long long g, F get)
+__device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, long long g, F get, int kmask)
 {
     __shared__ int part[4][32];
     int e[4] = {0, 0, 0, 0};
@@ -161,6 +161,7 @@ __device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, 
         uint32_t h = __vsetgts4(get(v), 0u);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
+            if (!((kmask >> k) & 1)) continue;
             int bit = (h >> (8 * k)) & 1;
             int ref = J.cw ? (J.cw[((4ull * g + k) % (unsigned long long)J.n_cw) * P.n + v] != 0) : 0;
             e[k] += bit != ref;
@@ -176,14 +177,16 @@ __device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, 
         for (int k = 0; k < 4; k++) part[k][threadIdx.x >> 5] = e[k];
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long be = 0, fe = 0;
+        unsigned long long be = 0, fe = 0, nf = 0;
         for (int k = 0; k < 4; k++) {
+            if (!((kmask >> k) & 1)) continue;
             int t = 0;
             for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) t += part[k][w];
             be += t;
             fe += t != 0;
+            nf++;
         }
-        atomicAdd(J.counts + 0, 4ull);
+        atomicAdd(J.counts + 0, nf);
         atomicAdd(J.counts + 1, be);
         atomicAdd(J.counts + 2, fe);
     }
@@ -191,11 +194,11 @@ __device__ __forceinline__ void count_group_errors(const Plan& P, const Job& J, 
 
 // Writes hard decisions; get(v) returns the 4-frame byte word (values as x) of variable v.
 template <class F>
-__device__ __forceinline__ void write_group(const Plan& P, const Job& J, long long g, F get)
+__device__ __forceinline__ void write_group(const Plan& P, const Job& J, long long g, F get, int kmask = 0xF)
 {
     const int n = P.n;
     const long long lg = g - J.word0;
-    if (J.counts) count_group_errors(P, J, g, get);
+    if (J.counts) count_group_errors(P, J, g, get, kmask);
     if (!J.out) return;
     if (!J.out_packed) {
         uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + 4 * lg * n;
@@ -208,13 +211,15 @@ __device__ __forceinline__ void write_group(const Plan& P, const Job& J, long lo
                 for (int j = 0; j < 4; j++) a[j] = __vsetgts4(get(4 * q + j), 0u);
                 transpose4x4(a, w);
 #pragma unroll
-                for (int k = 0; k < 4; k++) o32[k * n4 + q] = w[k];
+                for (int k = 0; k < 4; k++)
+                    if ((kmask >> k) & 1) o32[k * n4 + q] = w[k];
             }
         } else {
             for (int v = threadIdx.x; v < n; v += blockDim.x) {
                 uint32_t h = __vsetgts4(get(v), 0u);
 #pragma unroll
-                for (int k = 0; k < 4; k++) o[k * n + v] = (h >> (8 * k)) & 1;
+                for (int k = 0; k < 4; k++)
+                    if ((kmask >> k) & 1) o[k * n + v] = (h >> (8 * k)) & 1;
             }
         }
     } else {
@@ -228,7 +233,8 @@ __device__ __forceinline__ void write_group(const Plan& P, const Job& J, long lo
                 if (v < n) acc |= __vsetgts4(get(v), 0u) << j;
             }
 #pragma unroll
-            for (int k = 0; k < 4; k++) o[k * nb + b] = (acc >> (8 * k)) & 0xff;
+            for (int k = 0; k < 4; k++)
+                if ((kmask >> k) & 1) o[k * nb + b] = (acc >> (8 * k)) & 0xff;
         }
     }
 }
@@ -270,6 +276,25 @@ template <> struct Access<PackF16x2> {
         auto x = [](uint16_t h) { return (uint32_t)(uint8_t)(int8_t)(-__half2int_rn(__ushort_as_half(h))); };
         uint32_t lo = msg[idx], hi = msg[stride + idx];
         return x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
+    }
+};
+
+// one pair-word (frames 2h, 2h+1 of the word); get/get_msg leave the other 2 bytes 0
+struct AccessHalf {
+    __device__ __forceinline__ static void put(uint32_t* app, int v, uint32_t w, int h)
+    {
+        app[v] = Access<PackF16x2>::pair(w, 2 * h);
+    }
+    __device__ __forceinline__ static uint32_t spread(uint32_t two, int h) { return two << (16 * h); }
+    __device__ __forceinline__ static uint32_t get(const uint32_t* app, int v, int h)
+    {
+        return spread(Access<PackF16x2>::unbias(app[v], 0x57f057f0u) & 0xffffu, h);
+    }
+    __device__ __forceinline__ static uint32_t get_msg(const uint32_t* msg, int idx, int h)
+    {
+        auto x = [](uint16_t hv) { return (uint32_t)(uint8_t)(int8_t)(-__half2int_rn(__ushort_as_half(hv))); };
+        uint32_t lo = msg[idx];
+        return spread(x(lo & 0xffff) | (x(lo >> 16) << 8), h);
     }
 };
 
@@ -381,6 +406,59 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
             const int j = i / P.m, r = i - j * P.m;
             if (j < P.rowdeg[r])
                 mo[(long long)P.edge_orig[i] * J.total_words + g] = Access<PK>::get_msg(msg, mstride, i);
+        }
+    }
+}
+
+// The level-scheduled kernel for PackF16x2h: a CTA holds frames 2h, 2h+1 of word g
+// (blockIdx.x = 2 * (g - word0) + h).  Same schedule and arithmetic as above.
+template <int KIND, int DT, bool EXACT>
+__global__ void __launch_bounds__(256) decode_levels_half_kernel(const Plan P, const Job J)
+{
+    using PK = PackF16x2h;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* app = reinterpret_cast<uint32_t*>(smem_raw);
+    uint32_t* msg = app + P.npad;
+    const long long g = J.word0 + (blockIdx.x >> 1);
+    const int h = blockIdx.x & 1;
+
+    read_group(P, J, g, [&](int v, uint32_t w) { AccessHalf::put(app, v, w, h); });
+    for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) msg[i] = 0;
+    __syncthreads();
+
+    uint32_t ov = 0;
+    for (int it = 0; it < J.iters; it++) {
+        const bool first = (it == 0);
+        for (int l = 0; l < P.nlevels; l++) {
+            const int2 lv = __ldg(P.levels + l);
+            for (int r = lv.x + threadIdx.x; r < lv.x + lv.y; r += blockDim.x) {
+                const int d = EXACT ? DT : __ldg(P.rowdeg + r);
+                const bool noclip = J.quirk && first && __ldg(P.rowcls + r);
+                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov);
+            }
+            __syncthreads();
+        }
+    }
+
+    const int kmask = 3 << (2 * h);
+    write_group(P, J, g, [&](int v) { return AccessHalf::get(app, v, h); }, kmask);
+    if (J.iters_out && threadIdx.x == 0 && h == 0) J.iters_out[g - J.word0] = J.iters;
+    if (J.app_out) {
+        uint8_t* ao = reinterpret_cast<uint8_t*>(J.app_out);
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
+            uint32_t w = AccessHalf::get(app, v, h);
+            for (int k = 2 * h; k < 2 * h + 2; k++) ao[((long long)v * J.total_words + g) * 4 + k] = w >> (8 * k);
+        }
+    }
+    if (J.msg_out) {
+        uint8_t* mo = reinterpret_cast<uint8_t*>(J.msg_out);
+        for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) {
+            const int j = i / P.m, r = i - j * P.m;
+            if (j < P.rowdeg[r]) {
+                uint32_t w = AccessHalf::get_msg(msg, i, h);
+                for (int k = 2 * h; k < 2 * h + 2; k++)
+                    mo[((long long)P.edge_orig[i] * J.total_words + g) * 4 + k] = w >> (8 * k);
+            }
         }
     }
 }

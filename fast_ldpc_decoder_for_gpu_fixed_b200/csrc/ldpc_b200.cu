@@ -84,7 +84,8 @@ struct ldpc_decoder {
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
-    int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel
+    int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA
+    int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
 };
 
@@ -280,12 +281,16 @@ const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2);
+const void* kernel_table_f16x2h(int kind, int variant);
 }
+
+// shared memory of the QC kernel: the APP of 4 frames, 8 bytes per variable
+static size_t qc_smem(const ldpc_code* c) { return (size_t)c->n * 8; }
 
 // QC register-message kernel, when the code is QC and a matching instantiation exists
 static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
 {
-    if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256) return nullptr;
+    if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > 65535) return nullptr;
     memset(&q, 0, sizeof q);
     q.z = c->z;
     q.n = c->n;
@@ -418,14 +423,16 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
     if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
     int npad = (c->n + 15) / 16 * 16;
-    size_t smem = smem_bytes(pack, npad, c->dmax, c->m);
+    // fp16x2 without early termination: 2 frames per CTA (half the shared memory)
+    const bool half = pack == LDPC_PACK_F16X2 && kind != LDPC_2NMS;
+    size_t smem = half ? 4 * ((size_t)npad + (size_t)c->dmax * c->m) : smem_bytes(pack, npad, c->dmax, c->m);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     QCParams probe;
     bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
-    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && (size_t)c->n * 8 <= (size_t)smem_max;
+    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && qc_smem(c) <= (size_t)smem_max;
     if (smem > (size_t)smem_max && !qc_ok)
         return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
                     smem, smem_max);
@@ -443,12 +450,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return rc;
     }
     const void* qk = (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2) ? qc_kernel_for(c, kind, d->qcp) : nullptr;
-    if (qk && (size_t)c->n * 8 <= (size_t)smem_max) {
+    if (qk && qc_smem(c) <= (size_t)smem_max) {
         d->kfn = qk;
         d->path = 1;
         d->pack = LDPC_PACK_F16X2;
-        d->smem = c->n * 8;
+        d->smem = (int)qc_smem(c);
         d->threads = c->z;
+    } else if (half) {
+        d->kfn = kernel_table_f16x2h(kind == LDPC_XMS ? LDPC_OMS : kind, degree_variant(c));
+        d->path = 2;
+        d->grid_mult = 2;
+        d->smem = (int)smem;
+        d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     } else {
         d->kfn = kernel_for(pack, kind, degree_variant(c));
         d->smem = (int)smem;
@@ -520,7 +533,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.app_out = app_out;
     J.msg_out = msg_out;
     void* args[] = {d->path == 1 ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
-    CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)words), dim3(d->threads), args, d->smem, st));
+    CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
 }
 

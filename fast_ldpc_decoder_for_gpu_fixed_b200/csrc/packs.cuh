@@ -257,6 +257,14 @@ struct PackF16x2 {
     }
 };
 
+// The same packing for a CTA that holds only 2 of the 4 frames of a word (one
+// pair-word): half the shared memory per CTA, twice the CTAs.  Not for 2NMS,
+// whose early termination is decided per 4-frame word.
+struct PackF16x2h : PackF16x2 {
+    static constexpr int WPC = 1;
+    static constexpr int ID = 3;
+};
+
 // ------------------------------------------------------------------------
 // 1 frame per lane, int8 storage, int32 arithmetic
 // ------------------------------------------------------------------------

@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
             const int d = EXACT ? DT : Q.deg[l];
             const bool noclip = J.quirk && it == 0 && Q.cls[l];
             // recompute the 2-instruction addresses each layer instead of pinning
-            // L*D of them in registers across iterations
+            // L*D of them in registers across iterations (a shared-memory table of
+            // them measured slower: the dependent load costs more than it saves)
             int kk = 8 * k;
             asm volatile("" : "+r"(kk));
             int off[DT];

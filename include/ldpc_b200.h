@@ -161,7 +161,8 @@ int ldpc_decode_noalloc(const ldpc_code* code, int kind, int pack, const int8_t*
 
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level
- * scheduled, 1 = QC register-message) */
+ * scheduled, 1 = QC register-message, 2 = level scheduled with 2 frames per
+ * CTA: LDPC_PACK_F16X2 for every kind but 2NMS) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
