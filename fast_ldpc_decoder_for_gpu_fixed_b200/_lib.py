@@ -12,9 +12,10 @@ LIB_PATH = os.path.join(_HERE, "libldpc_b200.so")
 LDPC_OK = 0
 ERRORS = {-1: "LDPC_ERR_ARG", -2: "LDPC_ERR_CUDA", -3: "LDPC_ERR_UNSUPPORTED", -4: "LDPC_ERR_NOMEM",
           -5: "LDPC_ERR_SHAPE"}
-KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4}
+KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 5}
 PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2}
 OUT_BYTES, OUT_PACKED = 0, 1
+FLAG_EARLY_STOP = 1
 
 # every entry point declared in include/ldpc_b200.h: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -32,7 +33,10 @@ SIGNATURES = {
     "ldpc_decode_device": (_I, [_P, _P, _P, _SZ, _I, _I, _P, _P]),
     "ldpc_decode_device_state": (_I, [_P, _P, _P, _SZ, _I, _P, _P, _P, _P]),
     "ldpc_decoder_info": (_I, [_P, _P]),
+    "ldpc_decoder_set_learned": (_I, [_P, _I, _P, _P]),
     "ldpc_decoder_destroy": (_I, [_P]),
+    "ldpc_train_step": (_I, [_P, _P, _P, _P, _SZ, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ldpc_train_stash_bytes": (_SZ, [_P, _SZ, _I]),
     "ldpc_last_error_string": (ctypes.c_char_p, []),
     "ldpc_version": (_I, []),
     "ldpc_simd_selftest": (_I, [_I, _P, _P, _P, _SZ, _P]),

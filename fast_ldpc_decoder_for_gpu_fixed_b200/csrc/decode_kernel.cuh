@@ -50,6 +50,7 @@ struct Job {
     long long word0;      // first word of this launch within the batch
     int iters;
     int quirk;            // 1: OMS first-iteration no-clip on second-group rows
+    int early;            // 1: syndrome early stop per word (LDPC_FLAG_EARLY_STOP)
     int32_t* iters_out;   // [words] or null
     int8_t* app_out;      // state dumps (reference device layouts) or null
     int8_t* msg_out;
@@ -63,7 +64,19 @@ struct Job {
     long long n_cw;
     unsigned long long* counts;  // [3] frames, bit errors, frame errors (or null)
     int n_vars;           // bits counted per frame
+    // KIND_LEARNED: magnitude tables [lut_its][2 row groups][128] (see packs.cuh)
+    const uint16_t* lut;
+    int lut_its;
 };
+
+// KIND_LEARNED: loads the tables of iteration `it` into shared memory (256 entries);
+// called by every thread at the top of an iteration, ends with a barrier
+__device__ __forceinline__ void load_iteration_lut(const Job& J, int it, uint16_t* slut)
+{
+    const int t = it < J.lut_its ? it : J.lut_its - 1;
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) slut[i] = J.lut[t * 256 + i];
+    __syncthreads();
+}
 
 // ---- prologue / epilogue: frame-major global <-> packed shared memory ----
 
@@ -320,11 +333,27 @@ template <> struct Access<PackI8> {
     }
 };
 
+// ---- syndrome early stop ----
+// true in some thread when a check has odd hard-decision parity (x > 0 is bit 1)
+// in one of the CTA's frames; rows are spread over the CTA's threads
+template <class PK>
+__device__ __forceinline__ bool rows_unsatisfied(const typename PK::S* app, const Plan& P)
+{
+    bool bad = false;
+    for (int r = threadIdx.x; r < P.m; r += blockDim.x) {
+        const int d = __ldg(P.rowdeg + r);
+        uint32_t acc = 0;
+        for (int j = 0; j < d; j++) acc ^= __vcmpgts4(Access<PK>::get(app, P.npad, __ldg(P.cols + j * P.m + r)), 0u);
+        bad |= acc != 0;
+    }
+    return bad;
+}
+
 // ---- one check row over all storage words of the group ----
 
 template <class PK, int KIND, int DT, bool EXACT>
 __device__ __forceinline__ void row_update(typename PK::S* app, typename PK::S* msg, const Plan& P,
-                                           int r, int d, bool noclip, typename PK::R& ov)
+                                           int r, int d, bool noclip, typename PK::R& ov, const uint16_t* lut)
 {
     using R = typename PK::R;
     int v[DT];
@@ -344,7 +373,7 @@ __device__ __forceinline__ void row_update(typename PK::S* app, typename PK::S* 
                 mm[j] = PK::ld_msg(M + j * P.m + r);
             }
         }
-        PK::template update<KIND, DT, EXACT>(x, mm, d, noclip, ov);
+        PK::template update<KIND, DT, EXACT>(x, mm, d, noclip, ov, lut);
 #pragma unroll
         for (int j = 0; j < DT; j++) {
             if (EXACT || j < d) {
@@ -363,6 +392,7 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* app = reinterpret_cast<S*>(smem_raw);
     S* msg = app + PK::WPC * P.npad;
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + PK::WPC * sizeof(S) * ((size_t)P.npad + (size_t)P.dmax * P.m));
     const long long g = J.word0 + blockIdx.x;
 
     read_group(P, J, g, [&](int v, uint32_t w) { Access<PK>::put(app, P.npad, v, w); });
@@ -377,18 +407,25 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
     for (int it = 0; it < J.iters; it++) {
         R ov = 0;
         const bool first = (it == 0);
+        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
         for (int l = 0; l < P.nlevels; l++) {
             const int2 lv = __ldg(P.levels + l);
             for (int r = lv.x + threadIdx.x; r < lv.x + lv.y; r += blockDim.x) {
                 const int d = EXACT ? DT : __ldg(P.rowdeg + r);
-                const bool noclip = J.quirk && first && __ldg(P.rowcls + r);
-                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov);
+                const int cls = __ldg(P.rowcls + r);
+                const bool noclip = J.quirk && first && cls;
+                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov, slut + 128 * cls);
             }
             __syncthreads();
         }
         executed = it + 1;
         if (KIND == KIND_2NMS && it >= 1) {
             if (!__syncthreads_or(ov != 0)) break;
+        }
+        // syndrome early stop: only after an iteration whose extrinsic parities were
+        // all even (free: the row update computes them) is the syndrome evaluated
+        if (KIND != KIND_2NMS && J.early) {
+            if (!__syncthreads_or(ov != 0) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) break;
         }
     }
 
@@ -419,6 +456,7 @@ __global__ void __launch_bounds__(256) decode_levels_half_kernel(const Plan P, c
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* app = reinterpret_cast<uint32_t*>(smem_raw);
     uint32_t* msg = app + P.npad;
+    uint16_t* slut = reinterpret_cast<uint16_t*>(msg + (size_t)P.dmax * P.m);
     const long long g = J.word0 + (blockIdx.x >> 1);
     const int h = blockIdx.x & 1;
 
@@ -429,12 +467,14 @@ __global__ void __launch_bounds__(256) decode_levels_half_kernel(const Plan P, c
     uint32_t ov = 0;
     for (int it = 0; it < J.iters; it++) {
         const bool first = (it == 0);
+        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
         for (int l = 0; l < P.nlevels; l++) {
             const int2 lv = __ldg(P.levels + l);
             for (int r = lv.x + threadIdx.x; r < lv.x + lv.y; r += blockDim.x) {
                 const int d = EXACT ? DT : __ldg(P.rowdeg + r);
-                const bool noclip = J.quirk && first && __ldg(P.rowcls + r);
-                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov);
+                const int cls = __ldg(P.rowcls + r);
+                const bool noclip = J.quirk && first && cls;
+                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov, slut + 128 * cls);
             }
             __syncthreads();
         }

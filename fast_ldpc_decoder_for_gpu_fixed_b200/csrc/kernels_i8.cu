@@ -7,11 +7,12 @@ namespace ldpc {
 #define LDPC_ENTRY(PK, KIND, D, EX) (const void*)decode_levels_kernel<PK, KIND, D, EX>,
 #define LDPC_ROW(KIND) {LDPC_DEGREE_VARIANTS(LDPC_ENTRY, PackI8, KIND)},
 
-// [kind: MS, OMS, NMS, 2NMS][variant: exact 6, exact 7, <=8, <=16, <=32]
+// [kind: MS, OMS, NMS, 2NMS, LEARNED][variant: exact 6, exact 7, <=8, <=16, <=32]
 const void* kernel_table_i8(int kind, int variant)
 {
-    static const void* table[4][5] = {LDPC_ROW(KIND_MS) LDPC_ROW(KIND_OMS) LDPC_ROW(KIND_NMS) LDPC_ROW(KIND_2NMS)};
-    if (kind < 0 || kind > 3 || variant < 0 || variant > 4) return nullptr;
+    static const void* table[5][5] = {LDPC_ROW(KIND_MS) LDPC_ROW(KIND_OMS) LDPC_ROW(KIND_NMS) LDPC_ROW(KIND_2NMS)
+                                      LDPC_ROW(KIND_LEARNED)};
+    if (kind < 0 || kind > 4 || variant < 0 || variant > 4) return nullptr;
     return table[kind][variant];
 }
 

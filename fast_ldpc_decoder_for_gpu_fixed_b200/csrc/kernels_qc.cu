@@ -9,7 +9,7 @@ namespace ldpc {
         return (const void*)decode_qc_kernel<KIND, D, EX, L, P2>;
 #define LDPC_QC_KINDS(D, EX, L, P2) \
     LDPC_QC(KIND_MS, D, EX, L, P2) LDPC_QC(KIND_OMS, D, EX, L, P2) \
-    LDPC_QC(KIND_NMS, D, EX, L, P2) LDPC_QC(KIND_2NMS, D, EX, L, P2)
+    LDPC_QC(KIND_NMS, D, EX, L, P2) LDPC_QC(KIND_2NMS, D, EX, L, P2) LDPC_QC(KIND_LEARNED, D, EX, L, P2)
 
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2)
 {

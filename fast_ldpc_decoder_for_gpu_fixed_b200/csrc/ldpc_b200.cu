@@ -71,6 +71,7 @@ struct ldpc_code {
 
 struct ldpc_decoder {
     int kind = 0, pack = 0, device = 0;
+    bool early = false;  // LDPC_FLAG_EARLY_STOP
     size_t nb_words = 0;
     int n = 0, m = 0, e = 0;
     Plan plan{};
@@ -87,7 +88,18 @@ struct ldpc_decoder {
     int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA
     int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
+    uint16_t* d_lut = nullptr;  // LDPC_LEARNED magnitude tables [its][2][128]
+    int lut_its = 0;
 };
+
+// Row schedule and CTA width of a decoder, for the training kernels (train.cu).
+int ldpc_internal_plan(const ldpc_decoder* d, Plan* plan, int* threads)
+{
+    if (!d || !d->d_cols) return -1;
+    *plan = d->plan;
+    *threads = std::min(256, std::max(32, (d->threads + 31) / 32 * 32));
+    return 0;
+}
 
 // ------------------------------------------------------------------------
 // codes
@@ -316,7 +328,7 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
         dt = std::max(dt, d);
     }
     bool pow2 = (c->z & (c->z - 1)) == 0;
-    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;
+    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
     return kernel_table_qc(k, dt, exact, c->mb, pow2);
 }
 
@@ -336,7 +348,8 @@ static int degree_variant(const ldpc_code* c)
 
 static const void* kernel_for(int pack, int kind, int variant)
 {
-    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // xMS = OMS arithmetic without the first-iteration quirk
+    // xMS = OMS arithmetic without the first-iteration quirk; LEARNED is row 4 of the tables
+    int k = (kind == LDPC_XMS) ? LDPC_OMS : (kind == LDPC_LEARNED ? 4 : kind);
     switch (pack) {
     case LDPC_PACK_SIMD4: return kernel_table_simd4(k, variant);
     case LDPC_PACK_F16X2: return kernel_table_f16x2(k, variant);
@@ -366,6 +379,7 @@ static void decoder_free(ldpc_decoder* d)
     cudaFree(d->d_edge_orig);
     cudaFree(d->d_in);
     cudaFree(d->d_out);
+    cudaFree(d->d_lut);
     if (d->s_comp) cudaStreamDestroy(d->s_comp);
     if (d->s_h2d) cudaStreamDestroy(d->s_h2d);
     if (d->s_d2h) cudaStreamDestroy(d->s_d2h);
@@ -415,29 +429,35 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
                                    int flags)
 {
     if (!out || !c) return fail(LDPC_ERR_ARG, "ldpc_decoder_create: null pointer");
-    if (kind < LDPC_MS || kind > LDPC_XMS) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
+    if (kind < LDPC_MS || kind > LDPC_LEARNED) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
     if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
-    if (flags != 0) return fail(LDPC_ERR_ARG, "flags must be 0");
+    if (flags & ~LDPC_FLAG_EARLY_STOP) return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
+    const bool early = flags & LDPC_FLAG_EARLY_STOP;
+    if (early && kind == LDPC_2NMS)
+        return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     const int pack_req = pack;
     if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
     if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
     if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
     int npad = (c->n + 15) / 16 * 16;
     // fp16x2 without early termination: 2 frames per CTA (half the shared memory)
-    const bool half = pack == LDPC_PACK_F16X2 && kind != LDPC_2NMS;
+    const bool half = pack == LDPC_PACK_F16X2 && kind != LDPC_2NMS && !early;
     size_t smem = half ? 4 * ((size_t)npad + (size_t)c->dmax * c->m) : smem_bytes(pack, npad, c->dmax, c->m);
+    const size_t lut_smem = kind == LDPC_LEARNED ? 512 : 0;  // the iteration's magnitude tables
+    smem += lut_smem;
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     QCParams probe;
     bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
-    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && qc_smem(c) <= (size_t)smem_max;
+    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && qc_smem(c) + 512 <= (size_t)smem_max;
     if (smem > (size_t)smem_max && !qc_ok)
         return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
                     smem, smem_max);
     ldpc_decoder* d = new ldpc_decoder();
     d->kind = kind;
+    d->early = early;
     d->pack = pack;
     d->device = dev;
     d->nb_words = nb_frames;
@@ -450,14 +470,14 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return rc;
     }
     const void* qk = (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2) ? qc_kernel_for(c, kind, d->qcp) : nullptr;
-    if (qk && qc_smem(c) <= (size_t)smem_max) {
+    if (qk && qc_smem(c) + lut_smem <= (size_t)smem_max) {
         d->kfn = qk;
         d->path = 1;
         d->pack = LDPC_PACK_F16X2;
-        d->smem = (int)qc_smem(c);
+        d->smem = (int)(qc_smem(c) + lut_smem);
         d->threads = c->z;
     } else if (half) {
-        d->kfn = kernel_table_f16x2h(kind == LDPC_XMS ? LDPC_OMS : kind, degree_variant(c));
+        d->kfn = kernel_table_f16x2h(kind == LDPC_XMS ? LDPC_OMS : (kind == LDPC_LEARNED ? 3 : kind), degree_variant(c));
         d->path = 2;
         d->grid_mult = 2;
         d->smem = (int)smem;
@@ -492,6 +512,36 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     return LDPC_OK;
 }
 
+extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8_t* offsets, const uint8_t* scales)
+{
+    if (!d || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: null pointer");
+    if (d->kind != LDPC_LEARNED) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: decoder kind is not LDPC_LEARNED");
+    if (n_iters < 1 || n_iters > LDPC_LEARNED_MAX_ITERS)
+        return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: n_iters must be in [1, %d]", LDPC_LEARNED_MAX_ITERS);
+    const bool fp16 = d->pack == LDPC_PACK_F16X2;
+    std::vector<uint16_t> lut((size_t)n_iters * 256);
+    for (int t = 0; t < n_iters; t++)
+        for (int g = 0; g < 2; g++)
+            for (int m = 0; m < 128; m++) {
+                int c = ((m * (int)scales[2 * t + g]) >> 7) - offsets[2 * t + g];
+                c = c < 0 ? 0 : (c > 31 ? 31 : c);
+                // fp16 bit pattern of the integer c (exact), or the plain integer
+                uint16_t v = (uint16_t)c;
+                if (fp16) {
+                    if (c == 0) v = 0;
+                    else {
+                        int e = 31 - __builtin_clz((unsigned)c);  // c < 32
+                        v = (uint16_t)(((e + 15) << 10) | ((c << (10 - e)) & 0x3ff));
+                    }
+                }
+                lut[(size_t)t * 256 + g * 128 + m] = v;
+            }
+    if (!d->d_lut) CUDA_TRY(cudaMalloc(&d->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
+    CUDA_TRY(cudaMemcpy(d->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    d->lut_its = n_iters;
+    return LDPC_OK;
+}
+
 extern "C" int ldpc_decoder_info(const ldpc_decoder* d, int* info)
 {
     if (!d || !info) return fail(LDPC_ERR_ARG, "ldpc_decoder_info: null pointer");
@@ -521,6 +571,11 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
 {
     Job J{};
     if (sim) J = *sim;
+    if (d->kind == LDPC_LEARNED) {
+        if (!d->d_lut) return fail(LDPC_ERR_ARG, "LDPC_LEARNED decoder: set its offsets and scales first");
+        J.lut = d->d_lut;
+        J.lut_its = d->lut_its;
+    }
     J.llr = llr;
     J.out = out;
     J.out_packed = out_packed;
@@ -529,6 +584,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.word0 = word0;
     J.iters = iters;
     J.quirk = d->kind == LDPC_OMS;
+    J.early = d->early ? 1 : 0;
     J.iters_out = iters_out;
     J.app_out = app_out;
     J.msg_out = msg_out;

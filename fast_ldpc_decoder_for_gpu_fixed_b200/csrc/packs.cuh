@@ -35,7 +35,13 @@
 
 namespace ldpc {
 
-enum { KIND_MS = 0, KIND_OMS = 1, KIND_NMS = 2, KIND_2NMS = 3, KIND_XMS = 4 };
+enum { KIND_MS = 0, KIND_OMS = 1, KIND_NMS = 2, KIND_2NMS = 3, KIND_XMS = 4, KIND_LEARNED = 5 };
+
+// KIND_LEARNED (no reference counterpart): the magnitude of a check's outgoing
+// messages is lut[min] from a 128-entry table of the current iteration and row
+// group, c = clamp(floor(min * scale_q7 / 128) - offset, 0, 31), built on the
+// host from the trained int8 offsets and Q1.7 scales.  The table holds plain
+// integers for PackSIMD4 / PackI8 and fp16 bit patterns for PackF16x2.
 
 // ------------------------------------------------------------------------
 // 4 frames per word, per-byte saturating SIMD
@@ -51,10 +57,19 @@ struct PackSIMD4 {
     __device__ __forceinline__ static void st_app(S* p, R v) { *p = v; }
     __device__ __forceinline__ static void st_msg(S* p, R v) { *p = v; }
 
-    template <int KIND>
-    __device__ __forceinline__ static void mags(R mn1, R mn2, bool noclip, R& c1, R& c2)
+    __device__ __forceinline__ static R lut4(R m, const uint16_t* lut)
     {
-        if (KIND == KIND_MS) {
+        return (R)lut[m & 0xff] | ((R)lut[(m >> 8) & 0xff] << 8) | ((R)lut[(m >> 16) & 0xff] << 16) |
+               ((R)lut[m >> 24] << 24);
+    }
+
+    template <int KIND>
+    __device__ __forceinline__ static void mags(R mn1, R mn2, bool noclip, R& c1, R& c2, const uint16_t* lut)
+    {
+        if (KIND == KIND_LEARNED) {
+            c1 = lut4(mn2, lut);
+            c2 = lut4(mn1, lut);
+        } else if (KIND == KIND_MS) {
             c1 = __vminu4(mn2, 0x1f1f1f1fu);
             c2 = __vminu4(mn1, 0x1f1f1f1fu);
         } else if (KIND == KIND_OMS) {
@@ -76,7 +91,8 @@ struct PackSIMD4 {
 
     // x[j]: APP in / APP out; m[j]: message in / out (all 4 byte lanes)
     template <int KIND, int DT, bool EXACT>
-    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov,
+                                                  const uint16_t* lut)
     {
         R mn1 = 0x7f7f7f7fu, mn2 = 0x7f7f7f7fu, s = 0;
 #pragma unroll
@@ -91,7 +107,7 @@ struct PackSIMD4 {
             }
         }
         R c1, c2;
-        mags<KIND>(mn1, mn2, noclip, c1, c2);
+        mags<KIND>(mn1, mn2, noclip, c1, c2, lut);
 #pragma unroll
         for (int j = 0; j < DT; j++) {
             if (EXACT || j < d) {
@@ -181,11 +197,22 @@ __device__ __forceinline__ uint32_t floor_scale(uint32_t m, uint32_t k, uint32_t
     return add(add(fma_relu(m, k, bias), C1024), CNEG1024);
 }
 
+// table lookup of both lanes: a + 1024 puts the integer a in the low 10 mantissa bits
+__device__ __forceinline__ uint32_t lut2(uint32_t a, const uint16_t* lut)
+{
+    const uint32_t i = add(a, C1024);
+    return (uint32_t)lut[i & 0x3ff] | ((uint32_t)lut[(i >> 16) & 0x3ff] << 16);
+}
+
 // row magnitudes from |min1| (a1) and |min2| (a2)
 template <int KIND>
-__device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2)
+__device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2,
+                                     const uint16_t* lut)
 {
-    if (KIND == KIND_MS) {
+    if (KIND == KIND_LEARNED) {
+        c1 = lut2(a2, lut);
+        c2 = lut2(a1, lut);
+    } else if (KIND == KIND_MS) {
         c1 = hmin(a2, C31);
         c2 = hmin(a1, C31);
     } else if (KIND == KIND_OMS) {
@@ -203,7 +230,8 @@ __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint
 
 // one row over one pair-word: b[j] biased APP in/out, m[j] negated message in/out
 template <int KIND, int DT, bool EXACT>
-__device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov)
+__device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov,
+                                    const uint16_t* lut)
 {
     uint32_t ut[DT];
     uint32_t mn1 = C127, mn2 = C127;
@@ -220,7 +248,7 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
     }
     const uint32_t a1 = mn1 & MAG, a2 = mn2 & MAG;
     uint32_t c1, c2;
-    mags<KIND>(a1, a2, noclip, c1, c2);
+    mags<KIND>(a1, a2, noclip, c1, c2, lut);
     const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
     const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
 #pragma unroll
@@ -251,9 +279,10 @@ struct PackF16x2 {
     __device__ __forceinline__ static void st_msg(S* p, R v) { *p = v; }
 
     template <int KIND, int DT, bool EXACT>
-    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov,
+                                                  const uint16_t* lut)
     {
-        h2::row<KIND, DT, EXACT>(x, m, d, noclip, ov);
+        h2::row<KIND, DT, EXACT>(x, m, d, noclip, ov, lut);
     }
 };
 
@@ -280,9 +309,12 @@ struct PackI8 {
     __device__ __forceinline__ static void st_msg(S* p, R v) { *p = (S)v; }
 
     template <int KIND>
-    __device__ __forceinline__ static void mags(int mn1, int mn2, bool noclip, int& c1, int& c2)
+    __device__ __forceinline__ static void mags(int mn1, int mn2, bool noclip, int& c1, int& c2, const uint16_t* lut)
     {
-        if (KIND == KIND_MS) {
+        if (KIND == KIND_LEARNED) {
+            c1 = lut[mn2];
+            c2 = lut[mn1];
+        } else if (KIND == KIND_MS) {
             c1 = min(mn2, 31);
             c2 = min(mn1, 31);
         } else if (KIND == KIND_OMS) {
@@ -300,7 +332,8 @@ struct PackI8 {
 
     // x[j]: APP (as x) in/out; m[j]: message stored negated (u = -msg) in/out
     template <int KIND, int DT, bool EXACT>
-    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov)
+    __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov,
+                                                  const uint16_t* lut)
     {
         int mn1 = 127, mn2 = 127, s = 0;
 #pragma unroll
@@ -315,7 +348,7 @@ struct PackI8 {
             }
         }
         int c1, c2;
-        mags<KIND>(mn1, mn2, noclip, c1, c2);
+        mags<KIND>(mn1, mn2, noclip, c1, c2, lut);
         const int sm = s >> 31;  // all ones when the parity of "x > 0" edges is odd
         c1 = (c1 ^ sm) - sm;
         c2 = (c2 ^ sm) - sm;

@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* app = reinterpret_cast<uint2*>(smem_raw);  // [n] (pair-word 0, pair-word 1)
     char* appb = reinterpret_cast<char*>(smem_raw);
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + (size_t)Q.n * 8);  // KIND_LEARNED
     const long long g = J.word0 + blockIdx.x;
     const int k = threadIdx.x;
 
@@ -71,6 +72,7 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
     int executed = 0;
     for (int it = 0; it < J.iters; it++) {
         uint32_t ov = 0;
+        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
 #pragma unroll
         for (int l = 0; l < L; l++) {
             const int d = EXACT ? DT : Q.deg[l];
@@ -91,8 +93,9 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
                     b1[j] = v.y;
                 }
             }
-            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov);
-            h2::row<KIND, DT, EXACT>(b1, msg[1][l], d, noclip, ov);
+            const uint16_t* lut = slut + 128 * Q.cls[l];
+            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov, lut);
+            h2::row<KIND, DT, EXACT>(b1, msg[1][l], d, noclip, ov, lut);
 #pragma unroll
             for (int j = 0; j < DT; j++)
                 if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
@@ -101,6 +104,31 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
         executed = it + 1;
         if (KIND == KIND_2NMS && it >= 1) {
             if (!__syncthreads_or(ov != 0)) break;
+        }
+        // syndrome early stop (see decode_levels_kernel): thread k checks row k of
+        // every layer.  For a biased APP b (x = 127 - b, an fp16 in [0, 255]),
+        // ((b | 0x8000) - 0x57f0) has bit 15 set iff b >= 127.0, i.e. iff the
+        // hard decision is 0; a row is satisfied when its count of 1s is even.
+        if (KIND != KIND_2NMS && J.early) {
+            if (!__syncthreads_or(ov != 0)) {
+                bool bad = false;
+                int kk = 8 * k;
+#pragma unroll
+                for (int l = 0; l < L; l++) {
+                    const int d = EXACT ? DT : Q.deg[l];
+                    uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+#pragma unroll
+                    for (int j = 0; j < DT; j++) {
+                        if (EXACT || j < d) {
+                            const uint2 v = *reinterpret_cast<const uint2*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk));
+                            acc0 ^= ((v.x | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
+                            acc1 ^= ((v.y | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
+                        }
+                    }
+                    bad |= (acc0 | acc1) != 0;
+                }
+                if (!__syncthreads_or(bad)) break;
+            }
         }
     }
 

@@ -73,10 +73,11 @@ def _ptr(x):
 
 
 class Decoder:
-    """One ldpc_decoder: ``kind`` in MS/OMS/NMS/2NMS/XMS, ``nb_frames`` 32-bit lanes
-    (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8."""
+    """One ldpc_decoder: ``kind`` in MS/OMS/NMS/2NMS/XMS/LEARNED, ``nb_frames`` 32-bit
+    lanes (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8;
+    ``early_stop`` sets LDPC_FLAG_EARLY_STOP (syndrome early stop per word)."""
 
-    def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO"):
+    def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO", early_stop=False):
         if isinstance(code, str):
             code = load_table(code)
         self.code = code if isinstance(code, Code) else code.code
@@ -86,14 +87,21 @@ class Decoder:
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().ldpc_decoder_create(
             ctypes.byref(h), self.native.handle, _lib.KINDS[self.kind], self.nb_frames,
-            _lib.PACKS[pack.upper()], 0))
+            _lib.PACKS[pack.upper()], _lib.FLAG_EARLY_STOP if early_stop else 0))
         self.handle = h
+        self.early_stop = bool(early_stop)
 
     def info(self):
         a = (ctypes.c_int * 8)()
         _lib.check(_lib.lib().ldpc_decoder_info(self.handle, a))
         keys = ("kind", "pack", "nb_frames", "threads", "smem", "ctas_per_sm", "regs", "path")
         return dict(zip(keys, list(a)))
+
+    def set_learned(self, offsets, scales):
+        """LDPC_LEARNED constants: [n_iters][2] int8 offsets and uint8 Q1.7 scales."""
+        off = np.ascontiguousarray(offsets, dtype=np.int8).reshape(-1, 2)
+        sc = np.ascontiguousarray(scales, dtype=np.uint8).reshape(-1, 2)
+        _lib.check(_lib.lib().ldpc_decoder_set_learned(self.handle, off.shape[0], off.ctypes.data, sc.ctypes.data))
 
     def decode_host(self, llr, hard, iters):
         """Synchronous host-buffer decode of all 4*nb_frames codewords (numpy arrays)."""
@@ -126,6 +134,21 @@ class Decoder:
         _lib.check(_lib.lib().ldpc_simulate(self.handle, int(n_words), int(iters), float(sigma), int(seed),
                                             int(offset), _ptr(d_codewords), int(n_codewords), int(nv),
                                             _ptr(d_counts), _ptr(d_hard), st))
+
+    def train_stash_bytes(self, frames, iters):
+        """Device bytes of the stash ``train_step`` needs for a backward pass."""
+        return int(_lib.lib().ldpc_train_stash_bytes(self.handle, int(frames), int(iters)))
+
+    def train_step(self, d_llr, d_kappa, frames, iters, d_alpha, d_beta, d_loss, d_bits=None, quantized=False,
+                   d_grad_alpha=None, d_grad_beta=None, d_stash=None, d_app=None, d_weights=None, stream=None):
+        """FP32 forward (and, with gradient buffers and a stash, backward) pass of the
+        learned min-sum decoder over ``frames`` frames (device buffers; see
+        ldpc_train_step in include/ldpc_b200.h)."""
+        st = getattr(stream, "cuda_stream", stream)
+        _lib.check(_lib.lib().ldpc_train_step(
+            self.handle, _ptr(d_llr), _ptr(d_bits), _ptr(d_kappa), int(frames), int(iters), int(bool(quantized)),
+            _ptr(d_alpha), _ptr(d_beta), _ptr(d_weights), _ptr(d_grad_alpha), _ptr(d_grad_beta), _ptr(d_loss),
+            _ptr(d_stash), _ptr(d_app), st))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -1,0 +1,207 @@
+"""Learned min-sum: training of the LDPC_LEARNED constants on the GPU, their
+quantisation, and FER/BER evaluation against plain OMS.
+
+The reference (src/decoder_oms/CUDA_OMS_SIMD.cu:73-74) uses one fixed offset
+(1) for every iteration.  LDPC_LEARNED replaces it by an offset and a scale per
+iteration and per row group, c = clamp(floor(min * scale / 128) - offset, 0, 31).
+They are trained here in FP32 by the project's own forward and backward kernels
+(ldpc_train_step, csrc/train.cu) through the unrolled layered decoder, on frames
+that the AWGN channel kernel (ldpc_channel_awgn) generates at Eb/N0 drawn
+uniformly from a range.  The loss is the BCE of the final soft output.
+Training runs in two phases: the real-valued relaxation, then
+quantisation-aware steps whose forward pass is exactly the int8 decoder
+(floored scale, integer offset), with straight-through gradients.
+Finally the constants are frozen to int8 offsets and Q1.7 scales.
+
+PyTorch only holds the buffers and applies Adam to the 4*T parameters; every
+decoder pass is one of this library's kernels.
+"""
+import numpy as np
+
+from . import _lib
+from .codes import Encoder, IRAEncoder
+from .decoder import Decoder
+
+
+def sigma_for(ebn0, rate):
+    """Noise deviation of the channel at Eb/N0 (dB) and code rate (ldpc_sigma)."""
+    return float(_lib.lib().ldpc_sigma(float(ebn0), float(rate), 0))
+
+
+def random_codewords(code, count, seed):
+    """``count`` codewords of random information bits (seeded), frame-major uint8."""
+    rng = np.random.default_rng(seed)
+    enc = IRAEncoder(code) if getattr(code, "ira_k", None) else Encoder(code)
+    return enc.encode(rng.integers(0, 2, size=(count, enc.k)))
+
+
+def quantize(alpha, beta):
+    """FP32 scales/offsets [T][2] -> (int8 offsets, uint8 Q1.7 scales)."""
+    alpha = np.asarray(alpha, dtype=np.float64)
+    beta = np.asarray(beta, dtype=np.float64)
+    off = np.clip(np.rint(beta), -128, 127).astype(np.int8)
+    sc = np.clip(np.rint(alpha * 128.0), 0, 255).astype(np.uint8)
+    return off, sc
+
+
+class Trainer:
+    """Trains per-iteration, per-row-group scales and offsets for ``code``.
+
+    Each step draws ``batch`` frames: ``batch // sub`` channel calls of ``sub``
+    frames, each at its own Eb/N0 ~ U[ebn0], over ``n_codewords`` seeded random
+    codewords (``sub`` must be a multiple of ``n_codewords``).  ``iters`` is the
+    number of unrolled decoder iterations (at most 32).
+    """
+
+    def __init__(self, code, iters=10, batch=4096, sub=512, ebn0=(1.0, 3.0), lr=0.03, seed=1,
+                 n_codewords=256, init_alpha=1.0, init_beta=1.0, weights="last", device="cuda"):
+        import torch
+        if sub % n_codewords or batch % sub:
+            raise ValueError("batch must be a multiple of sub, and sub a multiple of n_codewords")
+        self.torch = torch
+        self.code = code
+        self.T = int(iters)
+        self.batch = int(batch)
+        self.sub = int(sub)
+        self.ebn0 = tuple(ebn0)
+        self.rate = code.n_info / code.n
+        self.seed = int(seed)
+        self.rng = np.random.default_rng(seed)
+        self.dec = Decoder(code, "OMS", nb_frames=1)   # supplies the code's row schedule
+        dev = torch.device(device)
+        cw = random_codewords(code, n_codewords, seed + 7)
+        self.d_cw = torch.from_numpy(cw).to(dev)
+        self.n_cw = n_codewords
+        self.d_bits = self.d_cw.repeat(batch // n_codewords, 1).contiguous()
+        self.d_llr8 = torch.zeros(batch, code.n, dtype=torch.int8, device=dev)
+        self.d_llr = torch.zeros(batch, code.n, dtype=torch.float32, device=dev)
+        self.d_kappa = torch.zeros(batch, dtype=torch.float32, device=dev)
+        self.d_stash = torch.empty(self.dec.train_stash_bytes(batch, self.T), dtype=torch.uint8, device=dev)
+        self.d_loss = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.alpha = torch.full((self.T, 2), float(init_alpha), dtype=torch.float32, device=dev, requires_grad=True)
+        self.beta = torch.full((self.T, 2), float(init_beta), dtype=torch.float32, device=dev, requires_grad=True)
+        self.alpha.grad = torch.zeros_like(self.alpha)
+        self.beta.grad = torch.zeros_like(self.beta)
+        self.opt = torch.optim.Adam([self.alpha, self.beta], lr=lr)
+        # loss weight per iteration: "last" (the final soft output only) or "all"
+        # (every iteration's soft output, which rewards early convergence)
+        if isinstance(weights, str):
+            w = np.zeros(self.T, dtype=np.float32)
+            if weights == "last":
+                w[-1] = 1.0
+            elif weights == "all":
+                w[:] = 1.0 / self.T
+            else:
+                raise ValueError("weights: 'last', 'all' or an array of %d floats" % self.T)
+        else:
+            w = np.asarray(weights, dtype=np.float32).reshape(self.T)
+        self.d_weights = torch.from_numpy(w).to(dev)
+        self.calls = 0
+        self.history = []
+
+    def _frames(self):
+        """Fills the LLR batch from the channel kernel; kappa = 2/sigma^2 / 8 per frame."""
+        for j in range(self.batch // self.sub):
+            e = float(self.rng.uniform(*self.ebn0))
+            s = sigma_for(e, self.rate)
+            _lib.check(_lib.lib().ldpc_channel_awgn(
+                self.d_llr8[j * self.sub:(j + 1) * self.sub].data_ptr(), self.sub, self.code.n, s,
+                self.seed, self.calls, self.d_cw.data_ptr(), self.n_cw,
+                self.torch.cuda.current_stream().cuda_stream))
+            self.calls += 1
+            self.d_kappa[j * self.sub:(j + 1) * self.sub] = 1.0 / (4.0 * s * s)
+        self.d_llr.copy_(self.d_llr8)
+
+    def _used(self, quantized):
+        if not quantized:
+            return self.alpha.detach(), self.beta.detach()
+        return (self.torch.round(self.alpha.detach() * 128.0) / 128.0).contiguous(), \
+            self.torch.round(self.beta.detach()).contiguous()
+
+    def step(self, quantized=False):
+        """One training step; returns the loss as a device tensor (no sync)."""
+        self._frames()
+        a, b = self._used(quantized)
+        self.alpha.grad.zero_()
+        self.beta.grad.zero_()
+        self.d_loss.zero_()
+        self.dec.train_step(self.d_llr, self.d_kappa, self.batch, self.T, a, b, self.d_loss,
+                            d_bits=self.d_bits, quantized=quantized, d_grad_alpha=self.alpha.grad,
+                            d_grad_beta=self.beta.grad, d_stash=self.d_stash, d_weights=self.d_weights,
+                            stream=self.torch.cuda.current_stream())
+        self.opt.step()
+        with self.torch.no_grad():
+            self.alpha.clamp_(0.0, 255.0 / 128.0)
+            self.beta.clamp_(-8.0, 31.0)
+        return self.d_loss.clone()
+
+    def train(self, frames, qat_fraction=0.3, log_every=16):
+        """Trains on ``frames`` frames in total; the last ``qat_fraction`` of the
+        steps run the quantized forward pass.  Returns the loss history."""
+        steps = max(1, int(frames) // self.batch)
+        q0 = int(round(steps * (1.0 - qat_fraction)))
+        pending = []
+        for i in range(steps):
+            pending.append((i, self.step(quantized=i >= q0)))
+            if len(pending) >= log_every or i == steps - 1:
+                for k, l in pending:
+                    self.history.append((k, float(l.item())))
+                pending = []
+        return self.history
+
+    def validation_loss(self, ebn0, quantized=True, seed=99):
+        """Loss of the current constants on one fixed batch at ``ebn0`` dB
+        (forward pass only; comparable across calls)."""
+        s = sigma_for(ebn0, self.rate)
+        _lib.check(_lib.lib().ldpc_channel_awgn(self.d_llr8.data_ptr(), self.batch, self.code.n, s, seed, 0,
+                                                self.d_cw.data_ptr(), self.n_cw,
+                                                self.torch.cuda.current_stream().cuda_stream))
+        self.d_llr.copy_(self.d_llr8)
+        self.d_kappa.fill_(1.0 / (4.0 * s * s))
+        a, b = self._used(quantized)
+        self.d_loss.zero_()
+        self.dec.train_step(self.d_llr, self.d_kappa, self.batch, self.T, a, b, self.d_loss, d_bits=self.d_bits,
+                            quantized=quantized, d_weights=self.d_weights, stream=self.torch.cuda.current_stream())
+        return float(self.d_loss.item())
+
+    def constants(self):
+        """The frozen (int8 offsets, uint8 Q1.7 scales), [T][2] each."""
+        return quantize(self.alpha.detach().cpu().numpy(), self.beta.detach().cpu().numpy())
+
+    def close(self):
+        self.dec.close()
+
+
+def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewords=256, words_per_call=4096,
+             pack="AUTO", early_stop=False):
+    """Frame and bit error rates and mean iterations of the int8 decoder ``kind``
+    (with LDPC_LEARNED ``constants`` = (offsets, scales)) at ``ebn0`` dB over at
+    least ``frames`` frames of seeded random codewords: channel kernel, decode
+    with per-word iteration counts, error-count kernel.  Errors are counted over
+    all n bits.  Returns dict(frames, bit_errors, frame_errors, fer, ber, mean_iters)."""
+    import torch
+    words = min(words_per_call, max(1, (frames + 3) // 4))
+    dec = Decoder(code, kind, nb_frames=words, pack=pack, early_stop=early_stop)
+    if constants is not None:
+        dec.set_learned(*constants)
+    cw = torch.from_numpy(random_codewords(code, n_codewords, seed + 3)).cuda()
+    llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
+    hard = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    its = torch.zeros(words, dtype=torch.int32, device="cuda")
+    it_sum = torch.zeros(1, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(3, dtype=torch.int64, device="cuda")
+    s = sigma_for(ebn0, code.n_info / code.n)
+    st = torch.cuda.current_stream()
+    calls = (frames + 4 * words - 1) // (4 * words)
+    for c in range(calls):
+        _lib.check(_lib.lib().ldpc_channel_awgn(llr.data_ptr(), 4 * words, code.n, s, seed, c, cw.data_ptr(),
+                                                n_codewords, st.cuda_stream))
+        dec.decode_device(llr, hard, words, iters, d_iters=its, stream=st)
+        _lib.check(_lib.lib().ldpc_count_errors(hard.data_ptr(), 4 * words, code.n, code.n, cw.data_ptr(),
+                                                n_codewords, counts.data_ptr(), st.cuda_stream))
+        it_sum += its.sum()
+    torch.cuda.synchronize()
+    dec.close()
+    f, be, fe = (int(x) for x in counts.cpu().tolist())
+    return {"frames": f, "bit_errors": be, "frame_errors": fe, "fer": fe / f, "ber": be / (f * code.n),
+            "mean_iters": float(it_sum.item()) / (calls * words)}

@@ -51,6 +51,9 @@ extern "C" {
 #define LDPC_NMS 2  /* -NMS       : CGPU_Decoder_NMS_SIMD (x0.75)                 */
 #define LDPC_2NMS 3 /* -2NMS      : CGPU_Decoder_2NMS_SIMD (x0.75/x0.875, early term.) */
 #define LDPC_XMS 4  /* -xMS       : CGPU_Decoder_MS_SIMD_v2 (input already word-interleaved) */
+#define LDPC_LEARNED 5 /* learned offset/scale min-sum (no reference counterpart), see
+                          ldpc_decoder_set_learned */
+#define LDPC_LEARNED_MAX_ITERS 32
 
 /* frame packing of the on-chip decoder state */
 #define LDPC_PACK_AUTO (-1)
@@ -101,11 +104,20 @@ void ldpc_code_destroy(ldpc_code* code);
 
 /* ---- decoders ---------------------------------------------------------- */
 
+/* Syndrome early stop (no reference counterpart; not for LDPC_2NMS, which keeps
+ * the reference's own rule): a 4-frame word stops after an iteration in which
+ * every row's extrinsic sign parity was even for its 4 frames (the quantity
+ * 2NMS tests, CUDA_2NMS_SIMD.cu) and the hard decisions (x > 0 is bit 1) of all
+ * 4 frames then satisfy every check.  `iters` becomes the maximum; the
+ * iterations run are reported per word through d_iters_out. */
+#define LDPC_FLAG_EARLY_STOP 1
+
 /* nb_frames counts 32-bit lanes like the reference's constructor argument:
  * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
  * Unlike the reference (decoder_oms/CGPU_Decoder_OMS_SIMD.cu:101-105), any
  * nb_frames >= 1 is accepted.  The decoder owns its device buffers; the code
- * may be destroyed after this call.  pack = LDPC_PACK_*; flags = 0. */
+ * may be destroyed after this call.  pack = LDPC_PACK_*; flags = 0 or
+ * LDPC_FLAG_EARLY_STOP. */
 int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* code, int kind, size_t nb_frames,
                         int pack, int flags);
 
@@ -158,6 +170,38 @@ int ldpc_simulate(ldpc_decoder* dec, size_t n_words, int iters, float sigma, uin
  * race; issue them on one stream or synchronise between them. */
 int ldpc_decode_noalloc(const ldpc_code* code, int kind, int pack, const int8_t* d_llr,
                         uint8_t* d_hard, size_t n_words, int iters, void* stream);
+
+/* Constants of an LDPC_LEARNED decoder (no reference counterpart): for iteration
+ * t < n_iters and row group g (the reference's DEG_1 / DEG_2 groups), offsets[2t+g]
+ * (int8) and scales[2t+g] (Q1.7, 128 = 1.0) give the check-to-variable magnitude
+ * clamp(floor(min * scale / 128) - offset, 0, 31); iterations past n_iters reuse
+ * the last row.  scale 128 / offset 1 everywhere is OMS without its first-iteration
+ * quirk.  Trained by fast_ldpc_decoder_for_gpu_fixed_b200/learned.py. */
+int ldpc_decoder_set_learned(ldpc_decoder* dec, int n_iters, const int8_t* offsets,
+                             const uint8_t* scales);
+
+/* Training of the LDPC_LEARNED constants (no reference counterpart): one FP32
+ * forward pass of `iters` unrolled layered min-sum iterations over `frames`
+ * frames (d_llr: frames*n floats in the int8 decoder's LLR units, frame-major),
+ * with per-iteration, per-row-group real-valued alpha[2t+g] (scale) and
+ * beta[2t+g] (offset): magnitude clamp(alpha*min - beta, 0, 31), or
+ * clamp(floor(alpha*min) - beta, 0, 31) when `quantized` (with integer LLRs,
+ * alpha = s/128 and integer beta that is exactly the int8 LDPC_LEARNED decoder).
+ * d_loss[0] += sum over iterations t of d_weights[t] * (mean BCE of
+ * sigmoid(d_kappa[f] * APP after iteration t) against d_bits) (d_bits: frames*n
+ * 0/1 bytes, or null = all-zero codeword; d_weights: `iters` floats, or null =
+ * the last iteration only).  When d_grad_alpha, d_grad_beta and d_stash
+ * (ldpc_train_stash_bytes) are given, the backward pass adds d loss / d alpha
+ * and d loss / d beta (straight-through for min, sign, the saturations and the
+ * floor) into them.  d_app_out (frames*n floats, optional) receives the final
+ * APP.  The decoder supplies the code and its row schedule (any kind); the
+ * kernel runs on `stream`. */
+int ldpc_train_step(const ldpc_decoder* dec, const float* d_llr, const uint8_t* d_bits,
+                    const float* d_kappa, size_t frames, int iters, int quantized,
+                    const float* d_alpha, const float* d_beta, const float* d_weights,
+                    float* d_grad_alpha, float* d_grad_beta, float* d_loss, void* d_stash,
+                    float* d_app_out, void* stream);
+size_t ldpc_train_stash_bytes(const ldpc_decoder* dec, size_t frames, int iters);
 
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level

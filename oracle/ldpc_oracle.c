@@ -53,6 +53,34 @@
 #define K_NMS 2
 #define K_2NMS 3
 #define K_XMS 4
+#define K_LEARNED 5
+
+/* Learned min-sum (no reference counterpart): per iteration t and row group g an
+ * int8 offset beta and a Q1.7 scale q; c = clamp(floor(min * q / 128) - beta, 0, 31).
+ * scale 128 and offset 1 give OMS.  Iterations past the table reuse its last row. */
+#define LEARNED_MAX_IT 64
+static int g_learned_its = 0;
+static int8_t g_learned_off[LEARNED_MAX_IT][2];
+static uint8_t g_learned_scale[LEARNED_MAX_IT][2];
+
+int oracle_set_learned(int n_iters, const int8_t* offsets, const uint8_t* scales)
+{
+    if (n_iters < 1 || n_iters > LEARNED_MAX_IT) return -1;
+    g_learned_its = n_iters;
+    for (int t = 0; t < n_iters; t++)
+        for (int g = 0; g < 2; g++) {
+            g_learned_off[t][g] = offsets[2 * t + g];
+            g_learned_scale[t][g] = scales[2 * t + g];
+        }
+    return 0;
+}
+
+static inline int learned_mag(int it, int cls, int m)
+{
+    int t = it < g_learned_its ? it : g_learned_its - 1;
+    int c = ((m * (int)g_learned_scale[t][cls]) >> 7) - g_learned_off[t][cls];
+    return c < 0 ? 0 : (c > 31 ? 31 : c);
+}
 
 /* ---- per-byte semantics (simd_functions.h:89-130) ---------------------- */
 
@@ -96,6 +124,10 @@ static inline void check_mags(int kind, int it, int row_class, int min1, int min
         *c1 = (int8_t)((float)(int8_t)min2 * 0.875f);
         *c2 = (int8_t)((float)(int8_t)min1 * 0.750f);
         break;
+    case K_LEARNED:
+        *c1 = learned_mag(it, row_class, min2);
+        *c2 = learned_mag(it, row_class, min1);
+        break;
     }
 }
 
@@ -104,9 +136,23 @@ static inline void check_mags(int kind, int it, int row_class, int min1, int min
  * decision).  app: [4][n] int8 in/out; msg: [4][e] int8 scratch/out.
  * Returns the number of iterations executed.
  */
+/* 1 when the hard decisions (x > 0) of all 4 frames satisfy every check */
+static int word_syndrome_zero(int n, int m, const int32_t* row_ptr, const int32_t* cols, const int8_t* app)
+{
+    for (int lane = 0; lane < 4; lane++) {
+        const int8_t* A = app + (size_t)lane * n;
+        for (int r = 0; r < m; r++) {
+            int p = 0;
+            for (int k = row_ptr[r]; k < row_ptr[r + 1]; k++) p ^= (A[cols[k]] > 0);
+            if (p) return 0;
+        }
+    }
+    return 1;
+}
+
 static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                        const uint8_t* row_class, int kind, int iters,
-                       int8_t* app, int8_t* msg)
+                       int8_t* app, int8_t* msg, int early)
 {
     int e_total = row_ptr[m];
     int et = (kind == K_2NMS);
@@ -148,6 +194,10 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
         }
         executed = it + 1;
         if (et && it >= 1 && ov_sign == 0) break;
+        /* syndrome early stop (LDPC_FLAG_EARLY_STOP, no reference counterpart): after
+         * an iteration in which every row's extrinsic parity was even for all 4
+         * frames, stop if the hard decisions of all 4 frames form codewords */
+        if (early && ov_sign == 0 && word_syndrome_zero(n, m, row_ptr, cols, app)) break;
     }
     free(tv);
     return executed;
@@ -165,10 +215,10 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
  *             word[e*W+g] (d_MSG_C_2_V), e*nframes bytes.
  *   iters_out : optional, [W] iterations executed per word.
  */
-int oracle_decode(int n, int m, const int32_t* row_ptr, const int32_t* cols,
-                  const uint8_t* row_class, int kind, int iters, int nframes,
-                  int interleaved, const int8_t* llr, uint8_t* hard,
-                  int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads)
+int oracle_decode_ex(int n, int m, const int32_t* row_ptr, const int32_t* cols,
+                     const uint8_t* row_class, int kind, int iters, int nframes,
+                     int interleaved, const int8_t* llr, uint8_t* hard,
+                     int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads, int early)
 {
     if (nframes % 4 || iters < 1 || n <= 0 || m <= 0) return -1;
     int W = nframes / 4;
@@ -185,7 +235,7 @@ int oracle_decode(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                     ? llr[((size_t)v * W + g) * 4 + lane]
                     : llr[(size_t)f * n + v];
         }
-        int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg);
+        int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg, early);
         if (iters_out) iters_out[g] = ex;
         for (int lane = 0; lane < 4; lane++) {
             int f = 4 * g + lane;
@@ -202,6 +252,15 @@ int oracle_decode(int n, int m, const int32_t* row_ptr, const int32_t* cols,
         free(msg);
     }
     return 0;
+}
+
+int oracle_decode(int n, int m, const int32_t* row_ptr, const int32_t* cols,
+                  const uint8_t* row_class, int kind, int iters, int nframes,
+                  int interleaved, const int8_t* llr, uint8_t* hard,
+                  int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads)
+{
+    return oracle_decode_ex(n, m, row_ptr, cols, row_class, kind, iters, nframes, interleaved, llr, hard,
+                            app_out, msg_out, iters_out, nthreads, 0);
 }
 
 /* ---- layout restatements (transpose/GPU_Transpose_uint8.cu) ------------- */

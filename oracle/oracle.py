@@ -16,7 +16,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
 SOURCES = [os.path.join(HERE, "ldpc_oracle.c"), os.path.join(HERE, "ldpc_oracle_batch.c")]
 
-KINDS = {"MS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4}
+KINDS = {"MS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 5}
 
 _lib = None
 
@@ -40,6 +40,8 @@ def lib():
         i = ctypes.c_int
         L.oracle_decode.argtypes = [i, i, P, P, P, i, i, i, i, P, P, P, P, P, i]
         L.oracle_decode.restype = i
+        L.oracle_decode_ex.argtypes = [i, i, P, P, P, i, i, i, i, P, P, P, P, P, i, i]
+        L.oracle_decode_ex.restype = i
         L.oracle_decode_batch.argtypes = [i, i, P, P, P, i, i, i, i, P, P, i]
         L.oracle_decode_batch.restype = i
         L.oracle_batch_supported.restype = i
@@ -52,6 +54,8 @@ def lib():
         L.oracle_quantize.restype = i
         L.oracle_sigma.argtypes = [ctypes.c_double, ctypes.c_double, i]
         L.oracle_sigma.restype = ctypes.c_double
+        L.oracle_set_learned.argtypes = [i, P, P]
+        L.oracle_set_learned.restype = i
         L.oracle_philox.argtypes = [P, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
         L.oracle_awgn.argtypes = [P, P, ctypes.c_size_t, i, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, P,
                                   ctypes.c_size_t]
@@ -63,12 +67,13 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
-def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None):
+def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False):
     """Decodes ``llr`` (int8, nframes*n bytes, frame-major unless interleaved).
 
     Returns dict with ``hard`` [nframes, n] uint8, ``iters`` [nframes/4] and,
     if ``want_state``, ``app`` / ``msg`` in the reference's word-interleaved
-    device layouts (n*nframes and e*nframes bytes).
+    device layouts (n*nframes and e*nframes bytes).  ``early_stop``: the
+    syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word).
     """
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
@@ -80,9 +85,9 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     app = np.zeros(code.n * nframes, dtype=np.int8) if want_state else None
     msg = np.zeros(code.e * nframes, dtype=np.int8) if want_state else None
     nt = nthreads or os.cpu_count() or 1
-    rc = lib().oracle_decode(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
-                             k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
-                             _p(app), _p(msg), _p(it), nt)
+    rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
+                                k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
+                                _p(app), _p(msg), _p(it), nt, int(bool(early_stop)))
     if rc != 0:
         raise ValueError("oracle_decode rejected the arguments")
     out = {"hard": hard, "iters": it}
@@ -159,3 +164,11 @@ def awgn(frames, n, sigma, seed, offset=0, codewords=None):
     lib().oracle_awgn(_p(out), _p(y8), frames, n, float(sigma), seed, offset, _p(cw),
                       0 if cw is None else cw.shape[0])
     return out.reshape(frames, n), y8.reshape(frames, n)
+
+
+def set_learned(offsets, scales):
+    """Per-iteration [n_iters][2] int8 offsets and uint8 Q1.7 scales of the LEARNED kind."""
+    off = np.ascontiguousarray(offsets, dtype=np.int8).reshape(-1, 2)
+    sc = np.ascontiguousarray(scales, dtype=np.uint8).reshape(-1, 2)
+    if lib().oracle_set_learned(off.shape[0], _p(off), _p(sc)) != 0:
+        raise ValueError("bad learned table")

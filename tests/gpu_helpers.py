@@ -19,14 +19,16 @@ def make_llr(kind, count, seed, sigma=None, value=0):
     return llr_gen.llr(kind, count, seed, sigma=sigma, value=value)
 
 
-def gpu_decode(code, kind, llr, iters, words, pack="AUTO", state=True):
+def gpu_decode(code, kind, llr, iters, words, pack="AUTO", state=True, early_stop=False, constants=None):
     """Decodes 4*words frames on cuda:0; returns hard [frames, n], app/msg (reference
     device layouts, bytes) and the per-word iteration counts."""
     import pytest
     import torch
     from fast_ldpc_decoder_for_gpu_fixed_b200 import LdpcError
     try:
-        dec = Decoder(code, kind, nb_frames=words, pack=pack)
+        dec = Decoder(code, kind, nb_frames=words, pack=pack, early_stop=early_stop)
+        if constants is not None:
+            dec.set_learned(*constants)
     except LdpcError as e:
         if e.code == -3:  # the code's state does not fit one CTA with this packing
             pytest.skip(str(e))
