@@ -16,6 +16,8 @@ KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 
 PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2}
 OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
+EARLY_STOP_DEFAULT_SLACK = 128
+TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2
 
 # every entry point declared in include/ldpc_b200.h: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -34,6 +36,7 @@ SIGNATURES = {
     "ldpc_decode_device_state": (_I, [_P, _P, _P, _SZ, _I, _P, _P, _P, _P]),
     "ldpc_decoder_info": (_I, [_P, _P]),
     "ldpc_decoder_set_learned": (_I, [_P, _I, _P, _P]),
+    "ldpc_decoder_set_early_stop": (_I, [_P, _I, _I]),
     "ldpc_decoder_destroy": (_I, [_P]),
     "ldpc_train_step": (_I, [_P, _P, _P, _P, _SZ, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ldpc_train_stash_bytes": (_SZ, [_P, _SZ, _I]),

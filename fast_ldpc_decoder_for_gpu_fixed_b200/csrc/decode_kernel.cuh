@@ -51,6 +51,7 @@ struct Job {
     int iters;
     int quirk;            // 1: OMS first-iteration no-clip on second-group rows
     int early;            // 1: syndrome early stop per word (LDPC_FLAG_EARLY_STOP)
+    unsigned early_slack;  // evaluate the syndrome when at most this many (row, frame) pairs were odd
     int32_t* iters_out;   // [words] or null
     int8_t* app_out;      // state dumps (reference device layouts) or null
     int8_t* msg_out;
@@ -334,6 +335,21 @@ template <> struct Access<PackI8> {
 };
 
 // ---- syndrome early stop ----
+// After iteration `it`, the word stops when at most J.early_slack (row, frame)
+// pairs had odd extrinsic sign parity during the iteration (each thread's `odd`
+// counts its own; the row updates compute the parities anyway) and the hard
+// decisions of its frames then satisfy every check.  The count goes through a
+// double-buffered shared counter, so one barrier serves both the sum and the
+// reset for the next iteration.  Uniform across the CTA.
+__device__ __forceinline__ bool odd_rows_within_slack(const Job& J, unsigned odd, int it, unsigned* s_odd)
+{
+    if (odd) atomicAdd(&s_odd[it & 1], odd);
+    __syncthreads();
+    const unsigned total = s_odd[it & 1];
+    if (threadIdx.x == 0) s_odd[(it + 1) & 1] = 0;
+    return total <= J.early_slack;
+}
+
 // true in some thread when a check has odd hard-decision parity (x > 0 is bit 1)
 // in one of the CTA's frames; rows are spread over the CTA's threads
 template <class PK>
@@ -394,6 +410,8 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
     S* msg = app + PK::WPC * P.npad;
     uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + PK::WPC * sizeof(S) * ((size_t)P.npad + (size_t)P.dmax * P.m));
     const long long g = J.word0 + blockIdx.x;
+    __shared__ unsigned s_odd[2];
+    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
 
     read_group(P, J, g, [&](int v, uint32_t w) { Access<PK>::put(app, P.npad, v, w); });
     {
@@ -422,10 +440,8 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
         if (KIND == KIND_2NMS && it >= 1) {
             if (!__syncthreads_or(ov != 0)) break;
         }
-        // syndrome early stop: only after an iteration whose extrinsic parities were
-        // all even (free: the row update computes them) is the syndrome evaluated
         if (KIND != KIND_2NMS && J.early) {
-            if (!__syncthreads_or(ov != 0) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) break;
+            if (odd_rows_within_slack(J, ov, it, s_odd) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) break;
         }
     }
 

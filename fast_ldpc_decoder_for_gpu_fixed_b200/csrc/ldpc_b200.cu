@@ -72,6 +72,7 @@ struct ldpc_code {
 struct ldpc_decoder {
     int kind = 0, pack = 0, device = 0;
     bool early = false;  // LDPC_FLAG_EARLY_STOP
+    unsigned early_slack = LDPC_EARLY_STOP_DEFAULT_SLACK;
     size_t nb_words = 0;
     int n = 0, m = 0, e = 0;
     Plan plan{};
@@ -512,6 +513,19 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     return LDPC_OK;
 }
 
+extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int slack)
+{
+    if (!d) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: null decoder");
+    if (enabled && d->kind == LDPC_2NMS)
+        return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
+    if (enabled && d->path == 2)
+        return fail(LDPC_ERR_ARG, "early stop needs a decoder created with LDPC_FLAG_EARLY_STOP for this packing");
+    if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: slack must be >= 0");
+    d->early = enabled != 0;
+    d->early_slack = (unsigned)slack;
+    return LDPC_OK;
+}
+
 extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8_t* offsets, const uint8_t* scales)
 {
     if (!d || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: null pointer");
@@ -585,6 +599,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.iters = iters;
     J.quirk = d->kind == LDPC_OMS;
     J.early = d->early ? 1 : 0;
+    J.early_slack = d->early_slack;
     J.iters_out = iters_out;
     J.app_out = app_out;
     J.msg_out = msg_out;

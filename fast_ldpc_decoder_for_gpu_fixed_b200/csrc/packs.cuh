@@ -120,7 +120,7 @@ struct PackSIMD4 {
                 x[j] = __vaddss4(t, out);
             }
         }
-        ov |= s;
+        ov += __popc(s) >> 3;  // odd (row, frame) pairs: s is 0xff in each odd byte
     }
 };
 
@@ -263,7 +263,7 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
             b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)
         }
     }
-    ov |= mn1 & SIGN;
+    ov += __popc(mn1 & SIGN);  // odd (row, frame) pairs
 }
 }  // namespace h2
 
@@ -363,7 +363,7 @@ struct PackI8 {
                 x[j] = min(max(-(ut + um), -128), 127);
             }
         }
-        ov |= s & (int)0x80000000;
+        ov += (uint32_t)s >> 31;  // odd (row, frame) pairs
     }
 };
 

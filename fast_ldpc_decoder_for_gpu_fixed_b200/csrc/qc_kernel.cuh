@@ -44,8 +44,30 @@ __device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int k8)
     return Q.cz4[idx] + u;
 }
 
+template <int DT, bool EXACT, int L, bool POW2>
+__device__ __noinline__ bool qc_rows_unsatisfied(const QCParams& Q, const char* appb, int k)
+{
+    bool bad = false;
+    const int kk = 8 * k;
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+        const int d = EXACT ? DT : Q.deg[l];
+        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                const uint2 v = *reinterpret_cast<const uint2*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk));
+                acc0 ^= ((v.x | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
+                acc1 ^= ((v.y | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
+            }
+        }
+        bad |= (acc0 | acc1) != 0;
+    }
+    return bad;
+}
+
 template <int KIND, int DT, bool EXACT, int L, bool POW2>
-__global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, const Job J)
+__global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant__ QCParams Q, const Job J)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* app = reinterpret_cast<uint2*>(smem_raw);  // [n] (pair-word 0, pair-word 1)
@@ -53,6 +75,8 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
     uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + (size_t)Q.n * 8);  // KIND_LEARNED
     const long long g = J.word0 + blockIdx.x;
     const int k = threadIdx.x;
+    __shared__ unsigned s_odd[2];
+    if (k < 2) s_odd[k] = 0;
 
     Plan P;  // only n is used by the shared prologue / epilogue helpers
     P.n = Q.n;
@@ -105,28 +129,13 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const QCParams Q, con
         if (KIND == KIND_2NMS && it >= 1) {
             if (!__syncthreads_or(ov != 0)) break;
         }
-        // syndrome early stop (see decode_levels_kernel): thread k checks row k of
+        // syndrome early stop (odd_rows_within_slack): thread k checks row k of
         // every layer.  For a biased APP b (x = 127 - b, an fp16 in [0, 255]),
         // ((b | 0x8000) - 0x57f0) has bit 15 set iff b >= 127.0, i.e. iff the
         // hard decision is 0; a row is satisfied when its count of 1s is even.
         if (KIND != KIND_2NMS && J.early) {
-            if (!__syncthreads_or(ov != 0)) {
-                bool bad = false;
-                int kk = 8 * k;
-#pragma unroll
-                for (int l = 0; l < L; l++) {
-                    const int d = EXACT ? DT : Q.deg[l];
-                    uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
-#pragma unroll
-                    for (int j = 0; j < DT; j++) {
-                        if (EXACT || j < d) {
-                            const uint2 v = *reinterpret_cast<const uint2*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk));
-                            acc0 ^= ((v.x | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
-                            acc1 ^= ((v.y | 0x80008000u) - 0x57f057f0u) & 0x80008000u;
-                        }
-                    }
-                    bad |= (acc0 | acc1) != 0;
-                }
+            if (odd_rows_within_slack(J, ov, it, s_odd)) {
+                const bool bad = qc_rows_unsatisfied<DT, EXACT, L, POW2>(Q, appb, k);
                 if (!__syncthreads_or(bad)) break;
             }
         }

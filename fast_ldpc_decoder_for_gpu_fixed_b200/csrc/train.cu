@@ -14,21 +14,27 @@
 // a starts as the channel LLRs in the int8 decoders' units.  With integer LLRs,
 // alpha = s / 128 and integer beta, the quantized forward pass is exactly the
 // LDPC_LEARNED int8 decoder (offsets beta, Q1.7 scales s): every value is an
-// integer below 2^24, so FP32 holds it exactly.
-// Loss: sum over iterations t of w[t] * (mean over frames and variables of
-// BCE(sigmoid(kappa_f * a_v(t)), b_v)), a(t) the APP after iteration t, b the
-// transmitted bits (a positive LLR means bit 1) and kappa_f the frame's factor
-// from the decoder's LLR units to natural log-likelihood ratios; without
-// weights only the last iteration counts (w[T-1] = 1).
-// Every forward operation is one IEEE FP32 operation rounded to nearest (no
-// contraction into FMA), so a float32 emulation reproduces it bit for bit.
+// integer below 2^24, so FP32 holds it exactly.  Every forward operation is one
+// IEEE FP32 operation rounded to nearest (no contraction into FMA), so a float32
+// emulation reproduces the forward pass bit for bit.
+//
+// Loss, with w[t] the weight of iteration t (default: the last iteration only),
+// a(t) the APP after iteration t, b the transmitted bits (a positive LLR means
+// bit 1), kappa_f the frame's factor from the decoder's LLR units to natural
+// log-likelihood ratios and S_f(t) = sum_v BCE(sigmoid(kappa_f a_v(t)), b_v):
+//   bit loss   (LDPC_TRAIN_BIT_LOSS):   sum_t w[t] * mean_f S_f(t) / n
+//   frame loss (LDPC_TRAIN_FRAME_LOSS): sum_t w[t] * mean_f (1 - exp(-S_f(t)))
+// exp(-S_f) is the probability, under the soft output, that every bit of the
+// frame is right, so the frame loss is a soft frame error rate.
+//
 // Backward: the reverse row sequence (levels in reverse order, the rows of a
 // level in parallel, as in the forward pass).  Gradients are straight-through
 // for min and sign (the argmins and signs found in the forward pass are held
 // fixed), for the two saturations and for the floor; c's clamp passes the
-// gradient only where 0 < y < 31.  The forward pass records {min1, min2, i1 | i2 << 8,
-// sign bits} per row and iteration (16 bytes) and, for weighted iterations
-// before the last, the APP (4 bytes per variable) in a caller-provided stash.
+// gradient only where 0 < y < 31.  The forward pass records {min1, min2,
+// i1 | i2 << 8, sign bits} per row and iteration (16 bytes), and for weighted
+// iterations before the last the APP (4 bytes per variable) and S_f(t), in a
+// caller-provided stash.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -46,14 +52,17 @@ struct TrainArgs {
     float* grad_alpha;     // [T][2] accumulated
     float* grad_beta;      // [T][2] accumulated
     float* loss;           // [1] accumulated
-    uint4* stash;          // [frames][T][m], then the APPs [frames][T][n] floats
-    float* stash_app;
+    uint4* stash;          // [frames][T][m]
+    float* stash_app;      // [frames][T][n]
+    float* stash_s;        // [frames][T]
     const float* weights;  // [T] loss weight per iteration, or null (last only)
     float* app_out;        // [frames][n] final soft output, or null
     int T;
     int quantized;
+    int frame_loss;
     int backward;
-    float inv_count;       // 1 / (frames * n)
+    float inv_frames;      // 1 / frames
+    float inv_n;           // 1 / n
 };
 
 __device__ __forceinline__ float warp_sum(float x)
@@ -61,6 +70,18 @@ __device__ __forceinline__ float warp_sum(float x)
 #pragma unroll
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
+}
+
+// sum over the CTA (blockDim.x a multiple of 32, at most 256), returned to every thread
+__device__ __forceinline__ float block_sum(float x, float* scratch)
+{
+    x = warp_sum(x);
+    __syncthreads();  // scratch may still be read from a previous call
+    if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = x;
+    __syncthreads();
+    float s = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w];
+    return s;
 }
 
 __device__ __forceinline__ float pre_mag(float al, float be, float x, int quantized)
@@ -78,13 +99,24 @@ __device__ __forceinline__ float iter_weight(const TrainArgs& A, int t)
     return A.weights ? A.weights[t] : (t == A.T - 1 ? 1.f : 0.f);
 }
 
+// the loss term of iteration t for this frame from S = S_f(t), and the factor
+// that multiplies kappa * (sigmoid - b) in its gradient
+__device__ __forceinline__ float term_loss(const TrainArgs& A, float w, float S)
+{
+    return A.frame_loss ? w * (1.f - expf(-S)) * A.inv_frames : w * S * A.inv_n * A.inv_frames;
+}
+__device__ __forceinline__ float term_grad(const TrainArgs& A, float w, float S)
+{
+    return A.frame_loss ? w * expf(-S) * A.inv_frames : w * A.inv_n * A.inv_frames;
+}
+
 __global__ void __launch_bounds__(256) train_kernel(const Plan P, const TrainArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* a = reinterpret_cast<float*>(smem_raw);    // APP, then its gradient
     float* msg = a + P.npad;                          // messages [dmax][m], then their gradients
     __shared__ float gpar[4 * LDPC_LEARNED_MAX_ITERS];  // [t][g][d alpha, d beta]
-    __shared__ float lpart[8];
+    __shared__ float scratch[8];
     const long long f = blockIdx.x;
     const int T = A.T;
 
@@ -94,7 +126,8 @@ __global__ void __launch_bounds__(256) train_kernel(const Plan P, const TrainArg
     __syncthreads();
 
     const float kap = A.kappa[f];
-    float lsum = 0.f;
+    float floss = 0.f;  // this frame's loss (thread 0)
+    auto bit = [&](int v) { return A.bits ? (float)A.bits[f * P.n + v] : 0.f; };
 
     // ---------------- forward ----------------
     for (int t = 0; t < T; t++) {
@@ -136,35 +169,35 @@ __global__ void __launch_bounds__(256) train_kernel(const Plan P, const TrainArg
             }
             __syncthreads();
         }
-        // intermediate loss terms: their APPs are kept for the backward pass
+        // intermediate loss terms: their APPs and S_f(t) are kept for the backward pass
         const float w = iter_weight(A, t);
         if (t < T - 1 && w != 0.f) {
+            float part = 0.f;
             for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
-                const float b = A.bits ? (float)A.bits[f * P.n + v] : 0.f;
-                lsum += w * bce(kap * a[v], b);
+                part += bce(kap * a[v], bit(v));
                 if (A.backward) A.stash_app[((size_t)f * T + t) * P.n + v] = a[v];
             }
-            __syncthreads();  // the next iteration rewrites a
+            const float S = block_sum(part, scratch);  // also orders the reads of a before iteration t+1
+            floss += term_loss(A, w, S);
+            if (A.backward && threadIdx.x == 0) A.stash_s[(size_t)f * T + t] = S;
         }
     }
 
     // ---------------- final loss term and its gradient ----------------
-    const float wl = iter_weight(A, T - 1);
-    for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
-        const float z = kap * a[v];
-        const float b = A.bits ? (float)A.bits[f * P.n + v] : 0.f;
-        if (A.app_out) A.app_out[f * P.n + v] = a[v];
-        lsum += wl * bce(z, b);
-        a[v] = wl * kap * bce_grad(z, b) * A.inv_count;   // d loss / d a_v
-    }
-    for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) msg[i] = 0.f;
-    lsum = warp_sum(lsum);
-    if ((threadIdx.x & 31) == 0) lpart[threadIdx.x >> 5] = lsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float s = 0.f;
-        for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) s += lpart[w];
-        atomicAdd(A.loss, s * A.inv_count);
+    {
+        float part = 0.f;
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
+            if (A.app_out) A.app_out[f * P.n + v] = a[v];
+            part += bce(kap * a[v], bit(v));
+        }
+        const float w = iter_weight(A, T - 1);
+        const float S = block_sum(part, scratch);
+        floss += term_loss(A, w, S);
+        const float coef = term_grad(A, w, S);
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x) a[v] = coef * kap * bce_grad(kap * a[v], bit(v));
+        for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) msg[i] = 0.f;
+        if (threadIdx.x == 0) atomicAdd(A.loss, floss);
+        __syncthreads();
     }
     if (!A.backward) return;
 
@@ -174,10 +207,8 @@ __global__ void __launch_bounds__(256) train_kernel(const Plan P, const TrainArg
         const float w = iter_weight(A, t);
         if (t < T - 1 && w != 0.f) {  // the loss term on the APP after iteration t
             const float* keep = A.stash_app + ((size_t)f * T + t) * P.n;
-            for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
-                const float b = A.bits ? (float)A.bits[f * P.n + v] : 0.f;
-                a[v] += w * kap * bce_grad(kap * keep[v], b) * A.inv_count;
-            }
+            const float coef = term_grad(A, w, A.stash_s[(size_t)f * T + t]);
+            for (int v = threadIdx.x; v < P.n; v += blockDim.x) a[v] += coef * kap * bce_grad(kap * keep[v], bit(v));
             __syncthreads();
         }
         for (int l = P.nlevels - 1; l >= 0; l--) {
@@ -245,22 +276,27 @@ using namespace ldpc;
 int ldpc_internal_fail(int code, const char* msg);
 int ldpc_internal_plan(const ldpc_decoder* dec, Plan* plan, int* threads);
 
+static size_t stash_rows(const Plan& P, size_t frames, int iters) { return frames * (size_t)iters * P.m * sizeof(uint4); }
+static size_t stash_apps(const Plan& P, size_t frames, int iters) { return frames * (size_t)iters * P.n * sizeof(float); }
+
 extern "C" size_t ldpc_train_stash_bytes(const ldpc_decoder* dec, size_t frames, int iters)
 {
     Plan P;
     int threads = 0;
     if (!dec || iters < 1 || ldpc_internal_plan(dec, &P, &threads)) return 0;
-    return frames * (size_t)iters * ((size_t)P.m * sizeof(uint4) + (size_t)P.n * sizeof(float));
+    return stash_rows(P, frames, iters) + stash_apps(P, frames, iters) + frames * (size_t)iters * sizeof(float);
 }
 
 extern "C" int ldpc_train_step(const ldpc_decoder* dec, const float* d_llr, const uint8_t* d_bits,
-                               const float* d_kappa, size_t frames, int iters, int quantized,
+                               const float* d_kappa, size_t frames, int iters, int flags,
                                const float* d_alpha, const float* d_beta, const float* d_weights,
                                float* d_grad_alpha, float* d_grad_beta, float* d_loss, void* d_stash,
                                float* d_app_out, void* stream)
 {
     if (!dec || !d_llr || !d_kappa || !d_alpha || !d_beta || !d_loss)
         return ldpc_internal_fail(LDPC_ERR_ARG, "ldpc_train_step: null pointer");
+    if (flags & ~(LDPC_TRAIN_QUANTIZED | LDPC_TRAIN_FRAME_LOSS))
+        return ldpc_internal_fail(LDPC_ERR_ARG, "ldpc_train_step: unknown flags");
     const bool backward = d_grad_alpha || d_grad_beta || d_stash;
     if (backward && !(d_grad_alpha && d_grad_beta && d_stash))
         return ldpc_internal_fail(LDPC_ERR_ARG, "ldpc_train_step: gradients need grad_alpha, grad_beta and stash");
@@ -289,16 +325,19 @@ extern "C" int ldpc_train_step(const ldpc_decoder* dec, const float* d_llr, cons
     A.grad_alpha = d_grad_alpha;
     A.grad_beta = d_grad_beta;
     A.loss = d_loss;
-    A.stash = reinterpret_cast<uint4*>(d_stash);
-    A.stash_app = d_stash ? reinterpret_cast<float*>(reinterpret_cast<char*>(d_stash) +
-                                                     frames * (size_t)iters * P.m * sizeof(uint4))
-                          : nullptr;
+    char* sb = reinterpret_cast<char*>(d_stash);
+    A.stash = reinterpret_cast<uint4*>(sb);
+    A.stash_app = sb ? reinterpret_cast<float*>(sb + stash_rows(P, frames, iters)) : nullptr;
+    A.stash_s = sb ? reinterpret_cast<float*>(sb + stash_rows(P, frames, iters) + stash_apps(P, frames, iters))
+                   : nullptr;
     A.weights = d_weights;
     A.app_out = d_app_out;
     A.T = iters;
-    A.quantized = quantized ? 1 : 0;
+    A.quantized = (flags & LDPC_TRAIN_QUANTIZED) ? 1 : 0;
+    A.frame_loss = (flags & LDPC_TRAIN_FRAME_LOSS) ? 1 : 0;
     A.backward = backward ? 1 : 0;
-    A.inv_count = (float)(1.0 / ((double)frames * P.n));
+    A.inv_frames = (float)(1.0 / (double)frames);
+    A.inv_n = (float)(1.0 / (double)P.n);
     cudaError_t e = cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
         train_kernel<<<(unsigned)frames, threads, smem, (cudaStream_t)stream>>>(P, A);

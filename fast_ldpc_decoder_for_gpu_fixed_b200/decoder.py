@@ -90,12 +90,19 @@ class Decoder:
             _lib.PACKS[pack.upper()], _lib.FLAG_EARLY_STOP if early_stop else 0))
         self.handle = h
         self.early_stop = bool(early_stop)
+        self.early_slack = _lib.EARLY_STOP_DEFAULT_SLACK
 
     def info(self):
         a = (ctypes.c_int * 8)()
         _lib.check(_lib.lib().ldpc_decoder_info(self.handle, a))
         keys = ("kind", "pack", "nb_frames", "threads", "smem", "ctas_per_sm", "regs", "path")
         return dict(zip(keys, list(a)))
+
+    def set_early_stop(self, enabled=True, slack=_lib.EARLY_STOP_DEFAULT_SLACK):
+        """Syndrome early stop on/off and its slack (ldpc_decoder_set_early_stop)."""
+        _lib.check(_lib.lib().ldpc_decoder_set_early_stop(self.handle, int(bool(enabled)), int(slack)))
+        self.early_stop = bool(enabled)
+        self.early_slack = int(slack)
 
     def set_learned(self, offsets, scales):
         """LDPC_LEARNED constants: [n_iters][2] int8 offsets and uint8 Q1.7 scales."""
@@ -140,13 +147,15 @@ class Decoder:
         return int(_lib.lib().ldpc_train_stash_bytes(self.handle, int(frames), int(iters)))
 
     def train_step(self, d_llr, d_kappa, frames, iters, d_alpha, d_beta, d_loss, d_bits=None, quantized=False,
-                   d_grad_alpha=None, d_grad_beta=None, d_stash=None, d_app=None, d_weights=None, stream=None):
+                   d_grad_alpha=None, d_grad_beta=None, d_stash=None, d_app=None, d_weights=None,
+                   frame_loss=False, stream=None):
         """FP32 forward (and, with gradient buffers and a stash, backward) pass of the
         learned min-sum decoder over ``frames`` frames (device buffers; see
         ldpc_train_step in include/ldpc_b200.h)."""
         st = getattr(stream, "cuda_stream", stream)
+        flags = (_lib.TRAIN_QUANTIZED if quantized else 0) | (_lib.TRAIN_FRAME_LOSS if frame_loss else 0)
         _lib.check(_lib.lib().ldpc_train_step(
-            self.handle, _ptr(d_llr), _ptr(d_bits), _ptr(d_kappa), int(frames), int(iters), int(bool(quantized)),
+            self.handle, _ptr(d_llr), _ptr(d_bits), _ptr(d_kappa), int(frames), int(iters), flags,
             _ptr(d_alpha), _ptr(d_beta), _ptr(d_weights), _ptr(d_grad_alpha), _ptr(d_grad_beta), _ptr(d_loss),
             _ptr(d_stash), _ptr(d_app), st))
 

@@ -7,7 +7,9 @@ iteration and per row group, c = clamp(floor(min * scale / 128) - offset, 0, 31)
 They are trained here in FP32 by the project's own forward and backward kernels
 (ldpc_train_step, csrc/train.cu) through the unrolled layered decoder, on frames
 that the AWGN channel kernel (ldpc_channel_awgn) generates at Eb/N0 drawn
-uniformly from a range.  The loss is the BCE of the final soft output.
+uniformly from a range.  The loss is the BCE of the soft outputs ("bit") or a
+soft frame error rate ("frame": 1 - exp(-summed BCE) per frame), of the last
+iteration or of every iteration ("all", which rewards early convergence).
 Training runs in two phases: the real-valued relaxation, then
 quantisation-aware steps whose forward pass is exactly the int8 decoder
 (floored scale, integer offset), with straight-through gradients.
@@ -54,7 +56,7 @@ class Trainer:
     """
 
     def __init__(self, code, iters=10, batch=4096, sub=512, ebn0=(1.0, 3.0), lr=0.03, seed=1,
-                 n_codewords=256, init_alpha=1.0, init_beta=1.0, weights="last", device="cuda"):
+                 n_codewords=256, init_alpha=1.0, init_beta=1.0, weights="last", loss="bit", device="cuda"):
         import torch
         if sub % n_codewords or batch % sub:
             raise ValueError("batch must be a multiple of sub, and sub a multiple of n_codewords")
@@ -96,6 +98,9 @@ class Trainer:
         else:
             w = np.asarray(weights, dtype=np.float32).reshape(self.T)
         self.d_weights = torch.from_numpy(w).to(dev)
+        if loss not in ("bit", "frame"):
+            raise ValueError("loss: 'bit' (mean BCE) or 'frame' (soft frame error rate)")
+        self.frame_loss = loss == "frame"
         self.calls = 0
         self.history = []
 
@@ -128,7 +133,7 @@ class Trainer:
         self.dec.train_step(self.d_llr, self.d_kappa, self.batch, self.T, a, b, self.d_loss,
                             d_bits=self.d_bits, quantized=quantized, d_grad_alpha=self.alpha.grad,
                             d_grad_beta=self.beta.grad, d_stash=self.d_stash, d_weights=self.d_weights,
-                            stream=self.torch.cuda.current_stream())
+                            frame_loss=self.frame_loss, stream=self.torch.cuda.current_stream())
         self.opt.step()
         with self.torch.no_grad():
             self.alpha.clamp_(0.0, 255.0 / 128.0)
@@ -161,7 +166,8 @@ class Trainer:
         a, b = self._used(quantized)
         self.d_loss.zero_()
         self.dec.train_step(self.d_llr, self.d_kappa, self.batch, self.T, a, b, self.d_loss, d_bits=self.d_bits,
-                            quantized=quantized, d_weights=self.d_weights, stream=self.torch.cuda.current_stream())
+                            quantized=quantized, d_weights=self.d_weights, frame_loss=self.frame_loss,
+                            stream=self.torch.cuda.current_stream())
         return float(self.d_loss.item())
 
     def constants(self):

@@ -106,11 +106,14 @@ void ldpc_code_destroy(ldpc_code* code);
 
 /* Syndrome early stop (no reference counterpart; not for LDPC_2NMS, which keeps
  * the reference's own rule): a 4-frame word stops after an iteration in which
- * every row's extrinsic sign parity was even for its 4 frames (the quantity
- * 2NMS tests, CUDA_2NMS_SIMD.cu) and the hard decisions (x > 0 is bit 1) of all
- * 4 frames then satisfy every check.  `iters` becomes the maximum; the
- * iterations run are reported per word through d_iters_out. */
+ * at most `slack` (row, frame) pairs had odd extrinsic sign parity (the
+ * quantity 2NMS tests, CUDA_2NMS_SIMD.cu, counted over the word's 4 frames) and
+ * whose hard decisions (x > 0 is bit 1) of all 4 frames then satisfy every
+ * check.  The count only decides when the syndrome is evaluated: a word never
+ * stops on a non-codeword.  `iters` becomes the maximum; the iterations run
+ * are reported per word through d_iters_out. */
 #define LDPC_FLAG_EARLY_STOP 1
+#define LDPC_EARLY_STOP_DEFAULT_SLACK 128
 
 /* nb_frames counts 32-bit lanes like the reference's constructor argument:
  * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
@@ -184,24 +187,33 @@ int ldpc_decoder_set_learned(ldpc_decoder* dec, int n_iters, const int8_t* offse
  * forward pass of `iters` unrolled layered min-sum iterations over `frames`
  * frames (d_llr: frames*n floats in the int8 decoder's LLR units, frame-major),
  * with per-iteration, per-row-group real-valued alpha[2t+g] (scale) and
- * beta[2t+g] (offset): magnitude clamp(alpha*min - beta, 0, 31), or
- * clamp(floor(alpha*min) - beta, 0, 31) when `quantized` (with integer LLRs,
- * alpha = s/128 and integer beta that is exactly the int8 LDPC_LEARNED decoder).
- * d_loss[0] += sum over iterations t of d_weights[t] * (mean BCE of
- * sigmoid(d_kappa[f] * APP after iteration t) against d_bits) (d_bits: frames*n
- * 0/1 bytes, or null = all-zero codeword; d_weights: `iters` floats, or null =
- * the last iteration only).  When d_grad_alpha, d_grad_beta and d_stash
- * (ldpc_train_stash_bytes) are given, the backward pass adds d loss / d alpha
- * and d loss / d beta (straight-through for min, sign, the saturations and the
- * floor) into them.  d_app_out (frames*n floats, optional) receives the final
- * APP.  The decoder supplies the code and its row schedule (any kind); the
- * kernel runs on `stream`. */
+ * beta[2t+g] (offset): magnitude clamp(alpha*min - beta, 0, 31), or with
+ * LDPC_TRAIN_QUANTIZED clamp(floor(alpha*min) - beta, 0, 31) (with integer
+ * LLRs, alpha = s/128 and integer beta that is exactly the int8 LDPC_LEARNED
+ * decoder).  With S_f(t) the sum over the frame's bits of the BCE of
+ * sigmoid(d_kappa[f] * APP after iteration t) against d_bits (frames*n 0/1
+ * bytes, or null = all-zero codeword), d_loss[0] += sum_t d_weights[t] *
+ * mean_f S_f(t)/n, or with LDPC_TRAIN_FRAME_LOSS sum_t d_weights[t] *
+ * mean_f (1 - exp(-S_f(t))) (a soft frame error rate); d_weights: `iters`
+ * floats, or null = the last iteration only.  When d_grad_alpha, d_grad_beta
+ * and d_stash (ldpc_train_stash_bytes) are given, the backward pass adds
+ * d loss / d alpha and d loss / d beta (straight-through for min, sign, the
+ * saturations and the floor) into them.  d_app_out (frames*n floats, optional)
+ * receives the final APP.  The decoder supplies the code and its row schedule
+ * (any kind); the kernel runs on `stream`. */
+#define LDPC_TRAIN_QUANTIZED 1
+#define LDPC_TRAIN_FRAME_LOSS 2
 int ldpc_train_step(const ldpc_decoder* dec, const float* d_llr, const uint8_t* d_bits,
-                    const float* d_kappa, size_t frames, int iters, int quantized,
+                    const float* d_kappa, size_t frames, int iters, int flags,
                     const float* d_alpha, const float* d_beta, const float* d_weights,
                     float* d_grad_alpha, float* d_grad_beta, float* d_loss, void* d_stash,
                     float* d_app_out, void* stream);
 size_t ldpc_train_stash_bytes(const ldpc_decoder* dec, size_t frames, int iters);
+
+/* Turns the syndrome early stop on or off and sets its slack (default
+ * LDPC_EARLY_STOP_DEFAULT_SLACK).  Turning it on for a decoder created without
+ * LDPC_FLAG_EARLY_STOP fails for the 2-frames-per-CTA kernel (path 2). */
+int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
 
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level

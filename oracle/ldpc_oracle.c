@@ -163,6 +163,7 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
     int executed = 0;
     for (int it = 0; it < iters; it++) {
         int ov_sign = 0; /* OR over rows and lanes of the extrinsic sign parity */
+        int odd_rows = 0; /* (row, lane) pairs whose extrinsic sign parity was odd */
         for (int r = 0; r < m; r++) {
             int b = row_ptr[r], d = row_ptr[r + 1] - b;
             for (int lane = 0; lane < 4; lane++) {
@@ -190,14 +191,16 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
                     A[cols[b + j]] = (int8_t)sat8(t + out);
                 }
                 ov_sign |= sgn;
+                odd_rows += sgn;
             }
         }
         executed = it + 1;
         if (et && it >= 1 && ov_sign == 0) break;
-        /* syndrome early stop (LDPC_FLAG_EARLY_STOP, no reference counterpart): after
-         * an iteration in which every row's extrinsic parity was even for all 4
-         * frames, stop if the hard decisions of all 4 frames form codewords */
-        if (early && ov_sign == 0 && word_syndrome_zero(n, m, row_ptr, cols, app)) break;
+        /* syndrome early stop (LDPC_FLAG_EARLY_STOP, no reference counterpart;
+         * early = 1 + slack): after an iteration in which at most `slack` (row,
+         * lane) pairs had odd extrinsic parity, stop if the hard decisions of all
+         * 4 frames form codewords */
+        if (early && odd_rows <= early - 1 && word_syndrome_zero(n, m, row_ptr, cols, app)) break;
     }
     free(tv);
     return executed;

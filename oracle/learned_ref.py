@@ -10,7 +10,8 @@ per-row-group scale alpha and offset beta:
     c(x) = clamp(alpha * x - beta, 0, 31)         (quantized: floor(alpha * x) - beta)
 
 and the loss sum_t w[t] * mean BCE(sigmoid(kappa_f * APP after iteration t),
-transmitted bits) (no weights: the last iteration only).  The backward pass is
+transmitted bits) (no weights: the last iteration only), or the soft frame
+error rate sum_t w[t] * mean_f (1 - exp(-S_f(t))), S_f the frame's summed BCE.  The backward pass is
 the exact reverse of the row sequence, straight-through for min, sign, the
 saturations and the floor.  Rows are taken in table order; the GPU's level
 order gives the same result because rows of one level share no variable.
@@ -43,9 +44,11 @@ def _bce(z, b):
 
 
 def forward_backward(code, llr, bits, kappa, alpha, beta, quantized=False, backward=True, weights=None,
-                     forward_dtype=np.float64):
+                     forward_dtype=np.float64, frame_loss=False):
     """llr [F][n] (float), bits [F][n] 0/1 or None, kappa [F], alpha/beta [T][2],
-    weights [T] or None.  Returns (loss, app [F][n], d_alpha [T][2], d_beta [T][2])."""
+    weights [T] or None.  Returns (loss, app [F][n], d_alpha [T][2], d_beta [T][2]).
+    Loss per weighted iteration: mean_f S_f / n, or with ``frame_loss``
+    mean_f (1 - exp(-S_f)), S_f the frame's summed bit BCE."""
     ft = forward_dtype
     llr = np.asarray(llr, dtype=ft)
     F, n = llr.shape
@@ -62,7 +65,7 @@ def forward_backward(code, llr, bits, kappa, alpha, beta, quantized=False, backw
     ar = np.arange(F)
     a = llr.copy()
     msg = [np.zeros((F, len(c)), dtype=ft) for c, _ in rows]
-    stash, apps = [], []
+    stash, apps, S_all = [], [], []
     loss = 0.0
     for t in range(T):
         st_t = []
@@ -87,7 +90,11 @@ def forward_backward(code, llr, bits, kappa, alpha, beta, quantized=False, backw
         stash.append(st_t)
         apps.append(a.astype(np.float64))
         if w[t] != 0.0:
-            loss += w[t] * float(np.sum(_bce(kappa * apps[t], b)) / count)
+            S = np.sum(_bce(kappa * apps[t], b), axis=1)
+            S_all.append(S)
+            loss += w[t] * float(np.mean(1.0 - np.exp(-S)) if frame_loss else np.sum(S) / count)
+        else:
+            S_all.append(None)
     app = apps[-1].copy()
     if not backward:
         return loss, app, None, None
@@ -98,7 +105,8 @@ def forward_backward(code, llr, bits, kappa, alpha, beta, quantized=False, backw
     for t in range(T - 1, -1, -1):
         if w[t] != 0.0:
             z = kappa * apps[t]
-            ga += w[t] * kappa * (1.0 / (1.0 + np.exp(-z)) - b) / count
+            coef = np.exp(-S_all[t])[:, None] / F if frame_loss else 1.0 / count
+            ga += w[t] * coef * kappa * (1.0 / (1.0 + np.exp(-z)) - b)
         for r in range(len(rows) - 1, -1, -1):
             cols, g = rows[r]
             m1, m2, i1, i2, pos, par = stash[t][r]

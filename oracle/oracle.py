@@ -67,13 +67,15 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
-def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False):
+def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False,
+           early_slack=128):
     """Decodes ``llr`` (int8, nframes*n bytes, frame-major unless interleaved).
 
     Returns dict with ``hard`` [nframes, n] uint8, ``iters`` [nframes/4] and,
     if ``want_state``, ``app`` / ``msg`` in the reference's word-interleaved
     device layouts (n*nframes and e*nframes bytes).  ``early_stop``: the
-    syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word).
+    syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word) with
+    ``early_slack`` (ldpc_decoder_set_early_stop).
     """
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
@@ -87,7 +89,7 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     nt = nthreads or os.cpu_count() or 1
     rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
                                 k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
-                                _p(app), _p(msg), _p(it), nt, int(bool(early_stop)))
+                                _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0)
     if rc != 0:
         raise ValueError("oracle_decode rejected the arguments")
     out = {"hard": hard, "iters": it}

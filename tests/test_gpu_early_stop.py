@@ -50,6 +50,28 @@ def test_early_stop_qc_kernel(cuda):
         assert ref["iters"].min() < 10 and ref["iters"].max() == 20
 
 
+@pytest.mark.parametrize("slack", [0, 5, 1 << 20])
+def test_early_stop_slack(cuda, slack):
+    import torch
+    code = _qc()
+    words = 32
+    llr = np.concatenate([make_llr("awgn", 4 * 16 * code.n, 51 + i, sigma=llr_gen.sigma_for(e, 0.5))
+                          for i, e in enumerate((1.75, 2.5))])
+    ref = oracle.decode(code, "OMS", llr, 20, interleaved=False, want_state=True, early_stop=True,
+                        early_slack=slack)
+    for pack in ("AUTO", "SIMD4"):
+        dec = Decoder(code, "OMS", nb_frames=words, pack=pack, early_stop=True)
+        dec.set_early_stop(True, slack)
+        d_llr = torch.from_numpy(llr).cuda()
+        d_hard = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+        d_it = torch.zeros(words, dtype=torch.int32, device="cuda")
+        dec.decode_device(d_llr, d_hard, words, 20, d_iters=d_it)
+        torch.cuda.synchronize()
+        dec.close()
+        assert np.array_equal(d_it.cpu().numpy(), ref["iters"])
+        assert np.array_equal(d_hard.cpu().numpy().reshape(4 * words, code.n), ref["hard"])
+
+
 def test_early_stop_learned(cuda):
     code = _qc()
     words = 16

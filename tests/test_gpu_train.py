@@ -12,7 +12,8 @@ from fast_ldpc_decoder_for_gpu_fixed_b200.codes import qc_regular
 pytestmark = pytest.mark.gpu
 
 
-def _gpu_step(code, llr, bits, kappa, alpha, beta, quantized, backward=True, kind="OMS", weights=None):
+def _gpu_step(code, llr, bits, kappa, alpha, beta, quantized, backward=True, kind="OMS", weights=None,
+              frame_loss=False):
     import torch
     F = llr.shape[0]
     T = alpha.shape[0]
@@ -28,7 +29,7 @@ def _gpu_step(code, llr, bits, kappa, alpha, beta, quantized, backward=True, kin
     stash = torch.empty(dec.train_stash_bytes(F, T), dtype=torch.uint8, device="cuda") if backward else None
     d_w = d(weights, np.float32) if weights is not None else None
     dec.train_step(d_llr, d_kappa, F, T, d_a, d_b, loss, d_bits=d_bits, quantized=quantized, d_grad_alpha=ga,
-                   d_grad_beta=gb, d_stash=stash, d_app=app, d_weights=d_w)
+                   d_grad_beta=gb, d_stash=stash, d_app=app, d_weights=d_w, frame_loss=frame_loss)
     torch.cuda.synchronize()
     dec.close()
     out = [float(loss.item()), app.cpu().numpy()]
@@ -36,19 +37,22 @@ def _gpu_step(code, llr, bits, kappa, alpha, beta, quantized, backward=True, kin
     return out
 
 
-def _frames(code, F, sigma, seed):
+def _frames(code, F, sigma, seed, zero=False):
     rng = np.random.default_rng(seed)
     bits = rng.integers(0, 2, size=(F, code.n)).astype(np.uint8)
+    if zero:   # the all-zero codeword (frames that can decode)
+        bits[:] = 0
     y = (2.0 * bits - 1.0) + sigma * rng.standard_normal((F, code.n))
     return np.trunc(np.clip(8.0 * y, -31, 31)), bits, np.full(F, 1.0 / (4 * sigma * sigma))
 
 
-@pytest.mark.parametrize("name,weighted", [("576x288", False), ("1944x972", False), ("qc", False),
-                                           ("576x288", True), ("qc", True)])
-def test_train_step_matches_fp64_model(cuda, name, weighted):
+@pytest.mark.parametrize("name,weighted,frame", [("576x288", False, False), ("1944x972", False, False),
+                                                 ("qc", False, False), ("576x288", True, False), ("qc", True, False),
+                                                 ("576x288", True, True), ("qc", False, True)])
+def test_train_step_matches_fp64_model(cuda, name, weighted, frame):
     code = load_table(name) if name != "qc" else qc_regular(z=64, mb=8, nb=16, wc=3, seed=5)
     F, T = 12, 4
-    llr, bits, kappa = _frames(code, F, 0.9, 3)
+    llr, bits, kappa = _frames(code, F, 0.65 if frame else 0.9, 3, zero=frame)
     rng = np.random.default_rng(4)
     alpha = rng.uniform(0.6, 1.1, (T, 2)).astype(np.float32)
     beta = rng.uniform(-0.5, 1.5, (T, 2)).astype(np.float32)
@@ -56,11 +60,12 @@ def test_train_step_matches_fp64_model(cuda, name, weighted):
     # forward: the FP32 emulation (one rounding per operation) is bit-exact;
     # loss and gradients: FP64 from the same decisions
     l_ref, app_ref, ga_ref, gb_ref = learned_ref.forward_backward(code, llr, bits, kappa, alpha, beta, weights=w,
-                                                                  forward_dtype=np.float32)
-    l_gpu, app_gpu, ga, gb = _gpu_step(code, llr, bits, kappa, alpha, beta, False, weights=w)
+                                                                  forward_dtype=np.float32, frame_loss=frame)
+    l_gpu, app_gpu, ga, gb = _gpu_step(code, llr, bits, kappa, alpha, beta, False, weights=w, frame_loss=frame)
     assert np.array_equal(app_gpu.astype(np.float64), app_ref)
     assert l_gpu == pytest.approx(l_ref, rel=1e-5)
     scale = max(np.abs(ga_ref).max(), np.abs(gb_ref).max())
+    assert scale > 1e-4
     # tolerance: FP32 accumulation over frames x rows x iterations (atomics in any order)
     assert np.abs(ga - ga_ref).max() <= 5e-4 * scale
     assert np.abs(gb - gb_ref).max() <= 5e-4 * scale

@@ -15,22 +15,31 @@ def _llr(rng, frames, n, sigma):
     return np.trunc(np.clip(8.0 * y, -31, 31))
 
 
-@pytest.mark.parametrize("name,weighted", [("576x288", False), ("qc", False), ("576x288", True)])
-def test_gradients_match_finite_differences(name, weighted):
+@pytest.mark.parametrize("name,weighted,frame", [("576x288", False, False), ("qc", False, False),
+                                                 ("576x288", True, False), ("576x288", True, True),
+                                                 ("qc", False, True)])
+def test_gradients_match_finite_differences(name, weighted, frame):
     code = load_table(name) if name != "qc" else qc_regular(z=16, mb=8, nb=16, wc=3, seed=3)
     rng = np.random.default_rng(1)
-    F, T, sigma = 6, 3, 0.9
+    F, T = 6, 3
+    sigma = 0.65 if frame else 0.9   # the frame loss needs frames close to decoding
     llr = _llr(rng, F, code.n, sigma)
     bits = rng.integers(0, 2, size=(F, code.n))
-    llr = np.where(bits == 1, -llr, llr)   # codeword bits flip the BPSK sign
+    llr = np.where(bits == 1, -llr, llr)   # the transmitted bits flip the BPSK sign
+    if frame:   # the frame loss needs frames that can decode: send the all-zero codeword
+        bits[:] = 0
+        llr = _llr(np.random.default_rng(1), F, code.n, sigma)
     kappa = np.full(F, 1.0 / (4 * sigma * sigma))
     alpha = rng.uniform(0.6, 1.0, (T, 2))
     beta = rng.uniform(0.2, 1.5, (T, 2))
     w = np.array([0.25, 0.5, 1.0]) if weighted else None
-    loss, app, da, db = learned_ref.forward_backward(code, llr, bits, kappa, alpha, beta, weights=w)
+    loss, app, da, db = learned_ref.forward_backward(code, llr, bits, kappa, alpha, beta, weights=w,
+                                                     frame_loss=frame)
     assert np.abs(app).max() < 127          # no saturation: the model is smooth here
     eps = 1e-6
-    f = lambda a, b: learned_ref.forward_backward(code, llr, bits, kappa, a, b, backward=False, weights=w)[0]
+    f = lambda a, b: learned_ref.forward_backward(code, llr, bits, kappa, a, b, backward=False, weights=w,
+                                                  frame_loss=frame)[0]
+    assert np.abs(da).max() > 1e-3 and np.abs(db).max() > 1e-3
     used = sorted(set(code.row_class.tolist()))
     for t in range(T):
         for g in used:
