@@ -190,14 +190,23 @@ def qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name=None):
     return code
 
 
-def ira(n=64800, k=32400, group=360, frac_high=0.2, deg_high=8, deg_low=3, seed=2025, name=None):
+def ira(n=64800, k=32400, group=360, frac_high=0.2, deg_high=8, deg_low=3, seed=2025, name=None, layered=True):
     """Seeded IRA code (DVB-S2-like structure): information columns in groups of
     `group`; a fraction `frac_high` of the groups have degree `deg_high`, the rest
     `deg_low`; each group's first column draws its check rows uniformly from the
-    seed and the other columns of the group follow with a cyclic step of
-    (n - k) / group, as in DVB-S2.  The parity part is the dual-diagonal staircase
-    (parity j in checks j and j+1).  Defaults: N=64800, K=32400, 1/5 of the groups
-    of degree 8, the rest of degree 3 (check degree about 6)."""
+    seed (with distinct residues mod q when q allows) and the other columns of the
+    group follow with a cyclic step of q = (n - k) / group, as in DVB-S2.  The
+    parity part is the dual-diagonal staircase (parity j in checks j and j+1).
+    Defaults: N=64800, K=32400, 1/5 of the groups of degree 8, the rest of degree
+    3 (check degree about 6).
+
+    With `layered` the checks are listed in the order i + j*q (i = 0..q-1 outer,
+    j = 0..group-1 inner): the `group` checks of one i share no parity bit and,
+    because a group's base rows have distinct residues mod q, no information
+    bit, so the row-layered decoder runs each such layer in parallel.  In
+    natural order consecutive checks share a parity bit and the layered
+    schedule is fully serial.  The code is the same; ``code.ira_natural[r]`` is
+    the staircase index of row r."""
     m = n - k
     if k % group or m % group:
         raise ValueError("k and n-k must be multiples of the group size")
@@ -208,7 +217,12 @@ def ira(n=64800, k=32400, group=360, frac_high=0.2, deg_high=8, deg_low=3, seed=
     rows = [[] for _ in range(m)]
     for gi in range(ngroups):
         deg = deg_high if gi < n_high else deg_low
-        base = rng.choice(m, size=deg, replace=False)
+        # uniform rows with distinct residues mod q (when q allows): a column then
+        # meets each layer {i + j*q} at most once
+        if deg <= q:
+            base = rng.choice(q, size=deg, replace=False) + q * rng.integers(0, group, size=deg)
+        else:
+            base = rng.choice(m, size=deg, replace=False)
         for c in range(group):
             col = gi * group + c
             for b in base:
@@ -218,27 +232,41 @@ def ira(n=64800, k=32400, group=360, frac_high=0.2, deg_high=8, deg_low=3, seed=
         if j > 0:
             rows[j].append(k + j - 1)
     rows = [sorted(set(r)) for r in rows]
-    code = Code.from_rows(name or "ira%dx%d_s%d" % (n, m, seed), n, rows)
+    natural = np.arange(m)
+    if layered:
+        natural = (np.arange(q)[:, None] + q * np.arange(group)[None, :]).reshape(-1)
+        rows = [rows[j] for j in natural]
+    code = Code.from_rows(name or "ira%dx%d_s%d%s" % (n, m, seed, "" if layered else "_nat"), n, rows)
     code.ira_k = k
+    code.ira_natural = natural
     return code
 
 
 class IRAEncoder:
     """Linear-time systematic encoder of an `ira` code: p_j = p_{j-1} + (sum of the
-    information bits of check j), i.e. a cumulative XOR down the staircase."""
+    information bits of check j), i.e. a cumulative XOR down the staircase.  The
+    information part of H is kept sparse (one gather and one segmented XOR per
+    batch), so N = 64800 codes encode without a dense m x k matrix."""
 
     def __init__(self, code):
         self.n, self.k = code.n, code.ira_k
         m = code.m
-        h = np.zeros((m, self.k), dtype=np.uint8)
-        for r, cols in enumerate(code.rows()):
-            info = cols[cols < self.k]
-            h[r, info] ^= 1
-        self.hi = h.astype(np.float32)
+        natural = np.asarray(getattr(code, "ira_natural", np.arange(m)))
+        rp = np.asarray(code.row_ptr, dtype=np.int64)
+        cols = np.asarray(code.cols, dtype=np.int64)
+        nat_of_edge = np.repeat(natural, np.diff(rp))   # staircase index of each edge's check
+        keep = cols < self.k
+        order = np.argsort(nat_of_edge[keep], kind="stable")
+        self.cols = cols[keep][order]
+        counts = np.bincount(nat_of_edge[keep], minlength=m)
+        self.starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+        self.empty = counts == 0
 
     def encode(self, info):
         info = np.asarray(info, dtype=np.uint8)
-        s = np.mod(info.astype(np.float32) @ self.hi.T, 2).astype(np.uint8)
+        g = info[:, self.cols]
+        s = np.bitwise_xor.reduceat(g, np.minimum(self.starts, g.shape[1] - 1), axis=1)
+        s[:, self.empty] = 0
         par = np.bitwise_xor.accumulate(s, axis=1)
         return np.concatenate([info, par], axis=1)
 

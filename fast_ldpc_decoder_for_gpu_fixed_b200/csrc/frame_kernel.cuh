@@ -1,0 +1,294 @@
+// Row-layered decoder for long codes (DVB-S2 size, N = 64800): one frame per CTA,
+// everything on chip.
+//
+// The 4-frame state of a long code does not fit in one CTA's shared memory
+// (N = 64800 needs 259 KB of APP alone for 4 frames), and per-edge c->v messages
+// would add E bytes per frame (194 KB for the rate-1/2 IRA code).  But every
+// message of a min-sum check row is a function of four row quantities: the
+// magnitude c1 sent on the minimum edge, the magnitude c2 sent on the others,
+// the index of the minimum edge and one sign bit per edge.  Stored as one
+// 32-bit word per row (7 + 7 + 4 + 14 bits: degree <= 14, magnitudes <= 127,
+// which every kind but 2NMS satisfies), a frame's whole decoder state is
+// N + 4M bytes: 194 KB for N = 64800, M = 32400, inside one SM's shared memory.
+// No message crosses HBM; the prologue reads N LLR bytes and the epilogue
+// writes the hard decisions.
+//
+// The state reproduces the reference's per-edge messages exactly: edges whose
+// |t| equals min1 receive c1 in the reference (CUDA_OMS_SIMD.cu:73-90), and
+// when two edges tie at min1, min2 = min1 and c1 = c2, so one stored index
+// suffices.
+//
+// Early stop (ET) is per frame: the frame stops after an iteration in which at
+// most J.early_slack of its rows had odd extrinsic parity and its hard decisions
+// then satisfy every check.  Iteration counts are reported per frame.
+#pragma once
+#include "decode_kernel.cuh"
+
+namespace ldpc {
+
+constexpr int FRAME_MAX_THREADS = 512;
+constexpr int FRAME_MAX_DEGREE = 14;
+
+// Reads frame f (batch index) and calls put(v, x) with its int8 LLR of variable v.
+template <class F>
+__device__ __forceinline__ void read_frame(const Plan& P, const Job& J, long long f, F put)
+{
+    const int n = P.n;
+    if (J.gen) {
+        float mean = -1.0f;
+        const uint8_t* cw = J.cw ? J.cw + ((unsigned long long)f % (unsigned long long)J.n_cw) * n : nullptr;
+        if ((n & 3) == 0) {
+            for (int q = threadIdx.x; q < (n >> 2); q += blockDim.x) {
+                float u[4], gs[4];
+                uniforms4(((unsigned long long)f * n + 4 * q) >> 2, J.seed, J.offset, u);
+                box_muller4(u, gs);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (cw) mean = cw[4 * q + i] ? 1.0f : -1.0f;
+                    put(4 * q + i, quantise(mean + J.sigma * gs[i]));
+                }
+            }
+        } else {
+            for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                if (cw) mean = cw[v] ? 1.0f : -1.0f;
+                put(v, awgn_sample((unsigned long long)f * n + v, J.seed, J.offset, J.sigma, mean));
+            }
+        }
+        return;
+    }
+    if (J.interleaved) {  // word[v * W + g], byte k = frame 4g + k
+        const int8_t* src = J.llr + (f & 3);
+        const long long g = f >> 2;
+        for (int v = threadIdx.x; v < n; v += blockDim.x) put(v, __ldg(src + 4 * ((long long)v * J.total_words + g)));
+        return;
+    }
+    const int8_t* src = J.llr + (f - 4 * J.word0) * (long long)n;
+    if ((n & 15) == 0 && (reinterpret_cast<uintptr_t>(J.llr) & 15) == 0) {
+        const int4* s16 = reinterpret_cast<const int4*>(src);
+        for (int q = threadIdx.x; q < (n >> 4); q += blockDim.x) {
+            const int4 w = __ldg(s16 + q);
+            const uint32_t ws[4] = {(uint32_t)w.x, (uint32_t)w.y, (uint32_t)w.z, (uint32_t)w.w};
+#pragma unroll
+            for (int i = 0; i < 16; i++) put(16 * q + i, (int8_t)(ws[i >> 2] >> (8 * (i & 3))));
+        }
+    } else {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) put(v, __ldg(src + v));
+    }
+}
+
+// Hard decisions (x > 0) and error counts of frame f; x(v) returns the APP of v.
+template <class F>
+__device__ __forceinline__ void write_frame(const Plan& P, const Job& J, long long f, F x)
+{
+    const int n = P.n;
+    const long long lf = f - 4 * J.word0;
+    if (J.counts) {
+        __shared__ int part[FRAME_MAX_THREADS / 32];
+        int e = 0;
+        const uint8_t* cw = J.cw ? J.cw + ((unsigned long long)f % (unsigned long long)J.n_cw) * n : nullptr;
+        for (int v = threadIdx.x; v < J.n_vars; v += blockDim.x) e += (x(v) > 0) != (cw ? cw[v] != 0 : false);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = e;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+            atomicAdd(J.counts + 0, 1ull);
+            atomicAdd(J.counts + 1, (unsigned long long)t);
+            atomicAdd(J.counts + 2, (unsigned long long)(t != 0));
+        }
+    }
+    if (!J.out) return;
+    if (!J.out_packed) {
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + lf * n;
+        if ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(J.out) & 3) == 0) {
+            uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+            for (int q = threadIdx.x; q < (n >> 2); q += blockDim.x) {
+                uint32_t w = 0;
+#pragma unroll
+                for (int i = 0; i < 4; i++) w |= (uint32_t)(x(4 * q + i) > 0) << (8 * i);
+                o32[q] = w;
+            }
+        } else {
+            for (int v = threadIdx.x; v < n; v += blockDim.x) o[v] = x(v) > 0;
+        }
+    } else {
+        const int nb = (n + 7) >> 3;
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + lf * nb;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            uint32_t acc = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int v = 8 * b + j;
+                if (v < n) acc |= (uint32_t)(x(v) > 0) << j;
+            }
+            o[b] = (uint8_t)acc;
+        }
+    }
+}
+
+// true in some thread when a check of the frame has odd hard-decision parity
+__device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const Plan& P)
+{
+    bool bad = false;
+    for (int r = threadIdx.x; r < P.m; r += blockDim.x) {
+        const int d = __ldg(P.rowdeg + r);
+        int p = 0;
+        for (int j = 0; j < d; j++) p ^= app[__ldg(P.cols + j * P.m + r)] > 0;
+        bad |= p != 0;
+    }
+    return bad;
+}
+
+__device__ __forceinline__ int sat8(int x) { return min(max(x, -128), 127); }
+
+// One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134)
+// with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
+// sign bit j set when edge j's message is positive.  Returns the new state.
+// D: the row's degree (fully unrolled, no predication); v holds at least D columns.
+template <int KIND, int D, int DT>
+__device__ __forceinline__ uint32_t frame_row(int8_t* app, const int (&v)[DT], uint32_t st, bool first, bool noclip,
+                                              int& odd, const uint16_t* lut)
+{
+    int t[D];
+    const int oc1 = st & 0x7f, oc2 = (st >> 7) & 0x7f, oi = (st >> 14) & 0xf;
+    int mn1 = 127, mn2 = 127, i1 = 0, par = 0;
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+        {
+            int x = app[v[j]];
+            if (!first) {
+                const int mag = j == oi ? oc1 : oc2;
+                x = sat8(x - (((st >> (18 + j)) & 1) ? mag : -mag));
+            }
+            t[j] = x;
+            const int a = abs(x);  // 128 for -128, like vabs4
+            if (a < mn1) i1 = j;
+            mn2 = min(mn2, max(a, mn1));
+            mn1 = min(mn1, a);
+            par ^= x > 0;
+        }
+    }
+    int c1, c2;
+    PackI8::mags<KIND>(mn1, mn2, noclip, c1, c2, lut);
+    uint32_t signs = 0;
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+        {
+            const int s = par ^ (t[j] > 0);  // 1: positive message
+            const int mag = j == i1 ? c1 : c2;
+            app[v[j]] = (int8_t)sat8(t[j] + (s ? mag : -mag));
+            signs |= (uint32_t)s << j;
+        }
+    }
+    odd += par;
+    return (uint32_t)c1 | ((uint32_t)c2 << 7) | ((uint32_t)i1 << 14) | (signs << 18);
+}
+
+// Dispatches a row to the unrolled update for its degree d (<= DT).  Rows of a
+// level are sorted by degree, so the warps of a level mostly take one case.
+template <int KIND, int DT, bool EXACT>
+__device__ __forceinline__ uint32_t frame_row_any(int8_t* app, const int (&v)[DT], int d, uint32_t st, bool first,
+                                                  bool noclip, int& odd, const uint16_t* lut)
+{
+    if (EXACT) return frame_row<KIND, DT, DT>(app, v, st, first, noclip, odd, lut);
+#define LDPC_FRAME_CASE(D) \
+    case D:                \
+        if (D <= DT) return frame_row<KIND, (D <= DT ? D : DT), DT>(app, v, st, first, noclip, odd, lut);
+    switch (d) {
+        LDPC_FRAME_CASE(1) LDPC_FRAME_CASE(2) LDPC_FRAME_CASE(3) LDPC_FRAME_CASE(4) LDPC_FRAME_CASE(5)
+        LDPC_FRAME_CASE(6) LDPC_FRAME_CASE(7) LDPC_FRAME_CASE(8) LDPC_FRAME_CASE(9) LDPC_FRAME_CASE(10)
+        LDPC_FRAME_CASE(11) LDPC_FRAME_CASE(12) LDPC_FRAME_CASE(13) LDPC_FRAME_CASE(14)
+    }
+#undef LDPC_FRAME_CASE
+    return st;  // not reached: d <= FRAME_MAX_DEGREE
+}
+
+// The code-table entries of the row a thread updates in one level: its index,
+// degree, class and columns.  They do not depend on the frame's state, so they
+// are loaded two levels ahead; with one CTA per SM nothing else would hide the
+// L2 latency of tables too large for L1 (842 KB of columns for N = 64800).
+template <int DT>
+struct FrameRow {
+    int r, d, cls, end;  // row, degree (0: no row for this thread), class, end of the level
+    int v[DT];
+};
+
+template <int DT, bool EXACT>
+__device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow<DT>& x)
+{
+    const int2 lv = __ldg(P.levels + l);
+    x.r = lv.x + threadIdx.x;
+    x.end = lv.x + lv.y;
+    x.d = 0;
+    x.cls = 0;
+    if (x.r < x.end) {
+        x.d = EXACT ? DT : __ldg(P.rowdeg + x.r);
+        x.cls = __ldg(P.rowcls + x.r);
+#pragma unroll
+        for (int j = 0; j < DT; j++)  // every slot below dmax exists (padding is 0)
+            if (EXACT || j < P.dmax) x.v[j] = __ldg(P.cols + j * P.m + x.r);
+    }
+}
+
+template <int KIND, int DT, bool EXACT, bool ET>
+__global__ void __launch_bounds__(FRAME_MAX_THREADS) decode_frame_kernel(const Plan P, const Job J)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                                  // [npad]
+    uint32_t* state = reinterpret_cast<uint32_t*>(smem_raw + P.npad);                   // [m]
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad + 4 * (size_t)P.m);  // KIND_LEARNED
+    __shared__ unsigned s_odd[2];
+    const long long lf = blockIdx.x;
+    const long long f = 4 * J.word0 + lf;
+
+    read_frame(P, J, f, [&](int v, int x) { app[v] = (int8_t)x; });
+    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+    __syncthreads();
+
+    const int nl = P.nlevels;
+    FrameRow<DT> next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
+    fetch_row<DT, EXACT>(P, 0, next1);
+    fetch_row<DT, EXACT>(P, nl > 1 ? 1 : 0, next2);
+    int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
+    int executed = 0;
+    for (int it = 0; it < J.iters; it++) {
+        int odd = 0;
+        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
+        for (int l = 0; l < nl; l++) {
+            const FrameRow<DT> cur = next1;
+            next1 = next2;
+            fetch_row<DT, EXACT>(P, lf2, next2);
+            lf2 = lf2 + 1 == nl ? 0 : lf2 + 1;
+            if (cur.d) {
+                const bool noclip = J.quirk && it == 0 && cur.cls;
+                state[cur.r] = frame_row_any<KIND, DT, EXACT>(app, cur.v, cur.d, it == 0 ? 0u : state[cur.r],
+                                                              it == 0, noclip, odd, slut + 128 * cur.cls);
+            }
+            // levels wider than the CTA: the remaining rows load their entries directly
+            for (int r = cur.r + blockDim.x; r < cur.end; r += blockDim.x) {
+                FrameRow<DT> x;
+                x.d = EXACT ? DT : __ldg(P.rowdeg + r);
+                x.cls = __ldg(P.rowcls + r);
+#pragma unroll
+                for (int j = 0; j < DT; j++)
+                    if (EXACT || j < x.d) x.v[j] = __ldg(P.cols + j * P.m + r);
+                const bool noclip = J.quirk && it == 0 && x.cls;
+                state[r] = frame_row_any<KIND, DT, EXACT>(app, x.v, x.d, it == 0 ? 0u : state[r], it == 0, noclip,
+                                                          odd, slut + 128 * x.cls);
+            }
+            __syncthreads();
+        }
+        executed = it + 1;
+        if (ET) {
+            if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) && !__syncthreads_or(frame_rows_unsatisfied(app, P)))
+                break;
+        }
+    }
+
+    write_frame(P, J, f, [&](int v) { return (int)app[v]; });
+    if (J.iters_out && threadIdx.x == 0) J.iters_out[lf] = executed;
+}
+
+}  // namespace ldpc

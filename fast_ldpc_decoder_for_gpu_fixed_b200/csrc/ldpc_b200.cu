@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ldpc_b200.h"
+#include "frame_kernel.cuh"
 #include "qc_kernel.cuh"
 
 using namespace ldpc;
@@ -86,6 +87,7 @@ struct ldpc_decoder {
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
+    const void* kfn_alt = nullptr;  // the same kernel with the other early-stop setting (paths 1 and 3)
     int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA
     int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
@@ -293,15 +295,16 @@ namespace ldpc {
 const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
-const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2);
+const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et);
 const void* kernel_table_f16x2h(int kind, int variant);
+const void* kernel_table_frame(int kind, int variant, bool et);
 }
 
 // shared memory of the QC kernel: the APP of 4 frames, 8 bytes per variable
 static size_t qc_smem(const ldpc_code* c) { return (size_t)c->n * 8; }
 
 // QC register-message kernel, when the code is QC and a matching instantiation exists
-static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
+static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false)
 {
     if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > 65535) return nullptr;
     memset(&q, 0, sizeof q);
@@ -330,7 +333,7 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q)
     }
     bool pow2 = (c->z & (c->z - 1)) == 0;
     int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
-    return kernel_table_qc(k, dt, exact, c->mb, pow2);
+    return kernel_table_qc(k, dt, exact, c->mb, pow2, et && kind != LDPC_2NMS);
 }
 
 // variant: 0/1 = every row has degree 6/7 (fully unrolled), 2/3/4 = rows of
@@ -438,7 +441,9 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     const int pack_req = pack;
     if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
-    if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
+    if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_FRAME) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
+    bool frame = pack == LDPC_PACK_FRAME;
+    if (frame) pack = LDPC_PACK_I8;  // the arithmetic of that path
     if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
     int npad = (c->n + 15) / 16 * 16;
     // fp16x2 without early termination: 2 frames per CTA (half the shared memory)
@@ -453,9 +458,22 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     QCParams probe;
     bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
     qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && qc_smem(c) + 512 <= (size_t)smem_max;
-    if (smem > (size_t)smem_max && !qc_ok)
-        return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
-                    smem, smem_max);
+    if (!frame && smem > (size_t)smem_max && !qc_ok) {
+        if (pack_req != LDPC_PACK_AUTO || kind == LDPC_2NMS)
+            return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
+                        smem, smem_max);
+        frame = true;  // one frame per CTA with packed row state
+    }
+    const size_t frame_smem = (size_t)npad + 4 * (size_t)c->m + lut_smem;
+    if (frame) {
+        if (kind == LDPC_2NMS)
+            return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: 2NMS terminates per 4-frame word; use another pack");
+        if (c->dmax > FRAME_MAX_DEGREE)
+            return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: row degree %d > %d", c->dmax, FRAME_MAX_DEGREE);
+        if (frame_smem > (size_t)smem_max)
+            return fail(LDPC_ERR_UNSUPPORTED, "one frame's state needs %zu B of shared memory (> %d)", frame_smem,
+                        smem_max);
+    }
     ldpc_decoder* d = new ldpc_decoder();
     d->kind = kind;
     d->early = early;
@@ -470,9 +488,21 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         decoder_free(d);
         return rc;
     }
-    const void* qk = (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2) ? qc_kernel_for(c, kind, d->qcp) : nullptr;
-    if (qk && qc_smem(c) + lut_smem <= (size_t)smem_max) {
+    const void* qk = !frame && (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2)
+                         ? qc_kernel_for(c, kind, d->qcp, early)
+                         : nullptr;
+    if (frame) {
+        const int k = kind == LDPC_XMS ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
+        d->kfn = kernel_table_frame(k, degree_variant(c), early);
+        d->kfn_alt = kernel_table_frame(k, degree_variant(c), !early);
+        d->path = 3;
+        d->pack = LDPC_PACK_FRAME;
+        d->grid_mult = 4;
+        d->smem = (int)frame_smem;
+        d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32));
+    } else if (qk && qc_smem(c) + lut_smem <= (size_t)smem_max) {
         d->kfn = qk;
+        d->kfn_alt = qc_kernel_for(c, kind, d->qcp, !early);  // for ldpc_decoder_set_early_stop
         d->path = 1;
         d->pack = LDPC_PACK_F16X2;
         d->smem = (int)(qc_smem(c) + lut_smem);
@@ -489,6 +519,8 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     }
     cudaError_t e1 = cudaFuncSetAttribute(d->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
+    if (e1 == cudaSuccess && d->kfn_alt)
+        e1 = cudaFuncSetAttribute(d->kfn_alt, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
     cudaFuncAttributes fa;
     cudaError_t e2 = cudaFuncGetAttributes(&fa, d->kfn);
     cudaError_t e3 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->ctas_per_sm, d->kfn, d->threads, d->smem);
@@ -521,6 +553,7 @@ extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int sla
     if (enabled && d->path == 2)
         return fail(LDPC_ERR_ARG, "early stop needs a decoder created with LDPC_FLAG_EARLY_STOP for this packing");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: slack must be >= 0");
+    if ((d->path == 1 || d->path == 3) && (enabled != 0) != d->early) std::swap(d->kfn, d->kfn_alt);
     d->early = enabled != 0;
     d->early_slack = (unsigned)slack;
     return LDPC_OK;
@@ -634,6 +667,8 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
+    if (d->path == 3 && (d_app || d_msg))
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME decoders have no state dumps");
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
                   (cudaStream_t)stream);

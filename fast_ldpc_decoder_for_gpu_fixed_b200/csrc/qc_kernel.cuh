@@ -66,7 +66,9 @@ __device__ __noinline__ bool qc_rows_unsatisfied(const QCParams& Q, const char* 
     return bad;
 }
 
-template <int KIND, int DT, bool EXACT, int L, bool POW2>
+// ET: the syndrome early stop compiled in (J.early is then always set); without
+// it the extrinsic-parity count is dead code for every kind but 2NMS
+template <int KIND, int DT, bool EXACT, int L, bool POW2, bool ET>
 __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant__ QCParams Q, const Job J)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant
         // every layer.  For a biased APP b (x = 127 - b, an fp16 in [0, 255]),
         // ((b | 0x8000) - 0x57f0) has bit 15 set iff b >= 127.0, i.e. iff the
         // hard decision is 0; a row is satisfied when its count of 1s is even.
-        if (KIND != KIND_2NMS && J.early) {
+        if (KIND != KIND_2NMS && ET) {
             if (odd_rows_within_slack(J, ov, it, s_odd)) {
                 const bool bad = qc_rows_unsatisfied<DT, EXACT, L, POW2>(Q, appb, k);
                 if (!__syncthreads_or(bad)) break;

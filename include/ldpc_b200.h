@@ -60,6 +60,16 @@ extern "C" {
 #define LDPC_PACK_SIMD4 0 /* 4 frames per 32-bit word, saturating byte lanes      */
 #define LDPC_PACK_F16X2 1 /* 2 frames per 32-bit word, integer-valued fp16 lanes  */
 #define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
+/* 1 frame per CTA, everything in shared memory: the APP as int8 and each check
+ * row's messages packed into one 32-bit word (the two magnitudes, the minimum
+ * edge and the edges' signs), N + 4*M bytes per frame.  For long codes whose
+ * 4-frame state exceeds shared memory (N = 64800 rate 1/2: 194 KB).  Row degree
+ * <= 14.  LDPC_PACK_AUTO falls back to it when nothing else fits.  Not for
+ * LDPC_2NMS (whose early termination is per 4-frame word).  With
+ * LDPC_FLAG_EARLY_STOP each frame stops on its own.  On this path d_iters_out
+ * always receives one count per frame (4*n_words entries), and state dumps
+ * (ldpc_decode_device_state) are unsupported. */
+#define LDPC_PACK_FRAME 3
 
 /* output formats of ldpc_decode_device */
 #define LDPC_OUT_BYTES 0  /* frame-major 0/1 bytes [frames][n] (the reference's)  */
@@ -218,7 +228,8 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level
  * scheduled, 1 = QC register-message, 2 = level scheduled with 2 frames per
- * CTA: LDPC_PACK_F16X2 for every kind but 2NMS) */
+ * CTA: LDPC_PACK_F16X2 for every kind but 2NMS, 3 = one frame per CTA with
+ * packed row state: LDPC_PACK_FRAME) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);

@@ -137,9 +137,9 @@ static inline void check_mags(int kind, int it, int row_class, int min1, int min
  * Returns the number of iterations executed.
  */
 /* 1 when the hard decisions (x > 0) of all 4 frames satisfy every check */
-static int word_syndrome_zero(int n, int m, const int32_t* row_ptr, const int32_t* cols, const int8_t* app)
+static int word_syndrome_zero(int n, int m, const int32_t* row_ptr, const int32_t* cols, const int8_t* app, int nl)
 {
-    for (int lane = 0; lane < 4; lane++) {
+    for (int lane = 0; lane < nl; lane++) {
         const int8_t* A = app + (size_t)lane * n;
         for (int r = 0; r < m; r++) {
             int p = 0;
@@ -152,7 +152,7 @@ static int word_syndrome_zero(int n, int m, const int32_t* row_ptr, const int32_
 
 static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                        const uint8_t* row_class, int kind, int iters,
-                       int8_t* app, int8_t* msg, int early)
+                       int8_t* app, int8_t* msg, int early, int nl)
 {
     int e_total = row_ptr[m];
     int et = (kind == K_2NMS);
@@ -166,7 +166,7 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
         int odd_rows = 0; /* (row, lane) pairs whose extrinsic sign parity was odd */
         for (int r = 0; r < m; r++) {
             int b = row_ptr[r], d = row_ptr[r + 1] - b;
-            for (int lane = 0; lane < 4; lane++) {
+            for (int lane = 0; lane < nl; lane++) {
                 int8_t* A = app + (size_t)lane * n;
                 int8_t* M = msg + (size_t)lane * e_total;
                 int min1 = 127, min2 = 127, sgn = 0;
@@ -200,7 +200,7 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
          * early = 1 + slack): after an iteration in which at most `slack` (row,
          * lane) pairs had odd extrinsic parity, stop if the hard decisions of all
          * 4 frames form codewords */
-        if (early && odd_rows <= early - 1 && word_syndrome_zero(n, m, row_ptr, cols, app)) break;
+        if (early && odd_rows <= early - 1 && word_syndrome_zero(n, m, row_ptr, cols, app, nl)) break;
     }
     free(tv);
     return executed;
@@ -218,10 +218,14 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
  *             word[e*W+g] (d_MSG_C_2_V), e*nframes bytes.
  *   iters_out : optional, [W] iterations executed per word.
  */
+/* group: frames that stop together under the early stop (4 = a word, the
+ * level and QC kernels; 1 = each frame alone, the LDPC_PACK_HBM kernel, whose
+ * iteration counts are then per frame: iters_out holds nframes entries) */
 int oracle_decode_ex(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                      const uint8_t* row_class, int kind, int iters, int nframes,
                      int interleaved, const int8_t* llr, uint8_t* hard,
-                     int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads, int early)
+                     int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads, int early,
+                     int group)
 {
     if (nframes % 4 || iters < 1 || n <= 0 || m <= 0) return -1;
     int W = nframes / 4;
@@ -238,8 +242,16 @@ int oracle_decode_ex(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                     ? llr[((size_t)v * W + g) * 4 + lane]
                     : llr[(size_t)f * n + v];
         }
-        int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg, early);
-        if (iters_out) iters_out[g] = ex;
+        if (group == 1) {
+            for (int lane = 0; lane < 4; lane++) {
+                int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app + (size_t)lane * n,
+                                     msg + (size_t)lane * e_total, early, 1);
+                if (iters_out) iters_out[4 * g + lane] = ex;
+            }
+        } else {
+            int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg, early, 4);
+            if (iters_out) iters_out[g] = ex;
+        }
         for (int lane = 0; lane < 4; lane++) {
             int f = 4 * g + lane;
             for (int v = 0; v < n; v++) {
@@ -263,7 +275,7 @@ int oracle_decode(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                   int8_t* app_out, int8_t* msg_out, int32_t* iters_out, int nthreads)
 {
     return oracle_decode_ex(n, m, row_ptr, cols, row_class, kind, iters, nframes, interleaved, llr, hard,
-                            app_out, msg_out, iters_out, nthreads, 0);
+                            app_out, msg_out, iters_out, nthreads, 0, 4);
 }
 
 /* ---- layout restatements (transpose/GPU_Transpose_uint8.cu) ------------- */

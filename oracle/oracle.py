@@ -40,7 +40,7 @@ def lib():
         i = ctypes.c_int
         L.oracle_decode.argtypes = [i, i, P, P, P, i, i, i, i, P, P, P, P, P, i]
         L.oracle_decode.restype = i
-        L.oracle_decode_ex.argtypes = [i, i, P, P, P, i, i, i, i, P, P, P, P, P, i, i]
+        L.oracle_decode_ex.argtypes = [i, i, P, P, P, i, i, i, i, P, P, P, P, P, i, i, i]
         L.oracle_decode_ex.restype = i
         L.oracle_decode_batch.argtypes = [i, i, P, P, P, i, i, i, i, P, P, i]
         L.oracle_decode_batch.restype = i
@@ -68,14 +68,15 @@ def _p(a):
 
 
 def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False,
-           early_slack=128):
+           early_slack=128, per_frame=False):
     """Decodes ``llr`` (int8, nframes*n bytes, frame-major unless interleaved).
 
     Returns dict with ``hard`` [nframes, n] uint8, ``iters`` [nframes/4] and,
     if ``want_state``, ``app`` / ``msg`` in the reference's word-interleaved
     device layouts (n*nframes and e*nframes bytes).  ``early_stop``: the
     syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word) with
-    ``early_slack`` (ldpc_decoder_set_early_stop).
+    ``early_slack`` (ldpc_decoder_set_early_stop); ``per_frame``: every frame
+    stops on its own and ``iters`` has one entry per frame (LDPC_PACK_HBM).
     """
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
@@ -83,13 +84,14 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     llr = np.ascontiguousarray(llr, dtype=np.int8).reshape(-1)
     nframes = llr.size // code.n
     hard = np.zeros((nframes, code.n), dtype=np.uint8)
-    it = np.zeros(nframes // 4, dtype=np.int32)
+    it = np.zeros(nframes if per_frame else nframes // 4, dtype=np.int32)
     app = np.zeros(code.n * nframes, dtype=np.int8) if want_state else None
     msg = np.zeros(code.e * nframes, dtype=np.int8) if want_state else None
     nt = nthreads or os.cpu_count() or 1
     rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
                                 k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
-                                _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0)
+                                _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0,
+                                1 if per_frame else 4)
     if rc != 0:
         raise ValueError("oracle_decode rejected the arguments")
     out = {"hard": hard, "iters": it}

@@ -82,9 +82,15 @@ def test_error_statuses(cuda):
 
 
 def test_oversized_code_rejected(cuda):
-    with pytest.raises(fl.LdpcError) as e:
-        fl.Decoder(table("64800x32400"), "OMS", nb_frames=4)
-    assert e.value.code == -3
+    """The 4-frame state of N = 64800 does not fit in shared memory: an explicit
+    4-frame packing is rejected, and AUTO takes the one-frame-per-CTA path."""
+    for pack in ("SIMD4", "F16X2", "I8"):
+        with pytest.raises(fl.LdpcError) as e:
+            fl.Decoder(table("64800x32400"), "OMS", nb_frames=4, pack=pack)
+        assert e.value.code == -3
+    dec = fl.Decoder(table("64800x32400"), "OMS", nb_frames=4)
+    assert dec.info()["path"] == 3
+    dec.close()
 
 
 @pytest.mark.parametrize("op", range(10))

@@ -1,0 +1,139 @@
+"""LDPC_PACK_FRAME (one frame per CTA, packed row state in shared memory): GPU decoders
+against the CPU oracle for every kind it serves, with and without the
+per-frame early stop, on the reference tables and on the long IRA code whose
+state only this path can hold; the fused simulation and the plugin path."""
+import numpy as np
+import pytest
+
+import llr_gen
+from gpu_helpers import make_llr
+from oracle import oracle
+from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, LdpcError, load_table
+from fast_ldpc_decoder_for_gpu_fixed_b200.codes import ira
+
+pytestmark = pytest.mark.gpu
+
+
+def _decode(code, kind, llr, iters, words, early=False, slack=None, constants=None):
+    import torch
+    dec = Decoder(code, kind, nb_frames=words, pack="FRAME", early_stop=early)
+    if slack is not None:
+        dec.set_early_stop(True, slack)
+    if constants is not None:
+        dec.set_learned(*constants)
+    assert dec.info()["path"] == 3
+    d_llr = torch.from_numpy(np.ascontiguousarray(llr)).cuda()
+    d_hard = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    d_it = torch.zeros(4 * words, dtype=torch.int32, device="cuda")
+    dec.decode_device(d_llr, d_hard, words, iters, d_iters=d_it)
+    torch.cuda.synchronize()
+    dec.close()
+    return d_hard.cpu().numpy().reshape(4 * words, code.n), d_it.cpu().numpy()
+
+
+@pytest.mark.parametrize("kind", ["MS", "OMS", "NMS", "XMS"])
+@pytest.mark.parametrize("name", ["4000x2000", "576x288", "1944x972"])
+def test_frame_fixed_iterations(cuda, name, kind):
+    code = load_table(name)
+    words = 6
+    llr = make_llr("awgn", 4 * words * code.n, 3, sigma=llr_gen.sigma_for(1.5, 0.5))
+    ref = oracle.decode(code, kind, llr, 12)
+    hard, its = _decode(code, kind, llr, 12, words)
+    assert np.array_equal(hard, ref["hard"])
+    assert (its == 12).all()
+
+
+@pytest.mark.parametrize("slack", [0, 128])
+@pytest.mark.parametrize("name", ["576x288", "1944x972"])
+def test_frame_early_stop_per_frame(cuda, name, slack):
+    code = load_table(name)
+    words = 12
+    llr = np.concatenate([make_llr("awgn", 4 * 4 * code.n, 7 + i, sigma=llr_gen.sigma_for(e, 0.5))
+                          for i, e in enumerate((1.0, 2.5, 4.0))])
+    ref = oracle.decode(code, "OMS", llr, 25, early_stop=True, early_slack=slack, per_frame=True)
+    hard, its = _decode(code, "OMS", llr, 25, words, early=True, slack=slack)
+    assert np.array_equal(its, ref["iters"])
+    assert np.array_equal(hard, ref["hard"])
+    assert len(set(its.tolist())) > 3
+
+
+def test_frame_learned(cuda):
+    code = load_table("1944x972")
+    words = 4
+    off = np.array([[1, 2], [1, 1], [0, 1]], dtype=np.int8)
+    sc = np.array([[128, 120], [112, 128], [120, 104]], dtype=np.uint8)
+    oracle.set_learned(off, sc)
+    llr = make_llr("awgn", 4 * words * code.n, 9, sigma=llr_gen.sigma_for(1.75, 0.5))
+    ref = oracle.decode(code, "LEARNED", llr, 10)
+    hard, _ = _decode(code, "LEARNED", llr, 10, words, constants=(off, sc))
+    assert np.array_equal(hard, ref["hard"])
+
+
+def test_long_ira_code_takes_the_frame_path(cuda):
+    code = ira()   # N = 64800: the 4-frame state does not fit in shared memory
+    words = 2
+    dec = Decoder(code, "OMS", nb_frames=words, early_stop=True)
+    assert dec.info()["path"] == 3
+    dec.close()
+    llr = make_llr("awgn", 4 * words * code.n, 11, sigma=llr_gen.sigma_for(1.2, 0.5))
+    ref = oracle.decode(code, "OMS", llr, 30, early_stop=True, per_frame=True)
+    hard, its = _decode(code, "OMS", llr, 30, words, early=True)
+    assert np.array_equal(its, ref["iters"])
+    assert np.array_equal(hard, ref["hard"])
+    stopped = its < 30          # frames that stopped early hold codewords
+    assert stopped.sum() >= 4 and (code.syndrome(hard[stopped]) == 0).all()
+
+
+def test_frame_fused_simulation(cuda):
+    import torch
+    code = load_table("1944x972")
+    words = 16
+    dec = Decoder(code, "OMS", nb_frames=words, pack="FRAME", early_stop=True)
+    d_hard = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    counts = torch.zeros(3, dtype=torch.int64, device="cuda")
+    dec.simulate(words, 20, 0.85, 3, 1, counts, d_hard=d_hard, n_vars=code.n)
+    torch.cuda.synchronize()
+    dec.close()
+    llr, _ = oracle.awgn(4 * words, code.n, 0.85, 3, 1)
+    ref = oracle.decode(code, "OMS", llr, 20, early_stop=True, per_frame=True)
+    assert np.array_equal(d_hard.cpu().numpy().reshape(4 * words, code.n), ref["hard"])
+    be, fe, _ = oracle.count_errors(code.n, code.n, ref["hard"])
+    assert counts.cpu().tolist() == [4 * words, be, fe]
+
+
+def test_frame_host_decode(cuda):
+    code = load_table("576x288")
+    words = 40
+    llr = make_llr("awgn", 4 * words * code.n, 13, sigma=llr_gen.sigma_for(1.5, 0.5))
+    dec = Decoder(code, "OMS", nb_frames=words, pack="FRAME")
+    hard = np.zeros((4 * words, code.n), dtype=np.uint8)
+    dec.decode_host(llr.reshape(4 * words, code.n), hard, 15)
+    dec.close()
+    assert np.array_equal(hard, oracle.decode(code, "OMS", llr, 15)["hard"])
+
+
+def test_frame_rejections(cuda):
+    import torch
+    code = load_table("576x288")
+    with pytest.raises(LdpcError):
+        Decoder(code, "2NMS", nb_frames=4, pack="FRAME")
+    dec = Decoder(code, "OMS", nb_frames=4, pack="FRAME")
+    d = torch.zeros(16 * code.n, dtype=torch.int8, device="cuda")
+    h = torch.zeros(16 * code.n, dtype=torch.uint8, device="cuda")
+    with pytest.raises(LdpcError):
+        dec.decode_device_state(d, h, 4, 5, d_app=d)
+    dec.close()
+
+
+def test_reference_long_table(cuda):
+    """The reference's 64800x32400 table (its table order is a serial schedule)
+    decodes on the one-frame-per-CTA path exactly like the oracle."""
+    code = load_table("64800x32400")
+    words = 2
+    llr = make_llr("awgn", 4 * words * code.n, 17, sigma=llr_gen.sigma_for(1.5, 0.5))
+    ref = oracle.decode(code, "OMS", llr, 3)
+    dec = Decoder(code, "OMS", nb_frames=words)
+    assert dec.info()["path"] == 3
+    dec.close()
+    hard, _ = _decode(code, "OMS", llr, 3, words)
+    assert np.array_equal(hard, ref["hard"])
