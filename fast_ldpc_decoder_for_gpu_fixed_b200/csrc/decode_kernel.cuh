@@ -39,6 +39,9 @@ struct Plan {
     const uint8_t* rowcls;  // [m] 1 = reference's second degree group
     const int2* levels;     // [nlevels] (first r', row count)
     const int32_t* edge_orig;  // [dmax][m] edge index in table order (state dumps)
+    // [m][2] 32-byte row records (dmax <= 14): u16 columns 0..13, slot 14 unused,
+    // slot 15 = degree | class << 8; null when dmax > 14
+    const uint4* rowrec;
 };
 
 struct Job {

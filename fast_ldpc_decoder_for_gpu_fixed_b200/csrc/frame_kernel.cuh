@@ -146,9 +146,48 @@ __device__ __forceinline__ int sat8(int x) { return min(max(x, -128), 127); }
 // One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134)
 // with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
 // sign bit j set when edge j's message is positive.  Returns the new state.
-// D: the row's degree (fully unrolled, no predication); v holds at least D columns.
-template <int KIND, int D, int DT>
-__device__ __forceinline__ uint32_t frame_row(int8_t* app, const int (&v)[DT], uint32_t st, bool first, bool noclip,
+// The row a thread updates in one level: its record (columns, degree, class;
+// see Plan::rowrec) and its index.  Records do not depend on the frame's
+// state, so they are loaded two levels ahead: with one CTA per SM nothing else
+// hides the L2 latency of a table too large for L1 (1 MB for M = 32400).
+struct FrameRow {
+    uint4 c0, c1;
+    int r, end;  // row, end of its level
+    __device__ __forceinline__ int deg() const { return (c1.w >> 16) & 0xff; }
+    __device__ __forceinline__ int cls() const { return c1.w >> 24; }
+    __device__ __forceinline__ int col(int j) const  // j a compile-time constant after unrolling
+    {
+        const uint4& q = j < 8 ? c0 : c1;
+        const int k = (j & 7) >> 1;
+        const uint32_t w = k == 0 ? q.x : (k == 1 ? q.y : (k == 2 ? q.z : q.w));
+        return (j & 1) ? (int)(w >> 16) : (int)(w & 0xffff);
+    }
+};
+
+__device__ __forceinline__ void load_row(const Plan& P, int r, FrameRow& x)
+{
+    x.c0 = __ldg(P.rowrec + 2 * r);
+    x.c1 = __ldg(P.rowrec + 2 * r + 1);
+}
+
+__device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow& x)
+{
+    const int2 lv = __ldg(P.levels + l);
+    x.r = lv.x + threadIdx.x;
+    x.end = lv.x + lv.y;
+    if (x.r < x.end) {
+        load_row(P, x.r, x);
+    } else {
+        x.c1.w = 0;  // degree 0: no row for this thread
+    }
+}
+
+// One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134)
+// with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
+// sign bit j set when edge j's message is positive.  D: the row's degree (fully
+// unrolled).  Returns the new state.
+template <int KIND, int D>
+__device__ __forceinline__ uint32_t frame_row(int8_t* app, const FrameRow& row, uint32_t st, bool first, bool noclip,
                                               int& odd, const uint16_t* lut)
 {
     int t[D];
@@ -156,80 +195,49 @@ __device__ __forceinline__ uint32_t frame_row(int8_t* app, const int (&v)[DT], u
     int mn1 = 127, mn2 = 127, i1 = 0, par = 0;
 #pragma unroll
     for (int j = 0; j < D; j++) {
-        {
-            int x = app[v[j]];
-            if (!first) {
-                const int mag = j == oi ? oc1 : oc2;
-                x = sat8(x - (((st >> (18 + j)) & 1) ? mag : -mag));
-            }
-            t[j] = x;
-            const int a = abs(x);  // 128 for -128, like vabs4
-            if (a < mn1) i1 = j;
-            mn2 = min(mn2, max(a, mn1));
-            mn1 = min(mn1, a);
-            par ^= x > 0;
+        int x = app[row.col(j)];
+        if (!first) {
+            const int mag = j == oi ? oc1 : oc2;
+            x = sat8(x - (((st >> (18 + j)) & 1) ? mag : -mag));
         }
+        t[j] = x;
+        const int a = abs(x);  // 128 for -128, like vabs4
+        if (a < mn1) i1 = j;
+        mn2 = min(mn2, max(a, mn1));
+        mn1 = min(mn1, a);
+        par ^= x > 0;
     }
     int c1, c2;
     PackI8::mags<KIND>(mn1, mn2, noclip, c1, c2, lut);
     uint32_t signs = 0;
 #pragma unroll
     for (int j = 0; j < D; j++) {
-        {
-            const int s = par ^ (t[j] > 0);  // 1: positive message
-            const int mag = j == i1 ? c1 : c2;
-            app[v[j]] = (int8_t)sat8(t[j] + (s ? mag : -mag));
-            signs |= (uint32_t)s << j;
-        }
+        const int s = par ^ (t[j] > 0);  // 1: positive message
+        const int mag = j == i1 ? c1 : c2;
+        app[row.col(j)] = (int8_t)sat8(t[j] + (s ? mag : -mag));
+        signs |= (uint32_t)s << j;
     }
     odd += par;
     return (uint32_t)c1 | ((uint32_t)c2 << 7) | ((uint32_t)i1 << 14) | (signs << 18);
 }
 
-// Dispatches a row to the unrolled update for its degree d (<= DT).  Rows of a
-// level are sorted by degree, so the warps of a level mostly take one case.
+// Dispatches a row to the unrolled update for its degree.  Rows of a level are
+// sorted by degree, so the warps of a level mostly take one case.
 template <int KIND, int DT, bool EXACT>
-__device__ __forceinline__ uint32_t frame_row_any(int8_t* app, const int (&v)[DT], int d, uint32_t st, bool first,
+__device__ __forceinline__ uint32_t frame_row_any(int8_t* app, const FrameRow& row, uint32_t st, bool first,
                                                   bool noclip, int& odd, const uint16_t* lut)
 {
-    if (EXACT) return frame_row<KIND, DT, DT>(app, v, st, first, noclip, odd, lut);
+    if (EXACT) return frame_row<KIND, DT>(app, row, st, first, noclip, odd, lut);
 #define LDPC_FRAME_CASE(D) \
     case D:                \
-        if (D <= DT) return frame_row<KIND, (D <= DT ? D : DT), DT>(app, v, st, first, noclip, odd, lut);
-    switch (d) {
+        if (D <= DT) return frame_row<KIND, (D <= DT ? D : DT)>(app, row, st, first, noclip, odd, lut);
+    switch (row.deg()) {
         LDPC_FRAME_CASE(1) LDPC_FRAME_CASE(2) LDPC_FRAME_CASE(3) LDPC_FRAME_CASE(4) LDPC_FRAME_CASE(5)
         LDPC_FRAME_CASE(6) LDPC_FRAME_CASE(7) LDPC_FRAME_CASE(8) LDPC_FRAME_CASE(9) LDPC_FRAME_CASE(10)
         LDPC_FRAME_CASE(11) LDPC_FRAME_CASE(12) LDPC_FRAME_CASE(13) LDPC_FRAME_CASE(14)
     }
 #undef LDPC_FRAME_CASE
-    return st;  // not reached: d <= FRAME_MAX_DEGREE
-}
-
-// The code-table entries of the row a thread updates in one level: its index,
-// degree, class and columns.  They do not depend on the frame's state, so they
-// are loaded two levels ahead; with one CTA per SM nothing else would hide the
-// L2 latency of tables too large for L1 (842 KB of columns for N = 64800).
-template <int DT>
-struct FrameRow {
-    int r, d, cls, end;  // row, degree (0: no row for this thread), class, end of the level
-    int v[DT];
-};
-
-template <int DT, bool EXACT>
-__device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow<DT>& x)
-{
-    const int2 lv = __ldg(P.levels + l);
-    x.r = lv.x + threadIdx.x;
-    x.end = lv.x + lv.y;
-    x.d = 0;
-    x.cls = 0;
-    if (x.r < x.end) {
-        x.d = EXACT ? DT : __ldg(P.rowdeg + x.r);
-        x.cls = __ldg(P.rowcls + x.r);
-#pragma unroll
-        for (int j = 0; j < DT; j++)  // every slot below dmax exists (padding is 0)
-            if (EXACT || j < P.dmax) x.v[j] = __ldg(P.cols + j * P.m + x.r);
-    }
+    return st;  // not reached: degrees are 1..FRAME_MAX_DEGREE
 }
 
 template <int KIND, int DT, bool EXACT, bool ET>
@@ -248,35 +256,31 @@ __global__ void __launch_bounds__(FRAME_MAX_THREADS) decode_frame_kernel(const P
     __syncthreads();
 
     const int nl = P.nlevels;
-    FrameRow<DT> next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
-    fetch_row<DT, EXACT>(P, 0, next1);
-    fetch_row<DT, EXACT>(P, nl > 1 ? 1 : 0, next2);
+    FrameRow next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
+    fetch_row(P, 0, next1);
+    fetch_row(P, nl > 1 ? 1 : 0, next2);
     int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
     int executed = 0;
     for (int it = 0; it < J.iters; it++) {
         int odd = 0;
         if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
         for (int l = 0; l < nl; l++) {
-            const FrameRow<DT> cur = next1;
+            const FrameRow cur = next1;
             next1 = next2;
-            fetch_row<DT, EXACT>(P, lf2, next2);
+            fetch_row(P, lf2, next2);
             lf2 = lf2 + 1 == nl ? 0 : lf2 + 1;
-            if (cur.d) {
-                const bool noclip = J.quirk && it == 0 && cur.cls;
-                state[cur.r] = frame_row_any<KIND, DT, EXACT>(app, cur.v, cur.d, it == 0 ? 0u : state[cur.r],
-                                                              it == 0, noclip, odd, slut + 128 * cur.cls);
+            if (cur.r < cur.end) {
+                const bool noclip = J.quirk && it == 0 && cur.cls();
+                state[cur.r] = frame_row_any<KIND, DT, EXACT>(app, cur, it == 0 ? 0u : state[cur.r], it == 0, noclip,
+                                                              odd, slut + 128 * cur.cls());
             }
-            // levels wider than the CTA: the remaining rows load their entries directly
+            // levels wider than the CTA: the remaining rows load their records directly
             for (int r = cur.r + blockDim.x; r < cur.end; r += blockDim.x) {
-                FrameRow<DT> x;
-                x.d = EXACT ? DT : __ldg(P.rowdeg + r);
-                x.cls = __ldg(P.rowcls + r);
-#pragma unroll
-                for (int j = 0; j < DT; j++)
-                    if (EXACT || j < x.d) x.v[j] = __ldg(P.cols + j * P.m + r);
-                const bool noclip = J.quirk && it == 0 && x.cls;
-                state[r] = frame_row_any<KIND, DT, EXACT>(app, x.v, x.d, it == 0 ? 0u : state[r], it == 0, noclip,
-                                                          odd, slut + 128 * x.cls);
+                FrameRow x;
+                load_row(P, r, x);
+                const bool noclip = J.quirk && it == 0 && x.cls();
+                state[r] = frame_row_any<KIND, DT, EXACT>(app, x, it == 0 ? 0u : state[r], it == 0, noclip, odd,
+                                                          slut + 128 * x.cls());
             }
             __syncthreads();
         }

@@ -78,6 +78,7 @@ struct ldpc_decoder {
     int n = 0, m = 0, e = 0;
     Plan plan{};
     uint16_t* d_cols = nullptr;
+    void* d_rowrec = nullptr;
     uint8_t* d_rowdeg = nullptr;
     uint8_t* d_rowcls = nullptr;
     int2* d_levels = nullptr;
@@ -377,6 +378,7 @@ static void decoder_free(ldpc_decoder* d)
 {
     if (!d) return;
     cudaFree(d->d_cols);
+    cudaFree(d->d_rowrec);
     cudaFree(d->d_rowdeg);
     cudaFree(d->d_rowcls);
     cudaFree(d->d_levels);
@@ -405,6 +407,15 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
             eorig[(size_t)j * m + rp] = b + j;
         }
     }
+    if (dmax <= 14) {  // row records of the one-frame-per-CTA kernel
+        std::vector<uint16_t> rec((size_t)m * 16, 0);
+        for (int rp = 0; rp < m; rp++) {
+            for (int j = 0; j < deg[rp]; j++) rec[(size_t)rp * 16 + j] = cols[(size_t)j * m + rp];
+            rec[(size_t)rp * 16 + 15] = (uint16_t)(deg[rp] | (cls[rp] << 8));
+        }
+        CUDA_TRY(cudaMalloc(&d->d_rowrec, rec.size() * sizeof(uint16_t)));
+        CUDA_TRY(cudaMemcpy(d->d_rowrec, rec.data(), rec.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    }
     CUDA_TRY(cudaMalloc(&d->d_cols, cols.size() * sizeof(uint16_t)));
     CUDA_TRY(cudaMalloc(&d->d_edge_orig, eorig.size() * sizeof(int32_t)));
     CUDA_TRY(cudaMalloc(&d->d_rowdeg, m));
@@ -426,6 +437,7 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
     P.rowcls = d->d_rowcls;
     P.levels = d->d_levels;
     P.edge_orig = d->d_edge_orig;
+    P.rowrec = reinterpret_cast<const uint4*>(d->d_rowrec);
     return LDPC_OK;
 }
 
@@ -559,6 +571,18 @@ extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int sla
     return LDPC_OK;
 }
 
+// fp16 bit pattern of x, which must be exactly representable (normal or zero)
+static uint16_t half_bits(double x)
+{
+    if (x == 0.0) return 0;
+    const uint16_t sign = x < 0 ? 0x8000 : 0;
+    double a = x < 0 ? -x : x;
+    int e = 0;
+    while (a >= 2.0) { a /= 2.0; e++; }
+    while (a < 1.0) { a *= 2.0; e--; }
+    return (uint16_t)(sign | ((e + 15) << 10) | ((int)((a - 1.0) * 1024.0 + 0.5) & 0x3ff));
+}
+
 extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8_t* offsets, const uint8_t* scales)
 {
     if (!d || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: null pointer");
@@ -566,23 +590,33 @@ extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8
     if (n_iters < 1 || n_iters > LDPC_LEARNED_MAX_ITERS)
         return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: n_iters must be in [1, %d]", LDPC_LEARNED_MAX_ITERS);
     const bool fp16 = d->pack == LDPC_PACK_F16X2;
-    std::vector<uint16_t> lut((size_t)n_iters * 256);
-    for (int t = 0; t < n_iters; t++)
-        for (int g = 0; g < 2; g++)
-            for (int m = 0; m < 128; m++) {
-                int c = ((m * (int)scales[2 * t + g]) >> 7) - offsets[2 * t + g];
-                c = c < 0 ? 0 : (c > 31 ? 31 : c);
-                // fp16 bit pattern of the integer c (exact), or the plain integer
-                uint16_t v = (uint16_t)c;
-                if (fp16) {
-                    if (c == 0) v = 0;
-                    else {
-                        int e = 31 - __builtin_clz((unsigned)c);  // c < 32
-                        v = (uint16_t)(((e + 15) << 10) | ((c << (10 - e)) & 0x3ff));
-                    }
-                }
-                lut[(size_t)t * 256 + g * 128 + m] = v;
+    std::vector<uint16_t> lut((size_t)n_iters * 256, 0);
+    if (fp16) {
+        // the fp16 kernels compute floor(min * s / 128) - offset as round(min * k + b) with
+        // k = s / 128, b = -offset - 15/32 (packs.cuh, h2::mags): exact when k has at most 4
+        // fraction bits (s a multiple of 8) and b is an fp16 (|offset| <= 31)
+        for (int i = 0; i < 2 * n_iters; i++)
+            if (scales[i] % 8 != 0 || offsets[i] < -31 || offsets[i] > 31)
+                return fail(LDPC_ERR_UNSUPPORTED,
+                            "LDPC_PACK_F16X2 LDPC_LEARNED decoders need scales that are multiples of 8 and offsets "
+                            "in [-31, 31] (got scale %d, offset %d); use LDPC_PACK_SIMD4 or LDPC_PACK_I8 for others",
+                            (int)scales[i], (int)offsets[i]);
+        for (int t = 0; t < n_iters; t++)
+            for (int g = 0; g < 2; g++) {
+                const uint16_t k = half_bits(scales[2 * t + g] / 128.0);
+                const uint16_t b = half_bits(-offsets[2 * t + g] - 15.0 / 32.0);
+                uint16_t* e = &lut[(size_t)t * 256 + g * 128];
+                e[0] = e[1] = k;  // (k, k) and (b, b) as f16x2 words
+                e[2] = e[3] = b;
             }
+    } else {
+        for (int t = 0; t < n_iters; t++)
+            for (int g = 0; g < 2; g++)
+                for (int m = 0; m < 128; m++) {
+                    int c = ((m * (int)scales[2 * t + g]) >> 7) - offsets[2 * t + g];
+                    lut[(size_t)t * 256 + g * 128 + m] = (uint16_t)(c < 0 ? 0 : (c > 31 ? 31 : c));
+                }
+    }
     if (!d->d_lut) CUDA_TRY(cudaMalloc(&d->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
     CUDA_TRY(cudaMemcpy(d->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
     d->lut_its = n_iters;

@@ -38,10 +38,11 @@ namespace ldpc {
 enum { KIND_MS = 0, KIND_OMS = 1, KIND_NMS = 2, KIND_2NMS = 3, KIND_XMS = 4, KIND_LEARNED = 5 };
 
 // KIND_LEARNED (no reference counterpart): the magnitude of a check's outgoing
-// messages is lut[min] from a 128-entry table of the current iteration and row
-// group, c = clamp(floor(min * scale_q7 / 128) - offset, 0, 31), built on the
-// host from the trained int8 offsets and Q1.7 scales.  The table holds plain
-// integers for PackSIMD4 / PackI8 and fp16 bit patterns for PackF16x2.
+// messages is c = clamp(floor(min * scale_q7 / 128) - offset, 0, 31) with the
+// trained int8 offset and Q1.7 scale of the current iteration and row group.
+// PackSIMD4 / PackI8 read it from a 128-entry table of plain integers built on
+// the host; PackF16x2 computes it from (k, b) pairs stored at the head of the
+// same table (h2::mags).
 
 // ------------------------------------------------------------------------
 // 4 frames per word, per-byte saturating SIMD
@@ -190,18 +191,12 @@ __device__ __forceinline__ uint32_t max_xs(uint32_t a, uint32_t b)
     asm("max.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
 }
-// floor(m * k) for integer m in [0,127], k = 3/4 or 7/8: m*k - (1/2 - 2^-(bits+1)) is
-// exact, within 1/2 of the floor and never on a tie, so adding 1024 rounds it there.
+// floor(m * k) for integer m in [0,127], k with few fraction bits (3/4, 7/8, s/16):
+// m*k - (1/2 - 2^-(bits+1)) is exact, within 1/2 of the floor and never on a tie,
+// so adding 1024 rounds it there.
 __device__ __forceinline__ uint32_t floor_scale(uint32_t m, uint32_t k, uint32_t bias)
 {
     return add(add(fma_relu(m, k, bias), C1024), CNEG1024);
-}
-
-// table lookup of both lanes: a + 1024 puts the integer a in the low 10 mantissa bits
-__device__ __forceinline__ uint32_t lut2(uint32_t a, const uint16_t* lut)
-{
-    const uint32_t i = add(a, C1024);
-    return (uint32_t)lut[i & 0x3ff] | ((uint32_t)lut[(i >> 16) & 0x3ff] << 16);
 }
 
 // row magnitudes from |min1| (a1) and |min2| (a2)
@@ -210,8 +205,13 @@ __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint
                                      const uint16_t* lut)
 {
     if (KIND == KIND_LEARNED) {
-        c1 = lut2(a2, lut);
-        c2 = lut2(a1, lut);
+        // clamp(floor(a * k) - offset, 0, 31) = min(round(relu(a * k + b)), 31), b = -offset - 15/32:
+        // with k on a 1/16 grid, a * k + b is exact below 64 and never within 1/32 of a tie
+        // (ldpc_decoder_set_learned stores (k, k) and (b, b) at the head of the class's table)
+        const uint32_t k2 = *reinterpret_cast<const uint32_t*>(lut);
+        const uint32_t b2 = *reinterpret_cast<const uint32_t*>(lut + 2);
+        c1 = hmin(floor_scale(a2, k2, b2), C31);
+        c2 = hmin(floor_scale(a1, k2, b2), C31);
     } else if (KIND == KIND_MS) {
         c1 = hmin(a2, C31);
         c2 = hmin(a1, C31);

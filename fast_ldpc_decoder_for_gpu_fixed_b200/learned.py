@@ -18,6 +18,8 @@ Finally the constants are frozen to int8 offsets and Q1.7 scales.
 PyTorch only holds the buffers and applies Adam to the 4*T parameters; every
 decoder pass is one of this library's kernels.
 """
+import os
+
 import numpy as np
 
 from . import _lib
@@ -37,12 +39,18 @@ def random_codewords(code, count, seed):
     return enc.encode(rng.integers(0, 2, size=(count, enc.k)))
 
 
-def quantize(alpha, beta):
-    """FP32 scales/offsets [T][2] -> (int8 offsets, uint8 Q1.7 scales)."""
+SCALE_STEP = 8   # Q1.7 scales on a 1/16 grid: what the fp16 (QC) kernels compute exactly
+OFFSET_MAX = 31
+
+
+def quantize(alpha, beta, scale_step=SCALE_STEP):
+    """FP32 scales/offsets [T][2] -> (int8 offsets in [-31, 31], uint8 Q1.7 scales,
+    multiples of ``scale_step``)."""
     alpha = np.asarray(alpha, dtype=np.float64)
     beta = np.asarray(beta, dtype=np.float64)
-    off = np.clip(np.rint(beta), -128, 127).astype(np.int8)
-    sc = np.clip(np.rint(alpha * 128.0), 0, 255).astype(np.uint8)
+    off = np.clip(np.rint(beta), -OFFSET_MAX, OFFSET_MAX).astype(np.int8)
+    top = 255 // scale_step * scale_step
+    sc = np.clip(np.rint(alpha * 128.0 / scale_step) * scale_step, 0, top).astype(np.uint8)
     return off, sc
 
 
@@ -120,7 +128,8 @@ class Trainer:
     def _used(self, quantized):
         if not quantized:
             return self.alpha.detach(), self.beta.detach()
-        return (self.torch.round(self.alpha.detach() * 128.0) / 128.0).contiguous(), \
+        q = 128.0 / SCALE_STEP
+        return (self.torch.round(self.alpha.detach() * q) / q).contiguous(), \
             self.torch.round(self.beta.detach()).contiguous()
 
     def step(self, quantized=False):
@@ -136,8 +145,8 @@ class Trainer:
                             frame_loss=self.frame_loss, stream=self.torch.cuda.current_stream())
         self.opt.step()
         with self.torch.no_grad():
-            self.alpha.clamp_(0.0, 255.0 / 128.0)
-            self.beta.clamp_(-8.0, 31.0)
+            self.alpha.clamp_(0.0, (255 // SCALE_STEP * SCALE_STEP) / 128.0)
+            self.beta.clamp_(-8.0, float(OFFSET_MAX))
         return self.d_loss.clone()
 
     def train(self, frames, qat_fraction=0.3, log_every=16):
@@ -211,3 +220,86 @@ def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewor
     f, be, fe = (int(x) for x in counts.cpu().tolist())
     return {"frames": f, "bit_errors": be, "frame_errors": fe, "fer": fe / f, "ber": be / (f * code.n),
             "mean_iters": float(it_sum.item()) / (calls * words)}
+
+
+def save_constants(path, offsets, scales, **meta):
+    """Writes frozen constants ([T][2] int8 offsets, uint8 Q1.7 scales) and metadata as JSON."""
+    import json
+    doc = dict(meta)
+    doc["offsets"] = np.asarray(offsets, dtype=np.int8).tolist()
+    doc["scales"] = np.asarray(scales, dtype=np.uint8).tolist()
+    with open(path, "w") as f:
+        json.dump(doc, f, indent=1)
+
+
+def load_constants(path):
+    """(offsets, scales, metadata) from a file written by ``save_constants``."""
+    import json
+    with open(path) as f:
+        doc = json.load(f)
+    return np.asarray(doc["offsets"], dtype=np.int8), np.asarray(doc["scales"], dtype=np.uint8), doc
+
+
+TRAINED_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "trained")
+
+
+def _code_by_name(name):
+    from .codes import load_table, qc_regular
+    if name == "qc3x6_z256":
+        return qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
+    return load_table(name)
+
+
+def main(argv=None):
+    """python -m fast_ldpc_decoder_for_gpu_fixed_b200.learned --code qc3x6_z256 --out FILE:
+    trains, evaluates against plain OMS and writes the frozen constants."""
+    import argparse
+    import time
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--code", default="qc3x6_z256")
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--frames", type=int, default=2_000_000)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--ebn0", type=float, nargs=2, default=(1.0, 3.0))
+    ap.add_argument("--loss", default="bit", choices=("bit", "frame"))
+    ap.add_argument("--weights", default="all", choices=("all", "last"))
+    ap.add_argument("--init", default="oms", choices=("oms", "ms"))
+    ap.add_argument("--qat", type=float, default=1.0, help="fraction of the steps with the quantised forward pass")
+    ap.add_argument("--lr", type=float, default=0.01)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--eval-ebn0", type=float, nargs="*", default=(1.75, 2.0, 2.25))
+    ap.add_argument("--eval-frames", type=int, default=262144)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    code = _code_by_name(a.code)
+    tr = Trainer(code, iters=a.iters, batch=a.batch, lr=a.lr, seed=a.seed, weights=a.weights, loss=a.loss,
+                 init_alpha=1.0, init_beta=1.0 if a.init == "oms" else 0.0, ebn0=tuple(a.ebn0))
+    v0 = tr.validation_loss(2.0)
+    t0 = time.time()
+    tr.train(a.frames, qat_fraction=a.qat)
+    dt = time.time() - t0
+    v1 = tr.validation_loss(2.0)
+    off, sc = tr.constants()
+    tr.close()
+    evals = []
+    for e in a.eval_ebn0:
+        row = {"ebn0_db": e}
+        for name, kind, c in (("oms", "OMS", None), ("learned", "LEARNED", (off, sc))):
+            r = evaluate(code, kind, a.iters, e, a.eval_frames, constants=c, early_stop=True)
+            row[name] = {"fer": r["fer"], "frame_errors": r["frame_errors"], "ber": r["ber"],
+                         "mean_iters": r["mean_iters"]}
+        evals.append(row)
+    meta = {"code": a.code, "iterations": a.iters, "frames": a.frames, "batch": a.batch, "ebn0_db": list(a.ebn0),
+            "loss": a.loss, "weights": a.weights, "init": a.init, "qat_fraction": a.qat, "lr": a.lr, "seed": a.seed,
+            "train_seconds": round(dt, 2), "validation_loss_2db": [v0, v1],
+            "evaluation": evals, "evaluation_frames": a.eval_frames}
+    import json
+    print(json.dumps(meta), flush=True)
+    if a.out:
+        save_constants(a.out, off, sc, **meta)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

@@ -189,7 +189,11 @@ int ldpc_decode_noalloc(const ldpc_code* code, int kind, int pack, const int8_t*
  * (int8) and scales[2t+g] (Q1.7, 128 = 1.0) give the check-to-variable magnitude
  * clamp(floor(min * scale / 128) - offset, 0, 31); iterations past n_iters reuse
  * the last row.  scale 128 / offset 1 everywhere is OMS without its first-iteration
- * quirk.  Trained by fast_ldpc_decoder_for_gpu_fixed_b200/learned.py. */
+ * quirk.  LDPC_PACK_F16X2 decoders (and the QC path, which is fp16) compute the
+ * magnitude arithmetically and accept scales that are multiples of 8 (a 1/16
+ * grid) and offsets in [-31, 31] only (LDPC_ERR_UNSUPPORTED otherwise); the
+ * other packings take any constants.  Trained by
+ * fast_ldpc_decoder_for_gpu_fixed_b200/learned.py, which quantises to that grid. */
 int ldpc_decoder_set_learned(ldpc_decoder* dec, int n_iters, const int8_t* offsets,
                              const uint8_t* scales);
 

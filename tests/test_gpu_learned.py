@@ -12,10 +12,11 @@ from fast_ldpc_decoder_for_gpu_fixed_b200.codes import qc_regular
 pytestmark = pytest.mark.gpu
 
 
-def _tables(its, seed):
+def _tables(its, seed, step=1):
+    """Random constants; step=8 puts the scales on the 1/16 grid the fp16 kernels take."""
     rng = np.random.default_rng(seed)
     off = rng.integers(0, 4, size=(its, 2)).astype(np.int8)
-    sc = rng.integers(72, 129, size=(its, 2)).astype(np.uint8)
+    sc = (rng.integers(72 // step, 128 // step + 1, size=(its, 2)) * step).astype(np.uint8)
     return off, sc
 
 
@@ -37,7 +38,7 @@ def _gpu(code, llr, iters, words, pack, off, sc):
 def test_learned_level_kernels(cuda, name, pack):
     code = load_table(name)
     words = 8
-    off, sc = _tables(7, 3)
+    off, sc = _tables(7, 3, step=8 if pack == "F16X2" else 1)
     oracle.set_learned(off, sc)
     for inp in ("awgn", "uniform"):
         llr = make_llr(inp, 4 * words * code.n, 5, sigma=llr_gen.sigma_for(1.5, 0.5))
@@ -49,7 +50,7 @@ def test_learned_level_kernels(cuda, name, pack):
 def test_learned_qc_kernel(cuda):
     code = qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
     words = 10
-    off, sc = _tables(10, 4)
+    off, sc = _tables(10, 4, step=8)
     oracle.set_learned(off, sc)
     llr = make_llr("awgn", 4 * words * code.n, 6, sigma=llr_gen.sigma_for(1.5, 0.5))
     got, info = _gpu(code, llr, 10, words, "AUTO", off, sc)
@@ -75,3 +76,30 @@ def test_learned_requires_constants(cuda):
         dec.decode_device(d, d, 2, 5)
     with pytest.raises(LdpcError):
         dec.set_learned(np.zeros((33, 2)), np.zeros((33, 2)))
+
+
+def test_fp16_learned_needs_the_sixteenth_grid(cuda):
+    code = load_table("576x288")
+    dec = Decoder(code, "LEARNED", nb_frames=2, pack="F16X2")
+    with pytest.raises(LdpcError) as e:
+        dec.set_learned(np.ones((2, 2)), np.full((2, 2), 100))
+    assert e.value.code == -3
+    with pytest.raises(LdpcError):
+        dec.set_learned(np.full((2, 2), 40), np.full((2, 2), 128))
+    dec.set_learned(np.full((2, 2), -31), np.full((2, 2), 248))
+    dec.close()
+    dec = Decoder(code, "LEARNED", nb_frames=2, pack="SIMD4")
+    dec.set_learned(np.ones((2, 2)), np.full((2, 2), 100))   # tables take any constants
+    dec.close()
+
+
+def test_fp16_learned_extreme_constants(cuda):
+    """The arithmetic fp16 magnitude against the oracle's table at the corners of its range."""
+    code = load_table("1944x972")
+    words = 6
+    off = np.array([[-31, 31], [0, -5], [3, 0], [-1, 1]], dtype=np.int8)
+    sc = np.array([[248, 8], [128, 200], [64, 136], [240, 96]], dtype=np.uint8)
+    oracle.set_learned(off, sc)
+    llr = make_llr("uniform", 4 * words * code.n, 21)
+    got, _ = _gpu(code, llr, 9, words, "F16X2", off, sc)
+    assert np.array_equal(got, oracle.decode(code, "LEARNED", llr, 9, interleaved=False)["hard"])

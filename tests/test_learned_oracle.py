@@ -72,9 +72,11 @@ def test_quantized_forward_is_the_int8_learned_decoder(name):
 
 
 def test_quantize_rounds_and_saturates():
-    off, sc = quantize([[1.0, 0.5], [2.5, -0.1]], [[0.6, -200.0], [1.49, 300.0]])
-    assert off.tolist() == [[1, -128], [1, 127]]
+    off, sc = quantize([[1.0, 0.5], [2.5, -0.1]], [[0.6, -200.0], [1.49, 300.0]], scale_step=1)
+    assert off.tolist() == [[1, -31], [1, 31]]
     assert sc.tolist() == [[128, 64], [255, 0]]
+    _, sc8 = quantize([[0.96, 0.91], [2.5, 0.0]], [[0, 0], [0, 0]])   # the fp16 kernels' 1/16 grid
+    assert sc8.tolist() == [[120, 120], [248, 0]]
 
 
 def test_float32_forward_stays_close_to_float64():
