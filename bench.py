@@ -1,17 +1,23 @@
 #!/usr/bin/env python
 """Decoded info Gbit/s of the fixed-point LDPC decoder on B200 GPUs.
 
-Workload (one step = one decode of one batch):
+Default workload (the metric: learned-offset decoder vs plain OMS at equal FER):
   seeded regular (3,6) QC-LDPC, 8x16 base of Z=256 circulants (N=4096, K=2048,
   4-cycle free), random info bits through the systematic encoder, BPSK over AWGN
-  at Eb/N0 = 2.0 dB, int8 LLRs quantised like the reference channel
+  at Eb/N0 = 2.25 dB, int8 LLRs quantised like the reference channel
   (q = trunc(clamp(8y, -31, 31)), awgn_channel/CChanel_AWGN_SIMD.cu:21-24),
-  offset-min-sum (offset 1), 10 layered iterations, 65536 frames per GPU.
-
-  value : kernel-only throughput, LLRs already resident in HBM (268 MB per batch,
-          larger than the 126 MB L2, so no flush is needed between steps)
-  e2e   : the same metric through the reference-facing host call
-          (ldpc_decode_host: pinned host LLRs in, 0/1 bytes out, copies timed)
+  65536 frames per GPU, at most 10 layered iterations.
+  value      : the deployed learned-offset decoder (LDPC_LEARNED with the constants in
+               fast_ldpc_decoder_for_gpu_fixed_b200/trained/qc3x6_z256_T10.json,
+               syndrome early stop per 4-frame word), kernel only, LLRs resident in HBM
+  plain_oms  : the plain 8-bit OMS kernel (offset 1, 10 fixed iterations) on the same
+               batch and GPU; vs_plain_oms = value / plain_oms.value
+  fer        : both decoders on 2^20 further frames at the same Eb/N0 (untimed)
+  e2e        : the learned decoder through the reference-facing host call
+               (ldpc_decode_host: pinned host LLRs in, 0/1 bytes out, copies timed)
+Other workloads: --workload oms (plain OMS, fixed iterations), --table NAME (a
+reference H table, all-zero codeword), --workload ira (N=64800 IRA code, one frame
+per CTA, early stop, at most 50 iterations, 2048 frames).
 
 python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 Multi-GPU: torchrun ... bench.py --gpus N (weak scaling: every rank decodes its own batch).
@@ -30,7 +36,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "qc(3,6) N=4096 K=2048 Z=256 OMS offset1 10 layered iterations, 65536 frames, Eb/N0 2.0 dB"
+WORKLOAD = "qc(3,6) N=4096 K=2048 Z=256, 65536 frames, Eb/N0 %.2f dB: learned-offset int8 decoder with early stop " \
+           "(max %d layered iterations) vs plain OMS offset 1, %d fixed iterations"
+TRAINED = os.path.join(ROOT, "fast_ldpc_decoder_for_gpu_fixed_b200", "trained", "qc3x6_z256_T10.json")
 
 
 def parse():
@@ -43,14 +51,25 @@ def parse():
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--kind", default="OMS")
     ap.add_argument("--pack", default="AUTO")
-    ap.add_argument("--ebn0", type=float, default=2.0)
+    ap.add_argument("--ebn0", type=float, default=None, help="default 2.25 dB (learned), 2.0 (oms, table), 1.4 (ira)")
+    ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira"])
+    ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
+    ap.add_argument("--fer-frames", type=int, default=1 << 20)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qc", action="store_true", help="use the level-scheduled kernel even for the QC code")
     ap.add_argument("--table", default=None,
                     help="decode a reference H table (e.g. 4000x2000) with the all-zero codeword instead of the QC workload")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.table:
+        a.workload = "oms"
+    if a.ebn0 is None:
+        a.ebn0 = {"learned": 2.25, "oms": 2.0, "ira": 1.4}[a.workload]
+    if a.workload == "ira":
+        a.frames = min(a.frames, 2048) if a.frames != 65536 else 2048
+        a.iters = 50 if a.iters == 10 else a.iters
+    return a
 
 
 class _AllZero:
@@ -64,13 +83,16 @@ class _AllZero:
         return np.zeros((info.shape[0], self.n), dtype=np.uint8)
 
 
-def make_workload(frames, ebn0, seed, rank=0, table=None):
+def make_workload(frames, ebn0, seed, rank=0, table=None, workload="learned"):
     """Codewords + quantised channel LLRs (int8, frame-major) for `frames` frames."""
-    from fast_ldpc_decoder_for_gpu_fixed_b200.codes import Encoder, load_table, qc_regular
+    from fast_ldpc_decoder_for_gpu_fixed_b200.codes import Encoder, IRAEncoder, ira, load_table, qc_regular
     if table:
         code = load_table(table)
         enc = _AllZero(code)
         enc.n = code.n
+    elif workload == "ira":
+        code = ira()
+        enc = IRAEncoder(code)
     else:
         code = qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
         enc = Encoder(code)
@@ -159,28 +181,67 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    code, enc, cws, idx, llr, sigma = make_workload(min(args.frames, 65536), args.ebn0, args.seed)
+    code, enc, cws, idx, llr, sigma = make_workload(min(args.frames, 65536), args.ebn0, args.seed, 0, args.table,
+                                                    args.workload)
+    kind = "OMS" if args.workload == "learned" else args.kind   # the reference's best plain decoder
     per_step = max(1.0, 60.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
-        cpu_baseline(code, llr, args.iters, args.kind, min(per_step, 2.0), enc.k)
+        cpu_baseline(code, llr, args.iters, kind, min(per_step, 2.0), enc.k)
     vals, samples = [], []
     cores = os.cpu_count() or 1
     for _ in range(args.steps):
-        v, cores, s = cpu_baseline(code, llr, args.iters, args.kind, per_step, enc.k)
+        v, cores, s = cpu_baseline(code, llr, args.iters, kind, per_step, enc.k)
         vals.append(v)
         samples.append(s)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 4096 * 1000.0 / (value * 1e9) * 1e3 * 0 + (65536 * enc.k / (value * 1e9)) * 1e3,
+            "ms_per_step": llr.shape[0] * enc.k / (value * 1e9) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic (seeded QC codewords, AWGN)",
-            "config": {"workload": WORKLOAD, "l2": "inputs larger than L2"},
+            "config": {"workload": workload_name(args), "l2": "host CPU run", "kind": kind},
             "cpu_baseline": {"value": value, "unit": "Gbit/s", "cores": cores, "kind": "port",
                              "sample": samples[-1]},
             "e2e": {"value": value, "unit": "Gbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_name(args):
+    if args.workload == "learned":
+        return WORKLOAD % (args.ebn0, args.iters, args.iters)
+    if args.table:
+        return "reference table %s, all-zero codeword, %s, %d iterations, %d frames, Eb/N0 %.2f dB" % (
+            args.table, args.kind, args.iters, args.frames, args.ebn0)
+    if args.workload == "ira":
+        return "IRA N=64800 K=32400 (groups of 360, 1/5 degree 8), %s with early stop, max %d iterations, " \
+               "%d frames, Eb/N0 %.2f dB" % (args.kind, args.iters, args.frames, args.ebn0)
+    return "qc(3,6) N=4096 K=2048 Z=256 %s, %d layered iterations, %d frames, Eb/N0 %.2f dB" % (
+        args.kind, args.iters, args.frames, args.ebn0)
+
+
+def _timed(step, steps, stream, flush):
+    """Device time (ms) of `steps` calls of step(), bracketed by CUDA events on `stream`;
+    with `flush` the 126 MB L2 is overwritten (256 MB) between steps, outside the timed spans."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if flush:
+        scratch = torch.empty(256 * 2**20, dtype=torch.uint8, device="cuda")
+        total = 0.0
+        for k in range(steps):
+            scratch.fill_(k & 0xFF)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def main():
@@ -189,7 +250,8 @@ def main():
         return run_reference(args)
     import torch
     import torch.distributed as dist
-    from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib, replicas
+    from fast_ldpc_decoder_for_gpu_fixed_b200.learned import evaluate, load_constants
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -198,70 +260,95 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    code, enc, cws, idx, llr, sigma = make_workload(args.frames, args.ebn0, args.seed, rank, args.table)
+    code, enc, cws, idx, llr, sigma = make_workload(args.frames, args.ebn0, args.seed, rank, args.table,
+                                                    args.workload)
     code.no_qc = args.no_qc
     words = args.frames // 4
-    dec = Decoder(code, args.kind, nb_frames=words, pack=args.pack)
+    learned = args.workload == "learned"
+    early = args.workload in ("learned", "ira")
+    constants = load_constants(TRAINED)[:2] if learned else None
+    kind = "LEARNED" if learned else args.kind
+    dec = Decoder(code, kind, nb_frames=words, pack=args.pack, early_stop=early)
+    if constants is not None:
+        dec.set_learned(*constants)
+    if early and args.slack is not None:
+        dec.set_early_stop(True, args.slack)
     info = dec.info()
+    per_frame = info["path"] == 3
     stream = torch.cuda.current_stream()
     d_llr = torch.from_numpy(llr.reshape(-1)).cuda()
     d_out = torch.empty(args.frames * code.n, dtype=torch.uint8, device="cuda")
-    launches = 0
+    d_its = torch.zeros(args.frames if per_frame else words, dtype=torch.int32, device="cuda")
 
     def step():
-        dec.decode_device(d_llr, d_out, words, args.iters, _lib.OUT_BYTES, None, stream)
+        dec.decode_device(d_llr, d_out, words, args.iters, _lib.OUT_BYTES, d_its, stream)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    # error rates of this batch (not timed)
+    # error rates and iterations of this batch (not timed; every step decodes the same batch)
     hard = d_out.view(args.frames, code.n)
     ref_bits = torch.from_numpy(cws).cuda()[torch.from_numpy(idx).cuda()]
     err = (hard != ref_bits).sum(dim=1)
     fer = float((err > 0).float().mean())
     ber = float(err.sum()) / (args.frames * code.n)
+    mean_iters = float(d_its.float().mean()) if early else float(args.iters)
     del ref_bits, err, hard
 
-    sampler = ClockSampler(local)
-    # inputs smaller than twice the 126 MB L2: flush it between steps, outside the timed spans
     flush = llr.nbytes < 2 * 126 * 2**20
-    scratch = torch.empty(256 * 2**20, dtype=torch.uint8, device="cuda") if flush else None
+    sampler = ClockSampler(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if flush:
-        ms_sum = 0.0
-        for k in range(args.steps):
-            scratch.fill_(k & 0xFF)
-            e0.record(stream)
-            step()
-            e1.record(stream)
-            e1.synchronize()
-            ms_sum += e0.elapsed_time(e1)
-            launches += 1
-        torch.cuda.synchronize()
-        clocks = sampler.stop()
-    else:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-            launches += 1
-        e1.record(stream)
-        torch.cuda.synchronize()
-        clocks = sampler.stop()
-    ms = ms_sum if flush else e0.elapsed_time(e1)
-    from fast_ldpc_decoder_for_gpu_fixed_b200 import replicas
+    ms = _timed(step, args.steps, stream, flush)
+    clocks = sampler.stop()
+    launches = args.steps
     ms_max = replicas.max_over_ranks(ms, device="cuda")
     ms_step = ms_max / args.steps
     info_bits = args.frames * enc.k
     value = world * info_bits * args.steps / (ms_max * 1e-3) / 1e9
 
-    # roofline of the decode kernel (one launch per step)
-    edge_updates = args.frames * code.e * args.iters
+    # the plain 8-bit OMS kernel on the same batch and GPU (the metric's comparison)
+    plain = None
+    if learned:
+        pdec = Decoder(code, "OMS", nb_frames=words, pack=args.pack)
+
+        def pstep():
+            pdec.decode_device(d_llr, d_out, words, args.iters, _lib.OUT_BYTES, None, stream)
+
+        for _ in range(args.warmup):
+            pstep()
+        torch.cuda.synchronize()
+        pms = replicas.max_over_ranks(_timed(pstep, args.steps, stream, flush), device="cuda")
+        launches += args.steps
+        hard = d_out.view(args.frames, code.n)
+        ref_bits = torch.from_numpy(cws).cuda()[torch.from_numpy(idx).cuda()]
+        perr = (hard != ref_bits).sum(dim=1)
+        plain = {"value": world * info_bits * args.steps / (pms * 1e-3) / 1e9, "unit": "Gbit/s",
+                 "ms_per_step": pms / args.steps, "kernel": "qc_register_messages" if pdec.info()["path"] == 1
+                 else "level_scheduled", "iterations": args.iters, "batch_fer": float((perr > 0).float().mean()),
+                 "batch_ber": float(perr.sum()) / (args.frames * code.n)}
+        del ref_bits, perr, hard
+        pdec.close()
+
+    # equal-FER evidence on more frames (untimed)
+    fer_cmp = None
+    if learned and rank == 0 and args.fer_frames > 0:
+        fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=True)
+        fp = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames)
+        fer_cmp = {"frames": fl["frames"], "ebn0_db": args.ebn0,
+                   "learned_early_stop": {"fer": fl["fer"], "frame_errors": fl["frame_errors"], "ber": fl["ber"],
+                                          "mean_iters": fl["mean_iters"]},
+                   "plain_oms": {"fer": fp["fer"], "frame_errors": fp["frame_errors"], "ber": fp["ber"]}}
+
+    # roofline of the decode kernel (one launch per step), from the iterations it executed
     int_peak = _int_peak()
-    alg_ops = 2.0 * edge_updates          # 8 int8 lane-ops per edge-update at 4 lanes per 32-bit word
+    if per_frame:
+        edge_updates = float(d_its.sum().item()) * code.e
+    else:
+        edge_updates = float(d_its.sum().item()) * 4 * code.e if early else float(args.frames) * code.e * args.iters
+    alg_ops = (1.0 if per_frame else 2.0) * edge_updates
     achieved = alg_ops / (ms_step * 1e-3) / 1e12
     hbm_bytes = args.frames * code.n * 2  # int8 LLRs in + 0/1 bytes out
     peaks = _measured_peaks()
@@ -272,27 +359,36 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1:
-        v, cores, sample = cpu_baseline(code, llr, args.iters, args.kind, args.cpu_seconds, enc.k)
+        ckind = "OMS" if learned else args.kind
+        v, cores, sample = cpu_baseline(code, llr, min(args.iters, 10) if args.workload == "ira" else args.iters,
+                                        ckind, args.cpu_seconds, enc.k)
         cpu = {"value": v, "unit": "Gbit/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
+        kernel = {0: "level_scheduled", 1: "qc_register_messages", 2: "level_scheduled_2f",
+                  3: "frame_per_cta_packed_rows"}[info["path"]]
+        workload = workload_name(args)
         line = {
             "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int8",
-            "data": "synthetic (seeded QC codewords, AWGN, reference quantiser)",
-            "config": {"workload": WORKLOAD if not args.table else
-                       "reference table %s, all-zero codeword, %s, %d iterations, %d frames, Eb/N0 %.1f dB" % (
-                           args.table, args.kind, args.iters, args.frames, args.ebn0), "kind": args.kind, "pack": info["pack"], "frames_per_gpu": args.frames,
-                       "iterations": args.iters, "ebn0_db": args.ebn0, "fer": fer, "ber": ber,
-                       "l2": ("inputs %d MB: L2 flushed (256 MB write) between steps, outside the timed spans" % (llr.nbytes // 2**20))
-                       if flush else "inputs (%d MB) larger than the 126 MB L2; no flush" % (llr.nbytes // 2**20), "parallelism": "replicas" if world > 1 else "1gpu",
-                       "threads_per_cta": info["threads"], "smem_per_cta": info["smem"],
-                       "ctas_per_sm": info["ctas_per_sm"], "regs": info["regs"],
-                       "kernel": {0: "level_scheduled", 1: "qc_register_messages", 2: "level_scheduled_2f"}[info["path"]]},
+            "data": "synthetic (seeded codewords, AWGN, reference quantiser)",
+            "config": {"workload": workload, "kind": kind, "pack": info["pack"], "frames_per_gpu": args.frames,
+                       "max_iterations": args.iters, "early_stop": early, "mean_iterations": mean_iters,
+                       "ebn0_db": args.ebn0, "batch_fer": fer, "batch_ber": ber,
+                       "l2": ("inputs %d MB: L2 flushed (256 MB write) between steps, outside the timed spans" % (
+                           llr.nbytes // 2**20)) if flush else
+                       "inputs (%d MB) larger than the 126 MB L2; no flush" % (llr.nbytes // 2**20),
+                       "parallelism": "replicas" if world > 1 else "1gpu", "threads_per_cta": info["threads"],
+                       "smem_per_cta": info["smem"], "ctas_per_sm": info["ctas_per_sm"], "regs": info["regs"],
+                       "kernel": kernel},
+            "plain_oms": plain,
+            "vs_plain_oms": value / plain["value"] if plain else None,
+            "fer": fer_cmp,
             "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
                          "frac": achieved / int_peak, "traffic": None,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
+                         "ops_per_edge_update": 1.0 if per_frame else 2.0,
                          "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, all SMs)"},
             "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
                              "unit": "GB/s", "frac": (hbm_bytes / (ms_step * 1e-3) / 1e9) / peaks["hbm_gbs"]

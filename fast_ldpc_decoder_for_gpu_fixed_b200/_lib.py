@@ -16,6 +16,7 @@ KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 
 PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2, "FRAME": 3}
 OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
+BATCH_GRAPH = 2
 EARLY_STOP_DEFAULT_SLACK = 128
 TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2
 
@@ -38,6 +39,13 @@ SIGNATURES = {
     "ldpc_decoder_set_learned": (_I, [_P, _I, _P, _P]),
     "ldpc_decoder_set_early_stop": (_I, [_P, _I, _I]),
     "ldpc_decoder_destroy": (_I, [_P]),
+    "ldpc_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I, _I, _I]),
+    "ldpc_batch_decode": (_I, [_P, _P, _P, _P, _I, _I, _P, _P]),
+    "ldpc_batch_autotune": (_I, [_P, _P, _P, _P, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    "ldpc_batch_set_learned": (_I, [_P, _I, _P, _P]),
+    "ldpc_batch_set_early_stop": (_I, [_P, _I, _I]),
+    "ldpc_batch_info": (_I, [_P, _P]),
+    "ldpc_batch_destroy": (_I, [_P]),
     "ldpc_train_step": (_I, [_P, _P, _P, _P, _SZ, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ldpc_train_stash_bytes": (_SZ, [_P, _SZ, _I]),
     "ldpc_last_error_string": (ctypes.c_char_p, []),

@@ -403,17 +403,19 @@ __device__ __forceinline__ void row_update(typename PK::S* app, typename PK::S* 
     }
 }
 
+// Decodes word g (4 frames) with the level schedule, all state in the CTA's shared
+// memory (smem_raw: APP, messages, then the LEARNED table).  Every thread of the
+// CTA calls it; it has no barrier after its last shared-memory access, so a
+// caller that reuses the memory synchronises first.
 template <class PK, int KIND, int DT, bool EXACT>
-__global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const Job J)
+__device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, long long g, unsigned char* smem_raw,
+                                                   unsigned* s_odd)
 {
     using S = typename PK::S;
     using R = typename PK::R;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     S* app = reinterpret_cast<S*>(smem_raw);
     S* msg = app + PK::WPC * P.npad;
     uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + PK::WPC * sizeof(S) * ((size_t)P.npad + (size_t)P.dmax * P.m));
-    const long long g = J.word0 + blockIdx.x;
-    __shared__ unsigned s_odd[2];
     if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
 
     read_group(P, J, g, [&](int v, uint32_t w) { Access<PK>::put(app, P.npad, v, w); });
@@ -464,6 +466,14 @@ __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const 
                 mo[(long long)P.edge_orig[i] * J.total_words + g] = Access<PK>::get_msg(msg, mstride, i);
         }
     }
+}
+
+template <class PK, int KIND, int DT, bool EXACT>
+__global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const Job J)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_odd[2];
+    decode_word_levels<PK, KIND, DT, EXACT>(P, J, J.word0 + blockIdx.x, smem_raw, s_odd);
 }
 
 // The level-scheduled kernel for PackF16x2h: a CTA holds frames 2h, 2h+1 of word g

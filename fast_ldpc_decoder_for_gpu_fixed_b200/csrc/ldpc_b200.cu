@@ -583,14 +583,11 @@ static uint16_t half_bits(double x)
     return (uint16_t)(sign | ((e + 15) << 10) | ((int)((a - 1.0) * 1024.0 + 0.5) & 0x3ff));
 }
 
-extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8_t* offsets, const uint8_t* scales)
+// LDPC_LEARNED magnitude tables [n_iters][2][128] for the packing (fp16: (k, b) pairs)
+static int build_learned_lut(bool fp16, int n_iters, const int8_t* offsets, const uint8_t* scales,
+                             std::vector<uint16_t>& lut)
 {
-    if (!d || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: null pointer");
-    if (d->kind != LDPC_LEARNED) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: decoder kind is not LDPC_LEARNED");
-    if (n_iters < 1 || n_iters > LDPC_LEARNED_MAX_ITERS)
-        return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: n_iters must be in [1, %d]", LDPC_LEARNED_MAX_ITERS);
-    const bool fp16 = d->pack == LDPC_PACK_F16X2;
-    std::vector<uint16_t> lut((size_t)n_iters * 256, 0);
+    lut.assign((size_t)n_iters * 256, 0);
     if (fp16) {
         // the fp16 kernels compute floor(min * s / 128) - offset as round(min * k + b) with
         // k = s / 128, b = -offset - 15/32 (packs.cuh, h2::mags): exact when k has at most 4
@@ -617,6 +614,18 @@ extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8
                     lut[(size_t)t * 256 + g * 128 + m] = (uint16_t)(c < 0 ? 0 : (c > 31 ? 31 : c));
                 }
     }
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8_t* offsets, const uint8_t* scales)
+{
+    if (!d || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: null pointer");
+    if (d->kind != LDPC_LEARNED) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: decoder kind is not LDPC_LEARNED");
+    if (n_iters < 1 || n_iters > LDPC_LEARNED_MAX_ITERS)
+        return fail(LDPC_ERR_ARG, "ldpc_decoder_set_learned: n_iters must be in [1, %d]", LDPC_LEARNED_MAX_ITERS);
+    std::vector<uint16_t> lut;
+    int rc = build_learned_lut(d->pack == LDPC_PACK_F16X2, n_iters, offsets, scales, lut);
+    if (rc) return rc;
     if (!d->d_lut) CUDA_TRY(cudaMalloc(&d->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
     CUDA_TRY(cudaMemcpy(d->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
     d->lut_its = n_iters;
@@ -885,6 +894,331 @@ extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
 // receive chains and plugin hosts that reserve all GPU memory at start-up, where
 // cudaMalloc can stall for milliseconds, cudaFree synchronises the whole device,
 // and a framework-owned memory pool may refuse the request outright.  For them,
+// ------------------------------------------------------------------------
+// batches of several codes: one persistent kernel (batch_kernel.cu)
+// ------------------------------------------------------------------------
+
+namespace ldpc {
+const void* kernel_table_batch(int pack, int kind, int variant);
+size_t batch_code_bytes();
+void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, long long words,
+                     long long first_item, int quirk, int out_packed);
+}  // namespace ldpc
+
+struct ldpc_batch {
+    int kind = 0, device = 0, pack = LDPC_PACK_SIMD4, variant = 0;
+    bool early = false, use_graph = false;
+    unsigned slack = LDPC_EARLY_STOP_DEFAULT_SLACK;
+    std::vector<ldpc_decoder*> plans;  // each code's tables and schedule (decoder_setup)
+    void* d_codes = nullptr;           // BatchCode[n]
+    void* h_codes = nullptr;           // pinned staging of the same
+    unsigned long long* d_counter = nullptr;
+    const void* kfn = nullptr;
+    int threads = 128, smem = 0, ctas_per_sm = 0, grid = 0, sms = 0;
+    uint16_t* d_lut = nullptr;
+    int lut_its = 0;
+    std::vector<int8_t> off;
+    std::vector<uint8_t> sc;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uintptr_t> key;     // what the captured graph was made for
+    std::vector<uintptr_t> staged;  // what the staged records describe
+    cudaEvent_t done = nullptr;  // the last launch (h_codes may be rewritten after it)
+};
+
+static void batch_free(ldpc_batch* b)
+{
+    if (!b) return;
+    for (auto* d : b->plans) decoder_free(d);
+    cudaFree(b->d_codes);
+    cudaFreeHost(b->h_codes);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_lut);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->done) cudaEventDestroy(b->done);
+    delete b;
+}
+
+static size_t batch_smem(const ldpc_batch* b, int pack)
+{
+    size_t s = 0;
+    for (auto* d : b->plans)
+        s = std::max(s, smem_bytes(pack, d->plan.npad, d->plan.dmax, d->plan.m));
+    return s + (b->kind == LDPC_LEARNED ? 512 : 0);
+}
+
+// selects packing, CTA width and resident CTAs per SM (0 = as many as fit)
+static int batch_configure(ldpc_batch* b, int pack, int threads, int ctas_per_sm)
+{
+    const int k = b->kind == LDPC_LEARNED ? 4 : b->kind;
+    const void* kfn = kernel_table_batch(pack, k, b->variant);
+    if (!kfn) return fail(LDPC_ERR_UNSUPPORTED, "batch: no kernel for pack %d", pack);
+    int smem_max = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+    const size_t smem = batch_smem(b, pack);
+    if (smem > (size_t)smem_max)
+        return fail(LDPC_ERR_UNSUPPORTED, "batch: the largest code needs %zu B of shared memory with pack %d", smem, pack);
+    if (b->kind == LDPC_LEARNED && !b->off.empty()) {
+        std::vector<uint16_t> lut;
+        int rc = build_learned_lut(pack == LDPC_PACK_F16X2, b->lut_its, b->off.data(), b->sc.data(), lut);
+        if (rc) return rc;
+        if (!b->d_lut) CUDA_TRY(cudaMalloc(&b->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
+        CUDA_TRY(cudaMemcpy(b->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    }
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
+    if (occ < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch: kernel cannot be resident (%zu B, %d threads)", smem, threads);
+    b->pack = pack;
+    b->kfn = kfn;
+    b->threads = threads;
+    b->smem = (int)smem;
+    b->ctas_per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ) : occ;
+    b->grid = b->ctas_per_sm * b->sms;
+    b->key.clear();  // a captured graph no longer matches
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes, int n_codes, int kind, int pack,
+                                 int flags)
+{
+    if (!out || !codes || n_codes < 1) return fail(LDPC_ERR_ARG, "ldpc_batch_create: no codes");
+    if (kind < LDPC_MS || kind > LDPC_LEARNED || kind == LDPC_XMS)
+        return fail(LDPC_ERR_ARG, "ldpc_batch_create: kind %d (xMS reads interleaved input; use OMS)", kind);
+    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_BATCH_GRAPH)) return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
+    if ((flags & LDPC_FLAG_EARLY_STOP) && kind == LDPC_2NMS)
+        return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
+    if (pack != LDPC_PACK_AUTO && (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8))
+        return fail(LDPC_ERR_ARG, "ldpc_batch_create: pack %d (SIMD4, F16X2, I8 or AUTO)", pack);
+    int dmax = 0;
+    for (int i = 0; i < n_codes; i++) {
+        if (!codes[i]) return fail(LDPC_ERR_ARG, "ldpc_batch_create: null code %d", i);
+        dmax = std::max(dmax, codes[i]->dmax);
+    }
+    if (dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", dmax, kMaxDegree);
+    ldpc_batch* b = new ldpc_batch();
+    b->kind = kind;
+    b->early = flags & LDPC_FLAG_EARLY_STOP;
+    b->use_graph = flags & LDPC_BATCH_GRAPH;
+    b->variant = dmax <= 8 ? 0 : (dmax <= 16 ? 1 : 2);
+    cudaError_t e = cudaGetDevice(&b->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_codes, batch_code_bytes() * n_codes);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_codes, batch_code_bytes() * n_codes);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return fail(LDPC_ERR_CUDA, "ldpc_batch_create: %s", cudaGetErrorString(e));
+    }
+    for (int i = 0; i < n_codes; i++) {
+        ldpc_decoder* d = new ldpc_decoder();
+        b->plans.push_back(d);
+        int rc = decoder_setup(d, codes[i]);
+        if (rc) {
+            batch_free(b);
+            return rc;
+        }
+    }
+    int rc = LDPC_ERR_UNSUPPORTED;
+    const int order[3] = {LDPC_PACK_SIMD4, LDPC_PACK_I8, LDPC_PACK_F16X2};
+    for (int i = 0; i < 3 && rc; i++) {
+        const int p = pack == LDPC_PACK_AUTO ? order[i] : pack;
+        rc = batch_configure(b, p, 128, 0);
+        if (pack != LDPC_PACK_AUTO) break;
+    }
+    if (rc) {
+        batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_set_learned(ldpc_batch* b, int n_iters, const int8_t* offsets, const uint8_t* scales)
+{
+    if (!b || !offsets || !scales) return fail(LDPC_ERR_ARG, "ldpc_batch_set_learned: null pointer");
+    if (b->kind != LDPC_LEARNED) return fail(LDPC_ERR_ARG, "ldpc_batch_set_learned: batch kind is not LDPC_LEARNED");
+    if (n_iters < 1 || n_iters > LDPC_LEARNED_MAX_ITERS)
+        return fail(LDPC_ERR_ARG, "ldpc_batch_set_learned: n_iters must be in [1, %d]", LDPC_LEARNED_MAX_ITERS);
+    b->off.assign(offsets, offsets + 2 * n_iters);
+    b->sc.assign(scales, scales + 2 * n_iters);
+    b->lut_its = n_iters;
+    int rc = batch_configure(b, b->pack, b->threads, b->ctas_per_sm);
+    if (rc) {
+        b->off.clear();
+        b->sc.clear();
+        b->lut_its = 0;
+    }
+    return rc;
+}
+
+extern "C" int ldpc_batch_set_early_stop(ldpc_batch* b, int enabled, int slack)
+{
+    if (!b) return fail(LDPC_ERR_ARG, "ldpc_batch_set_early_stop: null batch");
+    if (enabled && b->kind == LDPC_2NMS)
+        return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
+    if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_batch_set_early_stop: slack must be >= 0");
+    b->early = enabled != 0;
+    b->slack = (unsigned)slack;
+    b->key.clear();
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
+                                 int iters, int out_format, int32_t* const* d_iters_out, void* stream)
+{
+    if (!b || !d_llr || !d_out || !n_words) return fail(LDPC_ERR_ARG, "ldpc_batch_decode: null pointer");
+    if (iters < 1) return fail(LDPC_ERR_ARG, "ldpc_batch_decode: iterations must be >= 1 (got %d)", iters);
+    if (out_format != LDPC_OUT_BYTES && out_format != LDPC_OUT_PACKED)
+        return fail(LDPC_ERR_ARG, "ldpc_batch_decode: unknown output format %d", out_format);
+    if (b->kind == LDPC_LEARNED && b->off.empty())
+        return fail(LDPC_ERR_ARG, "LDPC_LEARNED batch: set its offsets and scales first");
+    if (b->use_graph && !stream)
+        return fail(LDPC_ERR_ARG, "LDPC_BATCH_GRAPH: pass a stream (the legacy default stream cannot be captured)");
+    const int n = (int)b->plans.size();
+    long long total = 0;
+    std::vector<uintptr_t> recs = {(uintptr_t)out_format};
+    for (int i = 0; i < n; i++) {
+        if (n_words[i] > 0 && (!d_llr[i] || !d_out[i]))
+            return fail(LDPC_ERR_ARG, "ldpc_batch_decode: null buffer for code %d", i);
+        total += (long long)n_words[i];
+        recs.push_back((uintptr_t)d_llr[i]);
+        recs.push_back((uintptr_t)d_out[i]);
+        recs.push_back((uintptr_t)n_words[i]);
+        recs.push_back((uintptr_t)(d_iters_out ? d_iters_out[i] : nullptr));
+    }
+    if (total == 0) return LDPC_OK;
+    std::vector<uintptr_t> key = recs;
+    for (uintptr_t x : {(uintptr_t)b->kfn, (uintptr_t)b->grid, (uintptr_t)b->threads, (uintptr_t)iters,
+                        (uintptr_t)b->early, (uintptr_t)b->slack, (uintptr_t)stream, (uintptr_t)b->d_lut})
+        key.push_back(x);
+    CUDA_TRY(cudaSetDevice(b->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (recs != b->staged) {
+        // the staging buffer may still feed the previous launch's copy
+        CUDA_TRY(cudaEventSynchronize(b->done));
+        b->staged = recs;
+        long long first = 0;
+        for (int i = 0; i < n; i++) {
+            batch_code_fill(static_cast<char*>(b->h_codes) + i * batch_code_bytes(), b->plans[i]->plan, d_llr[i],
+                            d_out[i], d_iters_out ? d_iters_out[i] : nullptr, (long long)n_words[i], first,
+                            b->kind == LDPC_OMS, out_format == LDPC_OUT_PACKED);
+            first += (long long)n_words[i];
+        }
+    }
+    Job J{};
+    J.iters = iters;
+    J.quirk = b->kind == LDPC_OMS;
+    J.early = b->early ? 1 : 0;
+    J.early_slack = b->slack;
+    J.lut = b->d_lut;
+    J.lut_its = b->lut_its;
+    void* codes = b->d_codes;
+    unsigned long long* counter = b->d_counter;
+    void* args[] = {(void*)&codes, (void*)&n, (void*)&counter, (void*)&total, (void*)&J};
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(b->d_codes, b->h_codes, batch_code_bytes() * n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess)
+            e = cudaLaunchKernel(b->kfn, dim3((unsigned)b->grid), dim3(b->threads), args, b->smem, st);
+        return e;
+    };
+    if (b->use_graph) {
+        if (!b->exec || key != b->key) {
+            if (b->exec) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = enqueue();
+            cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "ldpc_batch_decode: graph capture: %s", cudaGetErrorString(e));
+            b->key = key;
+        }
+        CUDA_TRY(cudaGraphLaunch(b->exec, st));
+    } else {
+        CUDA_TRY(enqueue());
+    }
+    CUDA_TRY(cudaEventRecord(b->done, st));
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, void* const* d_out,
+                                   const size_t* n_words, int iters, int32_t* const* d_iters_out, double* best_ms,
+                                   void* stream)
+{
+    if (!b) return fail(LDPC_ERR_ARG, "ldpc_batch_autotune: null batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    const int packs[3] = {LDPC_PACK_SIMD4, LDPC_PACK_F16X2, LDPC_PACK_I8};
+    const int widths[3] = {64, 128, 256};
+    double best = 1e30;
+    int bp = b->pack, bt = b->threads, bc = 0;
+    const bool graph = b->use_graph;
+    b->use_graph = false;  // time the launches themselves
+    for (int p : packs) {
+        for (int t : widths) {
+            for (int half = 0; half < 2; half++) {
+                if (batch_configure(b, p, t, 0)) continue;
+                const int ctas = half ? std::max(1, b->ctas_per_sm / 2) : b->ctas_per_sm;
+                if (half && ctas == b->ctas_per_sm) continue;
+                if (batch_configure(b, p, t, ctas)) continue;
+                int rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, stream);
+                if (rc) continue;
+                float ms = 0.f;
+                cudaEventRecord(e0, st);
+                for (int r = 0; r < 3 && !rc; r++)
+                    rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, stream);
+                cudaEventRecord(e1, st);
+                if (rc || cudaEventSynchronize(e1) != cudaSuccess) continue;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms / 3 < best) {
+                    best = ms / 3;
+                    bp = p;
+                    bt = t;
+                    bc = ctas;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->use_graph = graph;
+    int rc = batch_configure(b, bp, bt, bc);
+    if (rc) return rc;
+    if (best_ms) *best_ms = best;
+    return best < 1e30 ? LDPC_OK : fail(LDPC_ERR_UNSUPPORTED, "ldpc_batch_autotune: no configuration ran");
+}
+
+extern "C" int ldpc_batch_info(const ldpc_batch* b, int* info)
+{
+    if (!b || !info) return fail(LDPC_ERR_ARG, "ldpc_batch_info: null pointer");
+    info[0] = b->kind;
+    info[1] = b->pack;
+    info[2] = b->threads;
+    info[3] = b->smem;
+    info[4] = b->ctas_per_sm;
+    info[5] = b->grid;
+    info[6] = b->use_graph;
+    info[7] = (int)b->plans.size();
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_destroy(ldpc_batch* b)
+{
+    if (!b) return LDPC_OK;
+    cudaError_t e = cudaDeviceSynchronize();
+    batch_free(b);
+    if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "ldpc_batch_destroy: %s", cudaGetErrorString(e));
+    return LDPC_OK;
+}
+
 // ldpc_decode_noalloc decodes with the level-scheduled kernel and no allocation:
 // the per-code tables that ldpc_decoder_create puts in its own device buffers
 // (column table, row degrees, row groups, level list) go instead into the

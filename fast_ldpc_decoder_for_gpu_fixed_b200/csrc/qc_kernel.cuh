@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant
 #pragma unroll
             for (int j = 0; j < DT; j++)
                 if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
-            __syncthreads();
+            // with the early stop, the barrier of the odd-row count closes the last layer
+            if (!(ET && KIND != KIND_2NMS && l == L - 1)) __syncthreads();
         }
         executed = it + 1;
         if (KIND == KIND_2NMS && it >= 1) {

@@ -171,6 +171,73 @@ class Decoder:
             pass
 
 
+class Batch:
+    """Several codes decoded by one persistent kernel (ldpc_batch_*).  ``codes``: a
+    list of ``Code``; ``graph``: capture launches in a CUDA graph; buffers are
+    lists (one torch CUDA tensor per code)."""
+
+    def __init__(self, codes, kind="OMS", pack="AUTO", early_stop=False, graph=False):
+        self.codes = [c if isinstance(c, Code) else c.code for c in codes]
+        self.natives = [NativeCode(c) for c in self.codes]
+        self.kind = kind.upper()
+        arr = (ctypes.c_void_p * len(codes))(*[nc.handle.value for nc in self.natives])
+        h = ctypes.c_void_p()
+        flags = (_lib.FLAG_EARLY_STOP if early_stop else 0) | (_lib.BATCH_GRAPH if graph else 0)
+        _lib.check(_lib.lib().ldpc_batch_create(ctypes.byref(h), arr, len(codes), _lib.KINDS[self.kind],
+                                                _lib.PACKS[pack.upper()], flags))
+        self.handle = h
+
+    @staticmethod
+    def _arrays(d_llr, d_out, n_words, d_iters):
+        n = len(d_llr)
+        llr = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_llr])
+        out = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_out])
+        words = (ctypes.c_size_t * n)(*[int(w) for w in n_words])
+        its = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_iters]) if d_iters is not None else None
+        return llr, out, words, its
+
+    def decode(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None):
+        st = getattr(stream, "cuda_stream", stream)
+        llr, out, words, its = self._arrays(d_llr, d_out, n_words, d_iters)
+        _lib.check(_lib.lib().ldpc_batch_decode(self.handle, llr, out, words, int(iters), int(out_format), its, st))
+
+    def autotune(self, d_llr, d_out, n_words, iters, d_iters=None, stream=None):
+        """Picks the fastest packing / CTA width / residency on these inputs; returns ms per decode."""
+        st = getattr(stream, "cuda_stream", stream)
+        llr, out, words, its = self._arrays(d_llr, d_out, n_words, d_iters)
+        best = ctypes.c_double()
+        _lib.check(_lib.lib().ldpc_batch_autotune(self.handle, llr, out, words, int(iters), its,
+                                                  ctypes.byref(best), st))
+        return best.value
+
+    def set_learned(self, offsets, scales):
+        off = np.ascontiguousarray(offsets, dtype=np.int8).reshape(-1, 2)
+        sc = np.ascontiguousarray(scales, dtype=np.uint8).reshape(-1, 2)
+        _lib.check(_lib.lib().ldpc_batch_set_learned(self.handle, off.shape[0], off.ctypes.data, sc.ctypes.data))
+
+    def set_early_stop(self, enabled=True, slack=_lib.EARLY_STOP_DEFAULT_SLACK):
+        _lib.check(_lib.lib().ldpc_batch_set_early_stop(self.handle, int(bool(enabled)), int(slack)))
+
+    def info(self):
+        a = (ctypes.c_int * 8)()
+        _lib.check(_lib.lib().ldpc_batch_info(self.handle, a))
+        keys = ("kind", "pack", "threads", "smem", "ctas_per_sm", "grid", "graph", "codes")
+        return dict(zip(keys, list(a)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.lib().ldpc_batch_destroy(self.handle)
+            self.handle = None
+        for nc in getattr(self, "natives", []):
+            nc.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------------------
 # reference-compatible plugin classes
 # ---------------------------------------------------------------------------

@@ -238,6 +238,48 @@ int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
 
+/* ---- batches of codes (no reference counterpart) ------------------------ */
+
+/* A batch decodes frames of several codes (different lengths and rates) in one
+ * persistent kernel launch: resident CTAs take 4-frame words of any code from a
+ * shared counter, so uneven per-code frame counts and per-word iteration counts
+ * (LDPC_FLAG_EARLY_STOP) keep every SM busy.  Arithmetic and results per word are
+ * those of ldpc_decoder_create with the same kind and pack (level schedule).
+ * kind: any but LDPC_XMS; pack: LDPC_PACK_SIMD4 / F16X2 / I8, or AUTO (the
+ * smallest state that fits; ldpc_batch_autotune then picks the fastest).
+ * flags: LDPC_FLAG_EARLY_STOP, LDPC_BATCH_GRAPH (launches captured once in a CUDA
+ * graph and replayed while buffers, sizes and settings stay the same; needs a
+ * stream other than the legacy default stream).  The codes may be destroyed
+ * after this call. */
+typedef struct ldpc_batch ldpc_batch;
+#define LDPC_BATCH_GRAPH 2
+int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes, int n_codes, int kind, int pack, int flags);
+
+/* Decodes n_words[c] 4-frame words of every code c: d_llr[c] frame-major int8
+ * LLRs, d_out[c] hard decisions (LDPC_OUT_BYTES or LDPC_OUT_PACKED), optional
+ * d_iters_out[c] (iterations per word) or d_iters_out null.  Asynchronous on
+ * `stream`. */
+int ldpc_batch_decode(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
+                      int iters, int out_format, int32_t* const* d_iters_out, void* stream);
+
+/* Times the packings (SIMD4, F16X2, I8), CTA widths (64, 128, 256) and resident
+ * CTAs per SM (as many as fit, or half) on these inputs (outputs are
+ * overwritten), keeps the fastest and returns its time per decode in *best_ms. */
+int ldpc_batch_autotune(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
+                        int iters, int32_t* const* d_iters_out, double* best_ms, void* stream);
+
+/* LDPC_LEARNED constants of the batch (all codes), as ldpc_decoder_set_learned. */
+int ldpc_batch_set_learned(ldpc_batch* batch, int n_iters, const int8_t* offsets, const uint8_t* scales);
+
+/* Early stop on/off and its slack, as ldpc_decoder_set_early_stop. */
+int ldpc_batch_set_early_stop(ldpc_batch* batch, int enabled, int slack);
+
+/* info[0..7] = kind, pack, threads per CTA, shared bytes per CTA, resident CTAs
+ * per SM, grid (CTAs of the persistent launch), graph mode, number of codes */
+int ldpc_batch_info(const ldpc_batch* batch, int* info);
+
+int ldpc_batch_destroy(ldpc_batch* batch);
+
 /* ---- channel and error counting (the simulation stages around the decoder) */
 
 /* Noise deviation for an Eb/N0 (or Es/N0 when es_n0) in dB at code rate `rate`,
