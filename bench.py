@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--kind", default="OMS")
     ap.add_argument("--pack", default="AUTO")
     ap.add_argument("--ebn0", type=float, default=None, help="default 2.25 dB (learned), 2.0 (oms, table), 1.4 (ira)")
-    ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira"])
+    ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira", "batch"])
     ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
     ap.add_argument("--fer-frames", type=int, default=1 << 20)
     ap.add_argument("--seed", type=int, default=2024)
@@ -65,7 +65,10 @@ def parse():
     if a.table:
         a.workload = "oms"
     if a.ebn0 is None:
-        a.ebn0 = {"learned": 2.25, "oms": 2.0, "ira": 1.4}[a.workload]
+        a.ebn0 = {"learned": 2.25, "oms": 2.0, "ira": 1.4, "batch": 3.0}[a.workload]
+    if a.workload == "batch":
+        a.frames = 200000 if a.frames == 65536 else a.frames
+        a.iters = 20 if a.iters == 10 else a.iters
     if a.workload == "ira":
         a.frames = min(a.frames, 2048) if a.frames != 65536 else 2048
         a.iters = 50 if a.iters == 10 else a.iters
@@ -207,6 +210,108 @@ def run_reference(args):
     return 0
 
 
+def batch_codes():
+    """The mixed batch: four seeded irregular QC codes with a 24-column base (rates
+    1/2, 2/3, 3/4, 5/6; Z from {27, 54, 81})."""
+    from fast_ldpc_decoder_for_gpu_fixed_b200.codes import qc_irregular
+    rng = np.random.default_rng(1201)
+    zs = rng.choice([27, 54, 81], size=4)
+    return [qc_irregular(z=int(z), rate=r, seed=1300 + i) for i, (z, r) in
+            enumerate(zip(zs, ((1, 2), (2, 3), (3, 4), (5, 6))))]
+
+
+def zipf_words(total_frames, n, s=1.2, seed=1201):
+    """Per-code word counts (4 frames each): Zipf(s) shares over a seeded order."""
+    rng = np.random.default_rng(seed + 1)
+    p = 1.0 / np.arange(1, n + 1) ** s
+    p = p[rng.permutation(n)] / p.sum()
+    return [max(1, int(round(total_frames * x / 4))) for x in p]
+
+
+def run_batch(args):
+    """Config 3: one persistent, graph-captured, autotuned launch over the mixed batch."""
+    import torch
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import Batch, Decoder, _lib
+    from fast_ldpc_decoder_for_gpu_fixed_b200.learned import random_codewords, sigma_for
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    codes = batch_codes()
+    words = zipf_words(args.frames, len(codes))
+    st = torch.cuda.Stream()
+    llrs, outs, its, cws = [], [], [], []
+    for i, (c, w) in enumerate(zip(codes, words)):
+        cw = torch.from_numpy(random_codewords(c, 64, 40 + i)).cuda()
+        d = torch.empty(4 * w * c.n, dtype=torch.int8, device="cuda")
+        _lib.check(_lib.lib().ldpc_channel_awgn(d.data_ptr(), 4 * w, c.n, sigma_for(args.ebn0, c.n_info / c.n),
+                                                args.seed, i, cw.data_ptr(), 64, None))
+        llrs.append(d)
+        outs.append(torch.empty(4 * w * c.n, dtype=torch.uint8, device="cuda"))
+        its.append(torch.zeros(w, dtype=torch.int32, device="cuda"))
+        cws.append(cw)
+    torch.cuda.synchronize()
+    b = Batch(codes, args.kind, early_stop=True, graph=True)
+    tune_ms = b.autotune(llrs, outs, words, args.iters, d_iters=its, stream=st)
+    info = b.info()
+
+    def step():
+        b.decode(llrs, outs, words, args.iters, d_iters=its, stream=st)
+
+    with torch.cuda.stream(st):
+        for _ in range(args.warmup):
+            step()
+    st.synchronize()
+    fe = fr = 0
+    it_tot = 0
+    edge_updates = 0.0
+    for c, w, o, it, cw in zip(codes, words, outs, its, cws):
+        hard = o.view(4 * w, c.n)
+        ref = cw[torch.arange(4 * w, device="cuda") % 64]
+        fe += int(((hard != ref).sum(dim=1) > 0).sum())
+        fr += 4 * w
+        it_tot += int(it.sum())
+        edge_updates += float(it.sum()) * 4 * c.e
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    with torch.cuda.stream(st):
+        ms = _timed(step, args.steps, st, False)
+    clocks = sampler.stop()
+    ms_step = ms / args.steps
+    info_bits = sum(4 * w * c.n_info for c, w in zip(codes, words))
+    value = info_bits / (ms_step * 1e-3) / 1e9
+    # the same frames as separate per-code launches (one decoder per code, default stream order)
+    decs = [Decoder(c, args.kind, nb_frames=w, early_stop=True) for c, w in zip(codes, words)]
+
+    def sep():
+        for dcd, l, o, w in zip(decs, llrs, outs, words):
+            dcd.decode_device(l, o, w, args.iters, stream=st)
+
+    with torch.cuda.stream(st):
+        for _ in range(args.warmup):
+            sep()
+        ms_sep = _timed(sep, args.steps, st, False)
+    for dcd in decs:
+        dcd.close()
+    int_peak = _int_peak()
+    achieved = 2.0 * edge_updates / (ms_step * 1e-3) / 1e12
+    line = {"metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8", "data": "synthetic (seeded codewords, AWGN, reference quantiser)",
+            "config": {"workload": "mixed batch: %s, Zipf(1.2) frame counts %s (%d frames), %s with early stop, "
+                       "max %d iterations, Eb/N0 %.2f dB, one persistent graph-captured launch" % (
+                           ", ".join("%s N=%d" % (c.name, c.n) for c in codes), [4 * w for w in words],
+                           4 * sum(words), args.kind, args.iters, args.ebn0, ),
+                       "mean_iterations": it_tot / sum(words), "fer": fe / fr, "autotuned": info,
+                       "autotune_ms": tune_ms, "l2": "inputs (%d MB) re-read each step" % (
+                           sum(4 * w * c.n for c, w in zip(codes, words)) // 2**20)},
+            "per_code_launches": {"value": info_bits / (ms_sep / args.steps * 1e-3) / 1e9, "unit": "Gbit/s",
+                                  "ms_per_step": ms_sep / args.steps},
+            "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
+                         "frac": achieved / int_peak, "traffic": None, "edge_updates_per_launch": edge_updates},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": args.steps, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    b.close()
+    return 0
+
+
 def workload_name(args):
     if args.workload == "learned":
         return WORKLOAD % (args.ebn0, args.iters, args.iters)
@@ -248,6 +353,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     import torch
     import torch.distributed as dist
     from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib, replicas

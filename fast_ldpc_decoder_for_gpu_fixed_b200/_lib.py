@@ -43,6 +43,7 @@ SIGNATURES = {
     "ldpc_batch_decode": (_I, [_P, _P, _P, _P, _I, _I, _P, _P]),
     "ldpc_batch_autotune": (_I, [_P, _P, _P, _P, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "ldpc_batch_set_learned": (_I, [_P, _I, _P, _P]),
+    "ldpc_batch_configure": (_I, [_P, _I, _I, _I, _I]),
     "ldpc_batch_set_early_stop": (_I, [_P, _I, _I]),
     "ldpc_batch_info": (_I, [_P, _P]),
     "ldpc_batch_destroy": (_I, [_P]),

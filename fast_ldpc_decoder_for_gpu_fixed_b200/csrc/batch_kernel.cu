@@ -22,9 +22,12 @@ struct BatchCode {
     long long first_item;   // items of the codes before this one
     int quirk;              // OMS first-iteration quirk (row classes of this code)
     int out_packed;
+    int variant;            // this code's row-degree class: 0 <= 8, 1 <= 16, 2 <= 32
 };
 
-template <class PK, int KIND, int DT>
+// VMAX: the largest degree class of the batch; each word runs the unrolled update
+// of its own code's class
+template <class PK, int KIND, int VMAX>
 __global__ void __launch_bounds__(256) decode_batch_kernel(const BatchCode* __restrict__ codes, int n_codes,
                                                            unsigned long long* counter, long long total, const Job base)
 {
@@ -48,19 +51,25 @@ __global__ void __launch_bounds__(256) decode_batch_kernel(const BatchCode* __re
         J.word0 = 0;
         J.quirk = bc.quirk;
         const Plan P = bc.plan;
-        decode_word_levels<PK, KIND, DT, false>(P, J, item - bc.first_item, smem_raw, s_odd);
+        const long long g = item - bc.first_item;
+        if (VMAX == 0 || bc.variant == 0)
+            decode_word_levels<PK, KIND, 8, false>(P, J, g, smem_raw, s_odd);
+        else if (VMAX == 1 || bc.variant == 1)
+            decode_word_levels<PK, KIND, (VMAX >= 1 ? 16 : 8), false>(P, J, g, smem_raw, s_odd);
+        else
+            decode_word_levels<PK, KIND, (VMAX >= 2 ? 32 : 8), false>(P, J, g, smem_raw, s_odd);
         __syncthreads();  // shared memory and s_item are reused by the next item
     }
 }
 
-#define LDPC_BATCH_ROW(PK, KIND)                                                                    \
-    {(const void*)decode_batch_kernel<PK, KIND, 8>, (const void*)decode_batch_kernel<PK, KIND, 16>, \
-     (const void*)decode_batch_kernel<PK, KIND, 32>},
+#define LDPC_BATCH_ROW(PK, KIND)                                                                  \
+    {(const void*)decode_batch_kernel<PK, KIND, 0>, (const void*)decode_batch_kernel<PK, KIND, 1>, \
+     (const void*)decode_batch_kernel<PK, KIND, 2>},
 #define LDPC_BATCH_PACK(PK)                                                                                         \
     {LDPC_BATCH_ROW(PK, KIND_MS) LDPC_BATCH_ROW(PK, KIND_OMS) LDPC_BATCH_ROW(PK, KIND_NMS) LDPC_BATCH_ROW(PK, KIND_2NMS) \
          LDPC_BATCH_ROW(PK, KIND_LEARNED)},
 
-// [pack: SIMD4, F16X2, I8][kind: MS, OMS, NMS, 2NMS, LEARNED][row degree <= 8, 16, 32]
+// [pack: SIMD4, F16X2, I8][kind: MS, OMS, NMS, 2NMS, LEARNED][largest degree class: <= 8, 16, 32]
 const void* kernel_table_batch(int pack, int kind, int variant)
 {
     static const void* table[3][5][3] = {LDPC_BATCH_PACK(PackSIMD4) LDPC_BATCH_PACK(PackF16x2) LDPC_BATCH_PACK(PackI8)};
@@ -73,9 +82,10 @@ size_t batch_code_bytes() { return sizeof(BatchCode); }
 
 // fills one BatchCode record on the host (the struct stays private to this file)
 void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, long long words,
-                     long long first_item, int quirk, int out_packed)
+                     long long first_item, int quirk, int out_packed, int variant)
 {
     BatchCode* b = reinterpret_cast<BatchCode*>(rec);
+    b->variant = variant;
     b->plan = plan;
     b->llr = llr;
     b->out = out;

@@ -46,6 +46,17 @@ static int fail(int code, const char* fmt, ...)
 
 int ldpc_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
+// The dynamic shared-memory limit is an attribute of the kernel function, shared by
+// every decoder that launches it: only ever raise it, so that a later decoder of a
+// smaller code does not lower it under an earlier one.
+cudaError_t ldpc_internal_raise_smem(const void* fn, size_t bytes)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess || (size_t)fa.maxDynamicSharedSizeBytes >= bytes) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 #define CUDA_TRY(x)                                                                          \
     do {                                                                                     \
         cudaError_t e_ = (x);                                                                \
@@ -530,9 +541,8 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     }
-    cudaError_t e1 = cudaFuncSetAttribute(d->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
-    if (e1 == cudaSuccess && d->kfn_alt)
-        e1 = cudaFuncSetAttribute(d->kfn_alt, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem);
+    cudaError_t e1 = ldpc_internal_raise_smem(d->kfn, d->smem);
+    if (e1 == cudaSuccess && d->kfn_alt) e1 = ldpc_internal_raise_smem(d->kfn_alt, d->smem);
     cudaFuncAttributes fa;
     cudaError_t e2 = cudaFuncGetAttributes(&fa, d->kfn);
     cudaError_t e3 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->ctas_per_sm, d->kfn, d->threads, d->smem);
@@ -902,7 +912,7 @@ namespace ldpc {
 const void* kernel_table_batch(int pack, int kind, int variant);
 size_t batch_code_bytes();
 void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, long long words,
-                     long long first_item, int quirk, int out_packed);
+                     long long first_item, int quirk, int out_packed, int variant);
 }  // namespace ldpc
 
 struct ldpc_batch {
@@ -910,6 +920,13 @@ struct ldpc_batch {
     bool early = false, use_graph = false;
     unsigned slack = LDPC_EARLY_STOP_DEFAULT_SLACK;
     std::vector<ldpc_decoder*> plans;  // each code's tables and schedule (decoder_setup)
+    std::vector<int> cls;              // degree class of each code: 0 <= 8, 1 <= 16, 2 <= 32
+    std::vector<int> dvar;             // its variant of the per-code kernels (degree_variant)
+    std::vector<int> widest;           // its widest level
+    // per-code strategy: each code's own level kernel, one launch per code
+    bool per_code = false;
+    std::vector<const void*> pc_kfn;
+    std::vector<int> pc_threads, pc_smem;
     void* d_codes = nullptr;           // BatchCode[n]
     void* h_codes = nullptr;           // pinned staging of the same
     unsigned long long* d_counter = nullptr;
@@ -946,28 +963,68 @@ static size_t batch_smem(const ldpc_batch* b, int pack)
     return s + (b->kind == LDPC_LEARNED ? 512 : 0);
 }
 
-// selects packing, CTA width and resident CTAs per SM (0 = as many as fit)
-static int batch_configure(ldpc_batch* b, int pack, int threads, int ctas_per_sm)
+// LDPC_LEARNED tables of the batch for a packing
+static int batch_lut(ldpc_batch* b, int pack)
 {
+    if (b->kind != LDPC_LEARNED || b->off.empty()) return LDPC_OK;
+    std::vector<uint16_t> lut;
+    int rc = build_learned_lut(pack == LDPC_PACK_F16X2, b->lut_its, b->off.data(), b->sc.data(), lut);
+    if (rc) return rc;
+    if (!b->d_lut) CUDA_TRY(cudaMalloc(&b->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
+    CUDA_TRY(cudaMemcpy(b->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    return LDPC_OK;
+}
+
+// selects the strategy: one persistent kernel with this packing, CTA width and
+// resident CTAs per SM (0 = as many as fit), or (per_code) one launch of each
+// code's own level kernel with this packing
+static int batch_configure(ldpc_batch* b, int pack, int threads, int ctas_per_sm, bool per_code = false)
+{
+    int smem_max = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+    const size_t lut = b->kind == LDPC_LEARNED ? 512 : 0;
+    if (per_code) {
+        std::vector<const void*> kf;
+        std::vector<int> th, sm;
+        for (size_t i = 0; i < b->plans.size(); i++) {
+            const Plan& P = b->plans[i]->plan;
+            const void* f = kernel_for(pack, b->kind, b->dvar[i]);
+            const size_t smem = smem_bytes(pack, P.npad, P.dmax, P.m) + lut;
+            if (!f || smem > (size_t)smem_max)
+                return fail(LDPC_ERR_UNSUPPORTED, "batch: code %zu does not fit pack %d", i, pack);
+            CUDA_TRY(ldpc_internal_raise_smem(f, smem));
+            kf.push_back(f);
+            th.push_back(std::min(256, std::max(32, (b->widest[i] + 31) / 32 * 32)));
+            sm.push_back((int)smem);
+        }
+        int rc = batch_lut(b, pack);
+        if (rc) return rc;
+        b->pc_kfn = kf;
+        b->pc_threads = th;
+        b->pc_smem = sm;
+        b->per_code = true;
+        b->pack = pack;
+        b->kfn = nullptr;
+        b->grid = 0;
+        b->threads = 0;
+        b->smem = 0;
+        b->ctas_per_sm = 0;
+        b->key.clear();
+        return LDPC_OK;
+    }
     const int k = b->kind == LDPC_LEARNED ? 4 : b->kind;
     const void* kfn = kernel_table_batch(pack, k, b->variant);
     if (!kfn) return fail(LDPC_ERR_UNSUPPORTED, "batch: no kernel for pack %d", pack);
-    int smem_max = 0;
-    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
     const size_t smem = batch_smem(b, pack);
     if (smem > (size_t)smem_max)
         return fail(LDPC_ERR_UNSUPPORTED, "batch: the largest code needs %zu B of shared memory with pack %d", smem, pack);
-    if (b->kind == LDPC_LEARNED && !b->off.empty()) {
-        std::vector<uint16_t> lut;
-        int rc = build_learned_lut(pack == LDPC_PACK_F16X2, b->lut_its, b->off.data(), b->sc.data(), lut);
-        if (rc) return rc;
-        if (!b->d_lut) CUDA_TRY(cudaMalloc(&b->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
-        CUDA_TRY(cudaMemcpy(b->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-    }
-    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int rc = batch_lut(b, pack);
+    if (rc) return rc;
+    CUDA_TRY(ldpc_internal_raise_smem(kfn, smem));
     int occ = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
     if (occ < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch: kernel cannot be resident (%zu B, %d threads)", smem, threads);
+    b->per_code = false;
     b->pack = pack;
     b->kfn = kfn;
     b->threads = threads;
@@ -1011,6 +1068,10 @@ extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes
         return fail(LDPC_ERR_CUDA, "ldpc_batch_create: %s", cudaGetErrorString(e));
     }
     for (int i = 0; i < n_codes; i++) {
+        const int dm = codes[i]->dmax;
+        b->cls.push_back(dm <= 8 ? 0 : (dm <= 16 ? 1 : 2));
+        b->dvar.push_back(degree_variant(codes[i]));
+        b->widest.push_back(codes[i]->widest);
         ldpc_decoder* d = new ldpc_decoder();
         b->plans.push_back(d);
         int rc = decoder_setup(d, codes[i]);
@@ -1043,7 +1104,7 @@ extern "C" int ldpc_batch_set_learned(ldpc_batch* b, int n_iters, const int8_t* 
     b->off.assign(offsets, offsets + 2 * n_iters);
     b->sc.assign(scales, scales + 2 * n_iters);
     b->lut_its = n_iters;
-    int rc = batch_configure(b, b->pack, b->threads, b->ctas_per_sm);
+    int rc = batch_configure(b, b->pack, b->threads, b->ctas_per_sm, b->per_code);
     if (rc) {
         b->off.clear();
         b->sc.clear();
@@ -1090,7 +1151,8 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
     if (total == 0) return LDPC_OK;
     std::vector<uintptr_t> key = recs;
     for (uintptr_t x : {(uintptr_t)b->kfn, (uintptr_t)b->grid, (uintptr_t)b->threads, (uintptr_t)iters,
-                        (uintptr_t)b->early, (uintptr_t)b->slack, (uintptr_t)stream, (uintptr_t)b->d_lut})
+                        (uintptr_t)b->early, (uintptr_t)b->slack, (uintptr_t)stream, (uintptr_t)b->d_lut,
+                        (uintptr_t)b->per_code, (uintptr_t)b->pack})
         key.push_back(x);
     CUDA_TRY(cudaSetDevice(b->device));
     cudaStream_t st = (cudaStream_t)stream;
@@ -1102,7 +1164,7 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
         for (int i = 0; i < n; i++) {
             batch_code_fill(static_cast<char*>(b->h_codes) + i * batch_code_bytes(), b->plans[i]->plan, d_llr[i],
                             d_out[i], d_iters_out ? d_iters_out[i] : nullptr, (long long)n_words[i], first,
-                            b->kind == LDPC_OMS, out_format == LDPC_OUT_PACKED);
+                            b->kind == LDPC_OMS, out_format == LDPC_OUT_PACKED, b->cls[i]);
             first += (long long)n_words[i];
         }
     }
@@ -1117,6 +1179,23 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
     unsigned long long* counter = b->d_counter;
     void* args[] = {(void*)&codes, (void*)&n, (void*)&counter, (void*)&total, (void*)&J};
     auto enqueue = [&]() -> cudaError_t {
+        if (b->per_code) {
+            for (int i = 0; i < n; i++) {
+                if (n_words[i] == 0) continue;
+                Job Jc = J;
+                Jc.llr = d_llr[i];
+                Jc.out = d_out[i];
+                Jc.out_packed = out_format == LDPC_OUT_PACKED;
+                Jc.iters_out = d_iters_out ? d_iters_out[i] : nullptr;
+                Jc.total_words = (long long)n_words[i];
+                Plan P = b->plans[i]->plan;
+                void* a[] = {(void*)&P, (void*)&Jc};
+                cudaError_t e = cudaLaunchKernel(b->pc_kfn[i], dim3((unsigned)n_words[i]), dim3(b->pc_threads[i]), a,
+                                                 b->pc_smem[i], st);
+                if (e != cudaSuccess) return e;
+            }
+            return cudaSuccess;
+        }
         cudaError_t e = cudaMemcpyAsync(b->d_codes, b->h_codes, batch_code_bytes() * n, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st);
         if (e == cudaSuccess)
@@ -1157,18 +1236,23 @@ extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, vo
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     const int packs[3] = {LDPC_PACK_SIMD4, LDPC_PACK_F16X2, LDPC_PACK_I8};
-    const int widths[3] = {64, 128, 256};
+    const int widths[4] = {64, 128, 256, 0};  // 0: the per-code strategy
     double best = 1e30;
     int bp = b->pack, bt = b->threads, bc = 0;
+    bool bpc = b->per_code;
     const bool graph = b->use_graph;
     b->use_graph = false;  // time the launches themselves
     for (int p : packs) {
         for (int t : widths) {
             for (int half = 0; half < 2; half++) {
-                if (batch_configure(b, p, t, 0)) continue;
-                const int ctas = half ? std::max(1, b->ctas_per_sm / 2) : b->ctas_per_sm;
-                if (half && ctas == b->ctas_per_sm) continue;
-                if (batch_configure(b, p, t, ctas)) continue;
+                if (t == 0) {
+                    if (half || batch_configure(b, p, 0, 0, true)) continue;
+                } else {
+                    if (batch_configure(b, p, t, 0)) continue;
+                    const int ctas = half ? std::max(1, b->ctas_per_sm / 2) : b->ctas_per_sm;
+                    if (half && ctas == b->ctas_per_sm) continue;
+                    if (batch_configure(b, p, t, ctas)) continue;
+                }
                 int rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, stream);
                 if (rc) continue;
                 float ms = 0.f;
@@ -1182,7 +1266,8 @@ extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, vo
                     best = ms / 3;
                     bp = p;
                     bt = t;
-                    bc = ctas;
+                    bc = b->ctas_per_sm;
+                    bpc = b->per_code;
                 }
             }
         }
@@ -1190,10 +1275,19 @@ extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, vo
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->use_graph = graph;
-    int rc = batch_configure(b, bp, bt, bc);
+    int rc = batch_configure(b, bp, bt, bc, bpc);
     if (rc) return rc;
     if (best_ms) *best_ms = best;
     return best < 1e30 ? LDPC_OK : fail(LDPC_ERR_UNSUPPORTED, "ldpc_batch_autotune: no configuration ran");
+}
+
+extern "C" int ldpc_batch_configure(ldpc_batch* b, int per_code, int pack, int threads, int ctas_per_sm)
+{
+    if (!b) return fail(LDPC_ERR_ARG, "ldpc_batch_configure: null batch");
+    if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8) return fail(LDPC_ERR_ARG, "ldpc_batch_configure: pack %d", pack);
+    if (!per_code && (threads < 32 || threads > 256 || threads % 32 || ctas_per_sm < 0))
+        return fail(LDPC_ERR_ARG, "ldpc_batch_configure: threads must be 32..256 in steps of 32, ctas_per_sm >= 0");
+    return batch_configure(b, pack, threads, ctas_per_sm, per_code != 0);
 }
 
 extern "C" int ldpc_batch_info(const ldpc_batch* b, int* info)
@@ -1207,6 +1301,7 @@ extern "C" int ldpc_batch_info(const ldpc_batch* b, int* info)
     info[5] = b->grid;
     info[6] = b->use_graph;
     info[7] = (int)b->plans.size();
+    info[8] = b->per_code;
     return LDPC_OK;
 }
 
@@ -1308,7 +1403,7 @@ extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const
     J.iters = iters;
     J.quirk = kind == LDPC_OMS;
     const int threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
-    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(ldpc_internal_raise_smem(kfn, smem));
     void* args[] = {(void*)&P, (void*)&J};
     CUDA_TRY(cudaLaunchKernel(kfn, dim3((unsigned)n_words), dim3(threads), args, smem, st));
     return LDPC_OK;

@@ -275,6 +275,7 @@ using namespace ldpc;
 
 int ldpc_internal_fail(int code, const char* msg);
 int ldpc_internal_plan(const ldpc_decoder* dec, Plan* plan, int* threads);
+cudaError_t ldpc_internal_raise_smem(const void* fn, size_t bytes);
 
 static size_t stash_rows(const Plan& P, size_t frames, int iters) { return frames * (size_t)iters * P.m * sizeof(uint4); }
 static size_t stash_apps(const Plan& P, size_t frames, int iters) { return frames * (size_t)iters * P.n * sizeof(float); }
@@ -338,7 +339,7 @@ extern "C" int ldpc_train_step(const ldpc_decoder* dec, const float* d_llr, cons
     A.backward = backward ? 1 : 0;
     A.inv_frames = (float)(1.0 / (double)frames);
     A.inv_n = (float)(1.0 / (double)P.n);
-    cudaError_t e = cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ldpc_internal_raise_smem((const void*)train_kernel, smem);
     if (e == cudaSuccess) {
         train_kernel<<<(unsigned)frames, threads, smem, (cudaStream_t)stream>>>(P, A);
         e = cudaGetLastError();

@@ -210,6 +210,11 @@ class Batch:
                                                   ctypes.byref(best), st))
         return best.value
 
+    def configure(self, per_code=False, pack="SIMD4", threads=128, ctas_per_sm=0):
+        """The strategy by hand (ldpc_batch_configure)."""
+        _lib.check(_lib.lib().ldpc_batch_configure(self.handle, int(bool(per_code)), _lib.PACKS[pack.upper()],
+                                                   int(threads), int(ctas_per_sm)))
+
     def set_learned(self, offsets, scales):
         off = np.ascontiguousarray(offsets, dtype=np.int8).reshape(-1, 2)
         sc = np.ascontiguousarray(scales, dtype=np.uint8).reshape(-1, 2)
@@ -219,9 +224,9 @@ class Batch:
         _lib.check(_lib.lib().ldpc_batch_set_early_stop(self.handle, int(bool(enabled)), int(slack)))
 
     def info(self):
-        a = (ctypes.c_int * 8)()
+        a = (ctypes.c_int * 9)()
         _lib.check(_lib.lib().ldpc_batch_info(self.handle, a))
-        keys = ("kind", "pack", "threads", "smem", "ctas_per_sm", "grid", "graph", "codes")
+        keys = ("kind", "pack", "threads", "smem", "ctas_per_sm", "grid", "graph", "codes", "per_code")
         return dict(zip(keys, list(a)))
 
     def close(self):

@@ -262,11 +262,19 @@ int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes, int n_cod
 int ldpc_batch_decode(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
                       int iters, int out_format, int32_t* const* d_iters_out, void* stream);
 
-/* Times the packings (SIMD4, F16X2, I8), CTA widths (64, 128, 256) and resident
- * CTAs per SM (as many as fit, or half) on these inputs (outputs are
- * overwritten), keeps the fastest and returns its time per decode in *best_ms. */
+/* Times, on these inputs (outputs are overwritten), the two strategies: the
+ * persistent kernel for each packing (SIMD4, F16X2, I8), CTA width (64, 128,
+ * 256) and residency (as many CTAs per SM as fit, or half), and one launch of
+ * each code's own kernel per packing (shared memory sized per code, all launches
+ * in the same graph with LDPC_BATCH_GRAPH); keeps the fastest and returns its
+ * time per decode in *best_ms. */
 int ldpc_batch_autotune(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
                         int iters, int32_t* const* d_iters_out, double* best_ms, void* stream);
+
+/* Sets the strategy by hand: per_code = 0: the persistent kernel with this pack,
+ * CTA width (32..256) and resident CTAs per SM (0 = as many as fit); per_code = 1:
+ * one launch of each code's own kernel with this pack. */
+int ldpc_batch_configure(ldpc_batch* batch, int per_code, int pack, int threads, int ctas_per_sm);
 
 /* LDPC_LEARNED constants of the batch (all codes), as ldpc_decoder_set_learned. */
 int ldpc_batch_set_learned(ldpc_batch* batch, int n_iters, const int8_t* offsets, const uint8_t* scales);
@@ -274,8 +282,10 @@ int ldpc_batch_set_learned(ldpc_batch* batch, int n_iters, const int8_t* offsets
 /* Early stop on/off and its slack, as ldpc_decoder_set_early_stop. */
 int ldpc_batch_set_early_stop(ldpc_batch* batch, int enabled, int slack);
 
-/* info[0..7] = kind, pack, threads per CTA, shared bytes per CTA, resident CTAs
- * per SM, grid (CTAs of the persistent launch), graph mode, number of codes */
+/* info[0..8] = kind, pack, threads per CTA, shared bytes per CTA, resident CTAs
+ * per SM, grid (CTAs of the persistent launch), graph mode, number of codes,
+ * strategy (0 = one persistent kernel, 1 = one launch per code; the CTA fields
+ * are 0 then) */
 int ldpc_batch_info(const ldpc_batch* batch, int* info);
 
 int ldpc_batch_destroy(ldpc_batch* batch);

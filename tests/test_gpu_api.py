@@ -112,3 +112,19 @@ def test_simd_ops_exhaustive(cuda, op):
         torch.cuda.synchronize()
         got = (dO.cpu().numpy().view(np.uint32) >> np.uint32(8 * lane)) & np.uint32(0xFF)
         assert np.array_equal(got, table_), "op %d lane %d" % (op, lane)
+
+
+def test_decoders_sharing_a_kernel(cuda):
+    """Two decoders whose codes use the same kernel with different shared-memory
+    sizes: creating the smaller one after the larger must not break the larger."""
+    import torch
+    big, small = table("1944x972"), table("576x288")   # both: the SIMD4 OMS kernel for degree <= 8
+    d_big = fl.Decoder(big, "OMS", nb_frames=4, pack="SIMD4")
+    d_small = fl.Decoder(small, "OMS", nb_frames=4, pack="SIMD4")
+    for code, dec in ((big, d_big), (small, d_small)):
+        llr = make_llr("awgn", 16 * code.n, 3, sigma=llr_gen.sigma_for(2.0, 0.5))
+        out = torch.zeros(16 * code.n, dtype=torch.uint8, device="cuda")
+        dec.decode_device(torch.from_numpy(llr).cuda(), out, 4, 8)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().reshape(16, code.n), oracle_decode(code, "OMS", llr, 8)["hard"])
+        dec.close()
