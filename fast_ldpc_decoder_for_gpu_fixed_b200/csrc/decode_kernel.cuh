@@ -267,22 +267,24 @@ template <> struct Access<PackSIMD4> {
 };
 
 template <> struct Access<PackF16x2> {
-    // x bytes of frames k0, k0+1 -> biased negated pair b = 127 - x
+    // x bytes of frames k0, k0+1 -> biased negated pair b = 127 - x.  As an unsigned
+    // byte, 127 - x is x ^ 0x7f for every int8 x; under the byte 0x64 it becomes the
+    // fp16 bit pattern of 1024 + (127 - x), and subtracting 1024 is exact.
     __device__ __forceinline__ static uint32_t pair(uint32_t w, int k0)
     {
-        int a = 127 - (int)(int8_t)(w >> (8 * k0)), b = 127 - (int)(int8_t)(w >> (8 * k0 + 8));
-        __half2 h = __halves2half2(__int2half_rn(a), __int2half_rn(b));
-        return h2u(h);
+        const uint32_t y = w ^ 0x7f7f7f7fu;
+        return h2::add(__byte_perm(y, 0x6464u, k0 == 0 ? 0x4140 : 0x4342), h2::CNEG1024);
     }
     __device__ __forceinline__ static void put(uint32_t* app, int npad, int v, uint32_t w)
     {
         app[v] = pair(w, 0);
         app[npad + v] = pair(w, 2);
     }
+    // the inverse of pair() for both pair-words: b + 1024 has the integer b in its low
+    // byte (b is an integer in [0, 255]), and x = 127 - b is that byte ^ 0x7f
     __device__ __forceinline__ static uint32_t unbias(uint32_t lo, uint32_t hi)
     {
-        auto x = [](uint16_t h) { return (uint32_t)(uint8_t)(int8_t)(127 - __half2int_rn(__ushort_as_half(h))); };
-        return x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
+        return __byte_perm(h2::add(lo, h2::C1024), h2::add(hi, h2::C1024), 0x6420) ^ 0x7f7f7f7fu;
     }
     __device__ __forceinline__ static uint32_t get(const uint32_t* app, int npad, int v)
     {
@@ -346,7 +348,10 @@ template <> struct Access<PackI8> {
 // reset for the next iteration.  Uniform across the CTA.
 __device__ __forceinline__ bool odd_rows_within_slack(const Job& J, unsigned odd, int it, unsigned* s_odd)
 {
-    if (odd) atomicAdd(&s_odd[it & 1], odd);
+    // one shared atomic per warp, not per thread (every thread of the CTA is here)
+    const unsigned lanes = __activemask();
+    const unsigned w = __reduce_add_sync(lanes, odd);
+    if (w && (int)(threadIdx.x & 31) == __ffs(lanes) - 1) atomicAdd(&s_odd[it & 1], w);
     __syncthreads();
     const unsigned total = s_odd[it & 1];
     if (threadIdx.x == 0) s_odd[(it + 1) & 1] = 0;

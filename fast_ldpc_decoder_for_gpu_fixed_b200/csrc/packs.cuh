@@ -199,19 +199,17 @@ __device__ __forceinline__ uint32_t floor_scale(uint32_t m, uint32_t k, uint32_t
     return add(add(fma_relu(m, k, bias), C1024), CNEG1024);
 }
 
-// row magnitudes from |min1| (a1) and |min2| (a2)
+// row magnitudes from |min1| (a1) and |min2| (a2); lk, lb: the LEARNED (k, k), (b, b) words
 template <int KIND>
-__device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2,
-                                     const uint16_t* lut)
+__device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2, uint32_t lk,
+                                     uint32_t lb)
 {
     if (KIND == KIND_LEARNED) {
         // clamp(floor(a * k) - offset, 0, 31) = min(round(relu(a * k + b)), 31), b = -offset - 15/32:
         // with k on a 1/16 grid, a * k + b is exact below 64 and never within 1/32 of a tie
         // (ldpc_decoder_set_learned stores (k, k) and (b, b) at the head of the class's table)
-        const uint32_t k2 = *reinterpret_cast<const uint32_t*>(lut);
-        const uint32_t b2 = *reinterpret_cast<const uint32_t*>(lut + 2);
-        c1 = hmin(floor_scale(a2, k2, b2), C31);
-        c2 = hmin(floor_scale(a1, k2, b2), C31);
+        c1 = hmin(floor_scale(a2, lk, lb), C31);
+        c2 = hmin(floor_scale(a1, lk, lb), C31);
     } else if (KIND == KIND_MS) {
         c1 = hmin(a2, C31);
         c2 = hmin(a1, C31);
@@ -229,9 +227,20 @@ __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint
 }
 
 // one row over one pair-word: b[j] biased APP in/out, m[j] negated message in/out
+// the LEARNED (k, b) words at the head of a class's table (zero for other kinds)
+template <int KIND>
+__device__ __forceinline__ void learned_kb(const uint16_t* lut, uint32_t& lk, uint32_t& lb)
+{
+    lk = lb = 0;
+    if (KIND == KIND_LEARNED) {
+        lk = reinterpret_cast<const uint32_t*>(lut)[0];
+        lb = reinterpret_cast<const uint32_t*>(lut)[1];
+    }
+}
+
 template <int KIND, int DT, bool EXACT>
 __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov,
-                                    const uint16_t* lut)
+                                    uint32_t lk, uint32_t lb)
 {
     uint32_t ut[DT];
     uint32_t mn1 = C127, mn2 = C127;
@@ -248,7 +257,7 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
     }
     const uint32_t a1 = mn1 & MAG, a2 = mn2 & MAG;
     uint32_t c1, c2;
-    mags<KIND>(a1, a2, noclip, c1, c2, lut);
+    mags<KIND>(a1, a2, noclip, c1, c2, lk, lb);
     const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
     const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
 #pragma unroll
@@ -282,7 +291,9 @@ struct PackF16x2 {
     __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov,
                                                   const uint16_t* lut)
     {
-        h2::row<KIND, DT, EXACT>(x, m, d, noclip, ov, lut);
+        uint32_t lk, lb;
+        h2::learned_kb<KIND>(lut, lk, lb);
+        h2::row<KIND, DT, EXACT>(x, m, d, noclip, ov, lk, lb);
     }
 };
 

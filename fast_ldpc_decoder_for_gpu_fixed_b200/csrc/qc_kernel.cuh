@@ -44,13 +44,15 @@ __device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int k8)
     return Q.cz4[idx] + u;
 }
 
-template <int DT, bool EXACT, int L, bool POW2>
+// true when row k of some layer in [L0, L1) has odd hard-decision parity in one of
+// the 4 frames (see the early stop in decode_qc_kernel)
+template <int DT, bool EXACT, int L0, int L1, bool POW2>
 __device__ __noinline__ bool qc_rows_unsatisfied(const QCParams& Q, const char* appb, int k)
 {
     bool bad = false;
     const int kk = 8 * k;
 #pragma unroll
-    for (int l = 0; l < L; l++) {
+    for (int l = L0; l < L1; l++) {
         const int d = EXACT ? DT : Q.deg[l];
         uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
 #pragma unroll
@@ -119,9 +121,10 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant
                     b1[j] = v.y;
                 }
             }
-            const uint16_t* lut = slut + 128 * Q.cls[l];
-            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov, lut);
-            h2::row<KIND, DT, EXACT>(b1, msg[1][l], d, noclip, ov, lut);
+            uint32_t lk, lb;  // LEARNED constants of this layer's class (registers only within the layer)
+            h2::learned_kb<KIND>(slut + 128 * Q.cls[l], lk, lb);
+            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov, lk, lb);
+            h2::row<KIND, DT, EXACT>(b1, msg[1][l], d, noclip, ov, lk, lb);
 #pragma unroll
             for (int j = 0; j < DT; j++)
                 if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
@@ -138,8 +141,11 @@ __global__ void __launch_bounds__(256, 2) decode_qc_kernel(const __grid_constant
         // hard decision is 0; a row is satisfied when its count of 1s is even.
         if (KIND != KIND_2NMS && ET) {
             if (odd_rows_within_slack(J, ov, it, s_odd)) {
-                const bool bad = qc_rows_unsatisfied<DT, EXACT, L, POW2>(Q, appb, k);
-                if (!__syncthreads_or(bad)) break;
+                // staged: the first layers alone reject most words that are not codewords yet
+                constexpr int LS = L > 2 ? 2 : L;
+                bool done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, 0, LS, POW2>(Q, appb, k));
+                if (LS < L && done) done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, LS, L, POW2>(Q, appb, k));
+                if (done) break;
             }
         }
     }
