@@ -162,7 +162,9 @@ def cpu_baseline(code, llr, iters, kind, budget_s, info_bits):
     returns (Gbit/s, cores, sample description)."""
     from oracle import oracle
     cores = os.cpu_count() or 1
-    probe = min(llr.shape[0], 1024)
+    probe = min(llr.shape[0], 1024) // 32 * 32   # the AVX2 port decodes 32-frame groups
+    if probe == 0:
+        return 0.0, cores, "no sample (fewer than 32 frames)"
     t = time.perf_counter()
     oracle.decode_batch(code, kind, llr[:probe], iters, nthreads=cores)
     dt = time.perf_counter() - t
