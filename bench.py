@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira", "batch"])
     ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
     ap.add_argument("--fer-frames", type=int, default=1 << 20)
+    ap.add_argument("--no-sweep", dest="sweep", action="store_false",
+                    help="skip the learned-vs-plain ratio over Eb/N0 1.5..2.5 dB")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qc", action="store_true", help="use the level-scheduled kernel even for the QC code")
@@ -451,6 +453,11 @@ def main():
                                           "mean_iters": fl["mean_iters"]},
                    "plain_oms": {"fer": fp["fer"], "frame_errors": fp["frame_errors"], "ber": fp["ber"]}}
 
+    # the ratio across the config-2 Eb/N0 range (untimed by the caller: extra lines of evidence)
+    sweep = None
+    if learned and rank == 0 and args.sweep:
+        sweep = _sweep(code, constants, args, stream)
+
     # roofline of the decode kernel (one launch per step), from the iterations it executed
     int_peak = _int_peak()
     if per_frame:
@@ -494,6 +501,7 @@ def main():
             "plain_oms": plain,
             "vs_plain_oms": value / plain["value"] if plain else None,
             "fer": fer_cmp,
+            "ebn0_sweep": sweep,
             "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
                          "frac": achieved / int_peak, "traffic": None,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
@@ -513,6 +521,42 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _sweep(code, constants, args, stream):
+    """Learned decoder with early stop vs plain OMS (10 fixed iterations) at each Eb/N0 of the
+    config-2 range: kernel Gbit/s of both on 65 536 channel frames, and their FER on 2^18 frames."""
+    import torch
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib
+    from fast_ldpc_decoder_for_gpu_fixed_b200.learned import evaluate, random_codewords, sigma_for
+    words = args.frames // 4
+    cw = torch.from_numpy(random_codewords(code, 64, 77)).cuda()
+    llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
+    out = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    its = torch.zeros(words, dtype=torch.int32, device="cuda")
+    ldec = Decoder(code, "LEARNED", nb_frames=words, early_stop=True)
+    ldec.set_learned(*constants)
+    pdec = Decoder(code, "OMS", nb_frames=words)
+    rows = []
+    for e in (1.5, 1.75, 2.0, 2.25, 2.5):
+        _lib.check(_lib.lib().ldpc_channel_awgn(llr.data_ptr(), 4 * words, code.n, sigma_for(e, code.n_info / code.n),
+                                                91, 0, cw.data_ptr(), 64, stream.cuda_stream))
+        row = {"ebn0_db": e}
+        for name, dec, d_its in (("learned_early_stop", ldec, its), ("plain_oms", pdec, None)):
+            def st():
+                dec.decode_device(llr, out, words, args.iters, _lib.OUT_BYTES, d_its, stream)
+            for _ in range(2):
+                st()
+            ms = _timed(st, 10, stream, False) / 10
+            r = evaluate(code, "LEARNED" if d_its is not None else "OMS", args.iters, e, 1 << 18,
+                         constants=constants if d_its is not None else None, early_stop=d_its is not None)
+            row[name] = {"gbps": 4 * words * code.n_info / (ms * 1e-3) / 1e9, "fer": r["fer"],
+                         "frame_errors": r["frame_errors"], "mean_iters": r["mean_iters"]}
+        row["ratio"] = row["learned_early_stop"]["gbps"] / row["plain_oms"]["gbps"]
+        rows.append(row)
+    ldec.close()
+    pdec.close()
+    return rows
 
 
 def _measured_peaks():
