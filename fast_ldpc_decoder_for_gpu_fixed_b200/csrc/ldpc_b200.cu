@@ -307,45 +307,65 @@ namespace ldpc {
 const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
-const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et);
+const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et, int wpt);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
 }
 
 // shared memory of the QC kernel: the APP of 4 frames, 8 bytes per variable
-static size_t qc_smem(const ldpc_code* c) { return (size_t)c->n * 8; }
+static size_t qc_smem(const ldpc_code* c, int wpt) { return (size_t)c->n * 4 * wpt; }
 
 // QC register-message kernel, when the code is QC and a matching instantiation exists
-static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false)
+// The QC register-message kernel for the code, or null: 4 frames per CTA (*wpt = 2)
+// when an instantiation matches the code's shape, else 2 frames per CTA (*wpt = 1)
+// with the smallest instantiated row degree that holds it.  Fills q for that layout.
+static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false, int* wpt_out = nullptr)
 {
-    if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > 65535) return nullptr;
+    if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > (1 << 20)) return nullptr;
+    int deg[QC_MAX_LAYERS], dt = 0;
+    bool exact = true;
+    for (int i = 0; i < c->mb; i++) {
+        int d = 0;
+        for (int j = 0; j < c->nb; j++)
+            if (c->shifts[i * c->nb + j] >= 0) d++;
+        if (d == 0 || d > QC_MAX_DEG) return nullptr;
+        for (int k = 1; k < c->z; k++)
+            if (c->row_class[i * c->z + k] != c->row_class[i * c->z]) return nullptr;
+        deg[i] = d;
+        if (i > 0 && d != dt) exact = false;
+        dt = std::max(dt, d);
+    }
+    const bool pow2 = (c->z & (c->z - 1)) == 0;
+    const int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
+    const bool e = et && kind != LDPC_2NMS;
+    int wpt = 2;
+    const void* f = kernel_table_qc(k, dt, exact, c->mb, pow2, e, 2);
+    if (!f) {
+        wpt = 1;
+        for (int D : {10, 14, 18, 24})
+            if (D >= dt && (f = kernel_table_qc(k, D, false, c->mb, false, e, 1))) break;
+    }
+    if (!f) return nullptr;
+    const int vb = 4 * wpt;  // APP bytes per variable
     memset(&q, 0, sizeof q);
     q.z = c->z;
     q.n = c->n;
     q.layers = c->mb;
-    int dt = 0;
-    bool exact = true;
+    q.zb = vb * c->z;
     for (int i = 0; i < c->mb; i++) {
         int d = 0;
         for (int j = 0; j < c->nb; j++) {
-            int s = c->shifts[i * c->nb + j];
-            if (s < 0) continue;
-            if (d >= QC_MAX_DEG) return nullptr;
-            q.cz4[i * QC_MAX_DEG + d] = j * c->z * 8;
-            q.s[i * QC_MAX_DEG + d] = 8 * s;
+            const int sh = c->shifts[i * c->nb + j];
+            if (sh < 0) continue;
+            q.cz4[i * QC_MAX_DEG + d] = vb * j * c->z;
+            q.s[i * QC_MAX_DEG + d] = vb * sh;
             d++;
         }
-        if (d == 0) return nullptr;
-        q.deg[i] = d;
+        q.deg[i] = deg[i];
         q.cls[i] = c->row_class[i * c->z];
-        for (int k = 1; k < c->z; k++)
-            if (c->row_class[i * c->z + k] != q.cls[i]) return nullptr;
-        if (i > 0 && d != dt) exact = false;
-        dt = std::max(dt, d);
     }
-    bool pow2 = (c->z & (c->z - 1)) == 0;
-    int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
-    return kernel_table_qc(k, dt, exact, c->mb, pow2, et && kind != LDPC_2NMS);
+    if (wpt_out) *wpt_out = wpt;
+    return f;
 }
 
 // variant: 0/1 = every row has degree 6/7 (fully unrolled), 2/3/4 = rows of
@@ -480,7 +500,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     QCParams probe;
     bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
-    qc_ok = qc_ok && qc_kernel_for(c, kind, probe) && qc_smem(c) + 512 <= (size_t)smem_max;
+    int probe_wpt = 2;
+    qc_ok = qc_ok && qc_kernel_for(c, kind, probe, false, &probe_wpt) && qc_smem(c, probe_wpt) + 512 <= (size_t)smem_max;
+    // the 2-frame QC kernel is an explicit LDPC_PACK_F16X2 choice: AUTO keeps the level kernels
+    // for those shapes (faster on some, slower on others, and a different early-stop unit)
+    qc_ok = qc_ok && (probe_wpt == 2 || pack_req == LDPC_PACK_F16X2);
     if (!frame && smem > (size_t)smem_max && !qc_ok) {
         if (pack_req != LDPC_PACK_AUTO || kind == LDPC_2NMS)
             return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
@@ -511,9 +535,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         decoder_free(d);
         return rc;
     }
+    int qc_wpt = 2;
     const void* qk = !frame && (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2)
-                         ? qc_kernel_for(c, kind, d->qcp, early)
+                         ? qc_kernel_for(c, kind, d->qcp, early, &qc_wpt)
                          : nullptr;
+    if (qc_wpt == 1 && pack_req != LDPC_PACK_F16X2) qk = nullptr;
     if (frame) {
         const int k = kind == LDPC_XMS ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
         d->kfn = kernel_table_frame(k, degree_variant(c), early);
@@ -523,12 +549,14 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->grid_mult = 4;
         d->smem = (int)frame_smem;
         d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32));
-    } else if (qk && qc_smem(c) + lut_smem <= (size_t)smem_max) {
+    } else if (qk && qc_smem(c, qc_wpt) + lut_smem <= (size_t)smem_max) {
+        QCParams alt;
         d->kfn = qk;
-        d->kfn_alt = qc_kernel_for(c, kind, d->qcp, !early);  // for ldpc_decoder_set_early_stop
-        d->path = 1;
+        d->kfn_alt = qc_kernel_for(c, kind, alt, !early);  // for ldpc_decoder_set_early_stop (same layout)
+        d->path = qc_wpt == 2 ? 1 : 4;
+        d->grid_mult = qc_wpt == 2 ? 1 : 2;
         d->pack = LDPC_PACK_F16X2;
-        d->smem = (int)(qc_smem(c) + lut_smem);
+        d->smem = (int)(qc_smem(c, qc_wpt) + lut_smem);
         d->threads = c->z;
     } else if (half) {
         d->kfn = kernel_table_f16x2h(kind == LDPC_XMS ? LDPC_OMS : (kind == LDPC_LEARNED ? 3 : kind), degree_variant(c));
@@ -575,7 +603,7 @@ extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int sla
     if (enabled && d->path == 2)
         return fail(LDPC_ERR_ARG, "early stop needs a decoder created with LDPC_FLAG_EARLY_STOP for this packing");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: slack must be >= 0");
-    if ((d->path == 1 || d->path == 3) && (enabled != 0) != d->early) std::swap(d->kfn, d->kfn_alt);
+    if ((d->path == 1 || d->path == 3 || d->path == 4) && (enabled != 0) != d->early) std::swap(d->kfn, d->kfn_alt);
     d->early = enabled != 0;
     d->early_slack = (unsigned)slack;
     return LDPC_OK;
@@ -689,7 +717,9 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.iters_out = iters_out;
     J.app_out = app_out;
     J.msg_out = msg_out;
-    void* args[] = {d->path == 1 ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
+    if (d->path == 4 && iters_out)  // each 2-frame CTA raises its word's count with atomicMax
+        CUDA_TRY(cudaMemsetAsync(iters_out, 0, sizeof(int32_t) * (size_t)words, st));
+    void* args[] = {(d->path == 1 || d->path == 4) ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
     CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
 }
@@ -720,8 +750,8 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
-    if (d->path == 3 && (d_app || d_msg))
-        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME decoders have no state dumps");
+    if ((d->path == 3 || d->path == 4) && (d_app || d_msg))
+        return fail(LDPC_ERR_UNSUPPORTED, "this decoder (path %d) has no state dumps", d->path);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
                   (cudaStream_t)stream);

@@ -58,7 +58,13 @@ extern "C" {
 /* frame packing of the on-chip decoder state */
 #define LDPC_PACK_AUTO (-1)
 #define LDPC_PACK_SIMD4 0 /* 4 frames per 32-bit word, saturating byte lanes      */
-#define LDPC_PACK_F16X2 1 /* 2 frames per 32-bit word, integer-valued fp16 lanes  */
+/* 2 frames per 32-bit word, integer-valued fp16 lanes.  On a QC code (ldpc_code_create_qc)
+ * whose shape has no 4-frame register kernel (more than 8 block rows or an irregular
+ * row degree, such as 24-column bases), an explicit LDPC_PACK_F16X2 selects the QC
+ * kernel with 2 frames per CTA (info path 4); LDPC_PACK_AUTO keeps the level kernels
+ * there.  With LDPC_FLAG_EARLY_STOP path 4 stops each frame pair (frames 4g, 4g+1 and
+ * 4g+2, 4g+3) on its own and reports per word the larger of its two pairs' counts. */
+#define LDPC_PACK_F16X2 1
 #define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
 /* 1 frame per CTA, everything in shared memory: the APP as int8 and each check
  * row's messages packed into one 32-bit word (the two magnitudes, the minimum
@@ -233,7 +239,8 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
  * per CTA, CTAs per SM, registers per thread, kernel path (0 = level
  * scheduled, 1 = QC register-message, 2 = level scheduled with 2 frames per
  * CTA: LDPC_PACK_F16X2 for every kind but 2NMS, 3 = one frame per CTA with
- * packed row state: LDPC_PACK_FRAME) */
+ * packed row state: LDPC_PACK_FRAME, 4 = QC register-message with 2 frames per
+ * CTA, see LDPC_PACK_F16X2) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);

@@ -218,9 +218,11 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
  *             word[e*W+g] (d_MSG_C_2_V), e*nframes bytes.
  *   iters_out : optional, [W] iterations executed per word.
  */
-/* group: frames that stop together under the early stop (4 = a word, the
- * level and QC kernels; 1 = each frame alone, the LDPC_PACK_HBM kernel, whose
- * iteration counts are then per frame: iters_out holds nframes entries) */
+/* group: frames that stop together under the early stop: 4 = a word (the level
+ * kernels and the 4-frame QC kernel); 2 = a frame pair (the 2-frame QC kernel;
+ * a word's count is the larger of its two pairs'); 1 = each frame alone (the
+ * one-frame-per-CTA kernel, whose counts are per frame: iters_out holds nframes
+ * entries) */
 int oracle_decode_ex(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                      const uint8_t* row_class, int kind, int iters, int nframes,
                      int interleaved, const int8_t* llr, uint8_t* hard,
@@ -248,6 +250,11 @@ int oracle_decode_ex(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                                      msg + (size_t)lane * e_total, early, 1);
                 if (iters_out) iters_out[4 * g + lane] = ex;
             }
+        } else if (group == 2) {
+            int ex0 = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg, early, 2);
+            int ex1 = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app + (size_t)2 * n,
+                                  msg + (size_t)2 * e_total, early, 2);
+            if (iters_out) iters_out[g] = ex0 > ex1 ? ex0 : ex1;
         } else {
             int ex = decode_word(n, m, row_ptr, cols, row_class, kind, iters, app, msg, early, 4);
             if (iters_out) iters_out[g] = ex;

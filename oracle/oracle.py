@@ -68,7 +68,7 @@ def _p(a):
 
 
 def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False,
-           early_slack=128, per_frame=False):
+           early_slack=128, per_frame=False, pairs=False):
     """Decodes ``llr`` (int8, nframes*n bytes, frame-major unless interleaved).
 
     Returns dict with ``hard`` [nframes, n] uint8, ``iters`` [nframes/4] and,
@@ -76,7 +76,9 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     device layouts (n*nframes and e*nframes bytes).  ``early_stop``: the
     syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word) with
     ``early_slack`` (ldpc_decoder_set_early_stop); ``per_frame``: every frame
-    stops on its own and ``iters`` has one entry per frame (LDPC_PACK_HBM).
+    stops on its own and ``iters`` has one entry per frame (LDPC_PACK_FRAME);
+    ``pairs``: frames 4g, 4g+1 and 4g+2, 4g+3 stop as pairs and ``iters`` has the
+    larger count of each word (the 2-frame QC kernel, decoder path 4).
     """
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
@@ -91,7 +93,7 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
                                 k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
                                 _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0,
-                                1 if per_frame else 4)
+                                1 if per_frame else (2 if pairs else 4))
     if rc != 0:
         raise ValueError("oracle_decode rejected the arguments")
     out = {"hard": hard, "iters": it}
