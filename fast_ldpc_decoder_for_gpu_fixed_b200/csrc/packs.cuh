@@ -185,6 +185,12 @@ __device__ __forceinline__ uint32_t min_xs(uint32_t a, uint32_t b)
     asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
 }
+__device__ __forceinline__ uint32_t habs(uint32_t a)
+{
+    uint32_t d;
+    asm("abs.f16x2 %0, %1;" : "=r"(d) : "r"(a));
+    return d;
+}
 __device__ __forceinline__ uint32_t max_xs(uint32_t a, uint32_t b)
 {
     uint32_t d;
@@ -255,7 +261,7 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
             mn2 = min_xs(mn2, mx);
         }
     }
-    const uint32_t a1 = mn1 & MAG, a2 = mn2 & MAG;
+    const uint32_t a1 = habs(mn1), a2 = habs(mn2);
     uint32_t c1, c2;
     mags<KIND>(a1, a2, noclip, c1, c2, lk, lb);
     const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
@@ -266,7 +272,8 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
             // |t| >= min1 on every edge, so sat(|t| - min1) is 0 on the minimum edge(s)
             // and 1 elsewhere: r = c1s there, c2s elsewhere (one FMA instead of a
             // compare and a select)
-            uint32_t r = fma(add_sat(ut[j] & MAG, na1), dcs, c1s);
+            // (abs.f16x2 rather than a mask: the abs folds into the saturating add)
+            uint32_t r = fma(add_sat(habs(ut[j]), na1), dcs, c1s);
             uint32_t mo = r ^ (ut[j] & SIGN);                   // flip by this edge's own sign
             m[j] = mo;
             b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)

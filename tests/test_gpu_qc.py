@@ -155,7 +155,7 @@ def test_pair_qc_kernel_other_paths(cuda):
     and the fused simulation run on the 2-frame kernel."""
     import torch
     from oracle import oracle
-    code = irregular((1, 2), 54)
+    code = irregular((1, 2), 64)  # row degrees <= 10: the 2-frame kernel holds it
     words = 6
     llr = make_llr("awgn", 4 * words * code.n, 53, sigma=llr_gen.sigma_for(2.0, 0.5))
     path, hard, _ = _pair_decode(code, "2NMS", llr, 15, words)
