@@ -16,6 +16,7 @@ KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 
 PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2, "FRAME": 3}
 OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
+FLAG_EARLY_STOP_FRAMES = 4
 BATCH_GRAPH = 2
 EARLY_STOP_DEFAULT_SLACK = 128
 TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2

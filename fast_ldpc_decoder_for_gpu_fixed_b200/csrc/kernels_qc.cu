@@ -4,7 +4,9 @@
 //     8 layers, Z a power of two);
 //   2 frames per CTA (WPT = 1): 24-column irregular bases (802.11n-like) at rates
 //     1/2, 2/3, 3/4, 5/6, i.e. 12, 8, 6, 4 layers of row degree up to 10, 14, 18, 24,
-//     any Z.  Not for 2NMS, whose early termination is per 4-frame word.
+//     any Z.  Not for 2NMS, whose early termination is per 4-frame word;
+//   the per-frame early stop with lane refill (decode_qc_refill_kernel) for the
+//     regular base, every kind but 2NMS.
 #include "qc_kernel.cuh"
 
 namespace ldpc {
@@ -24,6 +26,18 @@ const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2,
 {
     LDPC_QC_KINDS(6, true, 8, true)  // regular (3,6) rate-1/2 QC, 8x16 base (Z = 2^k)
     LDPC_QC_PAIR(10, 12) LDPC_QC_PAIR(14, 8) LDPC_QC_PAIR(18, 6) LDPC_QC_PAIR(24, 4)
+    return nullptr;
+}
+
+// per-frame early stop with lane refill (4 frames per CTA): the regular (3,6) base
+#define LDPC_QC_REFILL(KIND, D, EX, L, P2)                                          \
+    if (kind == KIND && dt == D && exact == EX && layers == L && pow2 == P2)           \
+        return (const void*)decode_qc_refill_kernel<KIND, D, EX, L, P2>;
+
+const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2)
+{
+    LDPC_QC_REFILL(KIND_MS, 6, true, 8, true) LDPC_QC_REFILL(KIND_OMS, 6, true, 8, true)
+    LDPC_QC_REFILL(KIND_NMS, 6, true, 8, true) LDPC_QC_REFILL(KIND_LEARNED, 6, true, 8, true)
     return nullptr;
 }
 

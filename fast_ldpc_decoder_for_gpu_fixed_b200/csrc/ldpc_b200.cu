@@ -99,8 +99,12 @@ struct ldpc_decoder {
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
-    const void* kfn_alt = nullptr;  // the same kernel with the other early-stop setting (paths 1 and 3)
-    int path = 0;     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA
+    const void* kfn_alt = nullptr;  // the same kernel with the other early-stop setting (paths 1, 3 and 4)
+    // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA,
+    // 3 = one frame per CTA, 4 = QC register-message, 2 frames per CTA, 5 = QC register-message with
+    // per-frame early stop and lane refill (persistent CTAs)
+    int path = 0;
+    int sms = 0;  // path 5: multiprocessors (grid size)
     int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
     uint16_t* d_lut = nullptr;  // LDPC_LEARNED magnitude tables [its][2][128]
@@ -308,6 +312,7 @@ const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et, int wpt);
+const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
 }
@@ -319,7 +324,9 @@ static size_t qc_smem(const ldpc_code* c, int wpt) { return (size_t)c->n * 4 * w
 // The QC register-message kernel for the code, or null: 4 frames per CTA (*wpt = 2)
 // when an instantiation matches the code's shape, else 2 frames per CTA (*wpt = 1)
 // with the smallest instantiated row degree that holds it.  Fills q for that layout.
-static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false, int* wpt_out = nullptr)
+// refill: the per-frame early-stop kernel with lane refill (4 frames per CTA) instead.
+static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false, int* wpt_out = nullptr,
+                                 bool refill = false)
 {
     if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > (1 << 20)) return nullptr;
     int deg[QC_MAX_LAYERS], dt = 0;
@@ -339,8 +346,9 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool
     const int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
     const bool e = et && kind != LDPC_2NMS;
     int wpt = 2;
-    const void* f = kernel_table_qc(k, dt, exact, c->mb, pow2, e, 2);
-    if (!f) {
+    const void* f =
+        refill ? kernel_table_qc_refill(k, dt, exact, c->mb, pow2) : kernel_table_qc(k, dt, exact, c->mb, pow2, e, 2);
+    if (!f && !refill) {
         wpt = 1;
         for (int D : {10, 14, 18, 24})
             if (D >= dt && (f = kernel_table_qc(k, D, false, c->mb, false, e, 1))) break;
@@ -478,8 +486,10 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (!out || !c) return fail(LDPC_ERR_ARG, "ldpc_decoder_create: null pointer");
     if (kind < LDPC_MS || kind > LDPC_LEARNED) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
     if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
-    if (flags & ~LDPC_FLAG_EARLY_STOP) return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
-    const bool early = flags & LDPC_FLAG_EARLY_STOP;
+    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES))
+        return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
+    const bool per_frame = flags & LDPC_FLAG_EARLY_STOP_FRAMES;
+    const bool early = (flags & LDPC_FLAG_EARLY_STOP) || per_frame;
     if (early && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     const int pack_req = pack;
@@ -549,6 +559,12 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->grid_mult = 4;
         d->smem = (int)frame_smem;
         d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32));
+    } else if (per_frame && qk && qc_wpt == 2 && qc_smem(c, 2) + QC_STAGE * (size_t)c->n <= (size_t)smem_max &&
+               (d->kfn = qc_kernel_for(c, kind, d->qcp, true, nullptr, true))) {
+        d->path = 5;
+        d->pack = LDPC_PACK_F16X2;
+        d->smem = (int)(qc_smem(c, 2) + QC_STAGE * (size_t)c->n);  // the APP and the staged frames
+        d->threads = c->z;
     } else if (qk && qc_smem(c, qc_wpt) + lut_smem <= (size_t)smem_max) {
         QCParams alt;
         d->kfn = qk;
@@ -568,6 +584,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->kfn = kernel_for(pack, kind, degree_variant(c));
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    }
+    if (per_frame && d->path != 3 && d->path != 5) {
+        decoder_free(d);
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_FRAMES: needs the QC register kernel with 4 frames per "
+                                          "CTA (the regular 8x16 base, Z a power of two) or LDPC_PACK_FRAME");
+    }
+    if (d->path == 5) {
+        cudaError_t ec = cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, dev);
+        if (ec != cudaSuccess) {
+            decoder_free(d);
+            return fail(LDPC_ERR_CUDA, "decoder setup: %s", cudaGetErrorString(ec));
+        }
     }
     cudaError_t e1 = ldpc_internal_raise_smem(d->kfn, d->smem);
     if (e1 == cudaSuccess && d->kfn_alt) e1 = ldpc_internal_raise_smem(d->kfn_alt, d->smem);
@@ -719,6 +747,15 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.msg_out = msg_out;
     if (d->path == 4 && iters_out)  // each 2-frame CTA raises its word's count with atomicMax
         CUDA_TRY(cudaMemsetAsync(iters_out, 0, sizeof(int32_t) * (size_t)words, st));
+    if (d->path == 5) {
+        // persistent CTAs, at most the resident ones, each decoding a strided share of the frames
+        if (iters > 255) return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_FRAMES: at most 255 iterations");
+        long long frames = 4 * words;
+        const long long grid = std::min(words, (long long)d->ctas_per_sm * d->sms);
+        void* a[] = {(void*)&d->qcp, (void*)&J, (void*)&frames};
+        CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
+        return LDPC_OK;
+    }
     void* args[] = {(d->path == 1 || d->path == 4) ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
     CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
@@ -750,7 +787,7 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
-    if ((d->path == 3 || d->path == 4) && (d_app || d_msg))
+    if (d->path >= 3 && (d_app || d_msg))
         return fail(LDPC_ERR_UNSUPPORTED, "this decoder (path %d) has no state dumps", d->path);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
@@ -763,6 +800,9 @@ extern "C" int ldpc_simulate(ldpc_decoder* d, size_t n_words, int iters, float s
 {
     if (!d || !d_counts) return fail(LDPC_ERR_ARG, "simulate: null pointer");
     if (d->kind == LDPC_XMS) return fail(LDPC_ERR_UNSUPPORTED, "simulate: xMS reads word-interleaved input; use OMS");
+    if (d->path == 5)
+        return fail(LDPC_ERR_UNSUPPORTED, "simulate: LDPC_FLAG_EARLY_STOP_FRAMES decoders read LLRs from memory "
+                                          "(ldpc_channel_awgn, then ldpc_decode_device)");
     if (iters < 1) return fail(LDPC_ERR_ARG, "simulate: iterations must be >= 1 (got %d)", iters);
     if (n_words < 1 || n_words > d->nb_words)
         return fail(LDPC_ERR_SHAPE, "simulate: %zu words requested, decoder holds %zu", n_words, d->nb_words);

@@ -208,7 +208,7 @@ __device__ __forceinline__ uint32_t floor_scale(uint32_t m, uint32_t k, uint32_t
 // row magnitudes from |min1| (a1) and |min2| (a2); lk, lb: the LEARNED (k, k), (b, b) words
 template <int KIND>
 __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2, uint32_t lk,
-                                     uint32_t lb)
+                                     uint32_t lb, uint32_t clip = C31)
 {
     if (KIND == KIND_LEARNED) {
         // clamp(floor(a * k) - offset, 0, 31) = min(round(relu(a * k + b)), 31), b = -offset - 15/32:
@@ -222,9 +222,9 @@ __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint
     } else if (KIND == KIND_OMS) {
         c1 = fma_relu(a2, ONE, NEG1);
         c2 = fma_relu(a1, ONE, NEG1);
-        if (!noclip) {
-            c1 = hmin(c1, C31);
-            c2 = hmin(c2, C31);
+        if (!noclip) {  // clip: C31, or per lane C31 / no clip (the first iteration of a lane's frame)
+            c1 = hmin(c1, clip);
+            c2 = hmin(c2, clip);
         }
     } else {
         c2 = floor_scale(a1, C075, CNEG0375);
@@ -244,9 +244,11 @@ __device__ __forceinline__ void learned_kb(const uint16_t* lut, uint32_t& lk, ui
     }
 }
 
-template <int KIND, int DT, bool EXACT>
+// LANES: ov counts odd rows per fp16 lane (bit 0 and bit 16 fields) instead of in total,
+// and clip is the per-lane OMS clip word
+template <int KIND, int DT, bool EXACT, bool LANES = false>
 __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov,
-                                    uint32_t lk, uint32_t lb)
+                                    uint32_t lk, uint32_t lb, uint32_t clip = C31)
 {
     uint32_t ut[DT];
     uint32_t mn1 = C127, mn2 = C127;
@@ -263,7 +265,7 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
     }
     const uint32_t a1 = habs(mn1), a2 = habs(mn2);
     uint32_t c1, c2;
-    mags<KIND>(a1, a2, noclip, c1, c2, lk, lb);
+    mags<KIND>(a1, a2, noclip, c1, c2, lk, lb, clip);
     const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
     const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
 #pragma unroll
@@ -279,7 +281,10 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
             b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)
         }
     }
-    ov += __popc(mn1 & SIGN);  // odd (row, frame) pairs
+    if (LANES)
+        ov += (mn1 & SIGN) >> 15;  // odd rows of each lane's frame
+    else
+        ov += __popc(mn1 & SIGN);  // odd (row, frame) pairs
 }
 }  // namespace h2
 

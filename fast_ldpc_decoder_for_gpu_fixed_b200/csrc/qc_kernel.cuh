@@ -216,4 +216,346 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     }
 }
 
+// ---- per-frame early stop with lane refill (decoder path 5) ----
+//
+// The 4 frames of a CTA (the fp16 halves of its two pair-words, "lanes" 0..3) are
+// independent: nothing in the row update mixes lanes.  So each lane can run its own
+// frame on its own schedule: the odd-row count, the syndrome check and the iteration
+// limit are evaluated per lane, the learned constants and the OMS first-iteration
+// clip follow each lane's own iteration number, and when a lane's frame stops the
+// CTA writes that frame's decisions and iteration count, puts its next frame into the
+// lane and zeroes the lane's messages.  CTAs are persistent: CTA c of G decodes
+// frames c, c + G, c + 2G, ... (static, so no atomics; at tens of frames per CTA the
+// per-frame iteration counts average out), and keeps its next QC_STAGE frames' LLRs
+// in shared memory, copied with cp.async when the previous ones were taken, so that a
+// refill does not wait on global memory.  A CTA exits when every lane is idle.  Each
+// frame's decisions and iteration count are those of decoding it alone, with the
+// early-stop rule (odd rows within the slack, then the syndrome) applied to that
+// frame only.
+
+constexpr int QC_LUT_ITS = 32;  // LDPC_LEARNED iteration rows (LDPC_LEARNED_MAX_ITERS)
+constexpr int QC_STAGE = 4;     // staged frames per CTA (a refill takes at most 4)
+
+// bit i set when lane i's frame has a row of odd hard-decision parity among rows k
+// of layers [L0, L1)
+template <int DT, bool EXACT, int L0, int L1, bool POW2>
+__device__ __noinline__ unsigned qc_rows_unsat_lanes(const QCParams& Q, const char* appb, int k)
+{
+    uint32_t bad0 = 0, bad1 = 0;
+    const int kb = 8 * k;
+#pragma unroll
+    for (int l = L0; l < L1; l++) {
+        const int d = EXACT ? DT : Q.deg[l];
+        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                const uint2 v = *reinterpret_cast<const uint2*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb));
+                acc0 ^= qc_zero_bits(v.x);
+                acc1 ^= qc_zero_bits(v.y);
+            }
+        }
+        bad0 |= acc0;
+        bad1 |= acc1;
+    }
+    return ((bad0 >> 15) & 1u) | ((bad0 >> 30) & 2u) | ((bad1 >> 13) & 4u) | ((bad1 >> 28) & 8u);
+}
+
+// CTA-wide OR of a lane mask through the shared slot *s (zero on entry); every thread calls it
+__device__ __forceinline__ unsigned cta_or_lanes(unsigned m, unsigned* s)
+{
+    const unsigned lanes = __activemask();
+    const unsigned w = __reduce_or_sync(lanes, m);
+    if (w && (int)(threadIdx.x & 31) == __ffs(lanes) - 1) atomicOr(s, w);
+    __syncthreads();
+    return *s;
+}
+
+// one frame's int8 LLRs (src: global memory, or a staging slot in shared memory) into
+// lane `lane` of the biased APP (apph[4 v + lane]), 4 variables per thread and step
+template <bool GLOBAL>
+__device__ __forceinline__ void qc_put_lane(const int8_t* src, uint16_t* apph, int n, int lane)
+{
+    if ((n & 3) == 0) {
+        const uint32_t* s4 = reinterpret_cast<const uint32_t*>(src);
+        for (int q = threadIdx.x; q < (n >> 2); q += blockDim.x) {
+            const uint32_t y = (GLOBAL ? __ldg(s4 + q) : s4[q]) ^ 0x7f7f7f7fu;  // see Access<PackF16x2>::pair
+            const uint32_t lo = h2::add(__byte_perm(y, 0x6464u, 0x4140), h2::CNEG1024);
+            const uint32_t hi = h2::add(__byte_perm(y, 0x6464u, 0x4342), h2::CNEG1024);
+            uint16_t* p = apph + 16 * q + lane;
+            p[0] = (uint16_t)lo;
+            p[4] = (uint16_t)(lo >> 16);
+            p[8] = (uint16_t)hi;
+            p[12] = (uint16_t)(hi >> 16);
+        }
+    } else {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const uint32_t y = (uint32_t)(uint8_t)(GLOBAL ? __ldg(src + v) : src[v]) ^ 0x7fu;
+            apph[4 * v + lane] = (uint16_t)h2::add(__byte_perm(y, 0x6464u, 0x4140), h2::CNEG1024);
+        }
+    }
+}
+
+// starts the copy of frame f's LLRs into a staging slot: cp.async (16-byte pieces,
+// completed by cp.async.wait_all) when source and size allow it, else plain copies
+__device__ __forceinline__ void qc_stage_frame(const Job& J, int8_t* slot, int n, long long f, bool async16)
+{
+    const int8_t* src = J.llr + f * n;
+    if (async16) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(slot);
+        for (int c = threadIdx.x; c < (n >> 4); c += blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * c), "l"(src + 16 * c) : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    } else {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) slot[v] = __ldg(src + v);
+    }
+}
+
+// lane `lane`'s hard decisions (x > 0, i.e. biased b < 127) as frame f of the output
+__device__ __forceinline__ void qc_store_lane(const Job& J, const uint16_t* apph, int n, long long f, int lane)
+{
+    if (!J.out) return;
+    auto bit = [&](int v) { return (uint32_t)((apph[4 * v + lane] & 0x7fffu) < 0x57f0u); };
+    if (!J.out_packed) {
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + f * n;
+        if ((n & 3) == 0) {
+            uint32_t* o4 = reinterpret_cast<uint32_t*>(o);
+            for (int q = threadIdx.x; q < (n >> 2); q += blockDim.x)
+                o4[q] = bit(4 * q) | (bit(4 * q + 1) << 8) | (bit(4 * q + 2) << 16) | (bit(4 * q + 3) << 24);
+        } else {
+            for (int v = threadIdx.x; v < n; v += blockDim.x) o[v] = (uint8_t)bit(v);
+        }
+    } else {
+        const int nb = (n + 7) >> 3;
+        uint8_t* o = reinterpret_cast<uint8_t*>(J.out) + f * nb;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            uint32_t acc = 0;
+            for (int j = 0; j < 8; j++) {
+                const int v = 8 * b + j;
+                if (v < n) acc |= bit(v) << j;
+            }
+            o[b] = (uint8_t)acc;
+        }
+    }
+}
+
+// frames: 4 * words of this launch.  Dynamic shared memory: the APP (8n bytes) and
+// QC_STAGE staging slots of n bytes.  J.iters <= 255 (per-lane iteration counts are
+// byte fields).  J.iters_out, when set, receives one count per frame.
+template <int KIND, int DT, bool EXACT, int L, bool POW2>
+__global__ void __launch_bounds__(256, 2) decode_qc_refill_kernel(const __grid_constant__ QCParams Q, const Job J,
+                                                                  long long frames)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint16_t* apph = reinterpret_cast<uint16_t*>(smem_raw);  // [n][4 lanes]
+    char* appb = reinterpret_cast<char*>(smem_raw);
+    int8_t* stage = reinterpret_cast<int8_t*>(smem_raw + 8 * (size_t)Q.n);  // [QC_STAGE][n]
+    const int k = threadIdx.x;
+    const long long G = gridDim.x;
+    const bool async16 = ((reinterpret_cast<uintptr_t>(J.llr) | (uintptr_t)Q.n) & 15) == 0;
+    __shared__ unsigned s_cnt[2][2];   // odd rows per lane (16-bit fields of pair-words 0, 1), by iteration parity
+    __shared__ unsigned s_bad[2][2];   // unsatisfied lanes of the two check stages, by iteration parity
+    __shared__ long long s_frame[4];   // frame of each lane, -1 = idle
+    __shared__ long long s_slot[QC_STAGE];  // frame staged in each slot, -1 = none (the frames run out)
+    __shared__ int s_src[4];           // refill: the slot each done lane takes
+    __shared__ int s_head;             // the slot holding the earliest staged frame
+    __shared__ __align__(16) uint32_t s_kb[2][4];  // LEARNED, per row group: k words of pair-words 0, 1, then b words
+    __shared__ uint32_t s_clip[2];     // OMS: clip words of second-group rows (per lane: 31, or none in iteration 0)
+    __shared__ uint16_t s_tab[QC_LUT_ITS][2][2];  // LEARNED: fp16 (k, b) per iteration and row group
+
+    if (k < 2) {
+        s_cnt[0][k] = s_cnt[1][k] = 0;
+        s_bad[0][k] = s_bad[1][k] = 0;
+    }
+    if (KIND == KIND_LEARNED)
+        for (int i = k; i < 4 * J.lut_its; i += blockDim.x)
+            s_tab[i >> 2][(i >> 1) & 1][i & 1] = J.lut[(i >> 2) * 256 + ((i >> 1) & 1) * 128 + 2 * (i & 1)];
+    if (k == 0) {
+        // this CTA's frames: blockIdx.x + G j; lanes take j = 0..3, the slots j = 4..7
+        for (int i = 0; i < 4; i++) {
+            const long long f = blockIdx.x + G * i;
+            s_frame[i] = f < frames ? f : -1;
+        }
+        for (int i = 0; i < QC_STAGE; i++) {
+            const long long f = blockIdx.x + G * (4 + i);
+            s_slot[i] = f < frames ? f : -1;
+        }
+        s_head = 0;
+    }
+    __syncthreads();
+    long long next = blockIdx.x + G * (4 + QC_STAGE);  // the next frame to stage (uniform)
+#pragma unroll
+    for (int i = 0; i < QC_STAGE; i++)
+        if (s_slot[i] >= 0) qc_stage_frame(J, stage + (size_t)i * Q.n, Q.n, s_slot[i], async16);
+    unsigned act = 0;  // lanes holding a frame (uniform across the CTA, like itp)
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const long long f = s_frame[i];
+        if (f >= 0) {
+            act |= 1u << i;
+            qc_put_lane<true>(J.llr + f * Q.n, apph, Q.n, i);
+        }
+    }
+    if (!act) {
+        if (async16) asm volatile("cp.async.wait_all;" ::: "memory");
+        return;
+    }
+    uint32_t itp = 0;  // iterations run by each lane's frame, byte i = lane i
+
+    uint32_t msg[2][L][DT];
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int j = 0; j < DT; j++) msg[w][l][j] = 0;
+
+    int par = 0;
+    for (;;) {
+        // this iteration's per-lane constants (the barrier also publishes refilled lanes)
+        if (k < 4) {
+            const int it = (itp >> (8 * k)) & 0xff;
+            uint16_t* h = reinterpret_cast<uint16_t*>(s_kb);
+            if (KIND == KIND_LEARNED) {
+                const int t = it < J.lut_its ? it : J.lut_its - 1;
+#pragma unroll
+                for (int g = 0; g < 2; g++) {
+                    h[8 * g + k] = s_tab[t][g][0];
+                    h[8 * g + 4 + k] = s_tab[t][g][1];
+                }
+            }
+            if (KIND == KIND_OMS)
+                reinterpret_cast<uint16_t*>(s_clip)[k] = (J.quirk && it == 0) ? 0x7bffu : 0x4fc0u;
+        }
+        __syncthreads();
+
+        uint32_t ov0 = 0, ov1 = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+            int kk = 8 * k;
+            asm volatile("" : "+r"(kk));
+            int off[DT];
+            uint32_t b0[DT], b1[DT];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    off[j] = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk);
+                    const uint2 v = *reinterpret_cast<const uint2*>(appb + off[j]);
+                    b0[j] = v.x;
+                    b1[j] = v.y;
+                }
+            }
+            uint32_t lk0 = 0, lk1 = 0, lb0 = 0, lb1 = 0;
+            if (KIND == KIND_LEARNED) {
+                const uint4 q = reinterpret_cast<const uint4*>(s_kb)[Q.cls[l]];
+                lk0 = q.x;
+                lk1 = q.y;
+                lb0 = q.z;
+                lb1 = q.w;
+            }
+            uint32_t cl0 = h2::C31, cl1 = h2::C31;
+            if (KIND == KIND_OMS && Q.cls[l]) {
+                cl0 = s_clip[0];
+                cl1 = s_clip[1];
+            }
+            h2::row<KIND, DT, EXACT, true>(b0, msg[0][l], d, false, ov0, lk0, lb0, cl0);
+            h2::row<KIND, DT, EXACT, true>(b1, msg[1][l], d, false, ov1, lk1, lb1, cl1);
+#pragma unroll
+            for (int j = 0; j < DT; j++)
+                if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
+            if (l < L - 1) __syncthreads();  // the count's barrier closes the last layer
+        }
+        {
+            const unsigned lanes = __activemask();
+            const unsigned w0 = __reduce_add_sync(lanes, ov0), w1 = __reduce_add_sync(lanes, ov1);
+            if ((int)(threadIdx.x & 31) == __ffs(lanes) - 1) {
+                if (w0) atomicAdd(&s_cnt[par][0], w0);
+                if (w1) atomicAdd(&s_cnt[par][1], w1);
+            }
+        }
+        __syncthreads();
+        const unsigned cnt01 = s_cnt[par][0], cnt23 = s_cnt[par][1];
+        if (k == 0) {  // slots of the next iteration (their last readers are past this iteration's barriers)
+            s_cnt[par ^ 1][0] = s_cnt[par ^ 1][1] = 0;
+            s_bad[par ^ 1][0] = s_bad[par ^ 1][1] = 0;
+        }
+        itp += (act & 1u) | ((act & 2u) << 7) | ((act & 4u) << 14) | ((act & 8u) << 21);
+
+        unsigned cand = 0, limit = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (!((act >> i) & 1u)) continue;
+            const unsigned c = ((i < 2 ? cnt01 : cnt23) >> (16 * (i & 1))) & 0xffffu;
+            if (J.early && c <= J.early_slack) cand |= 1u << i;
+            if ((int)((itp >> (8 * i)) & 0xffu) >= J.iters) limit |= 1u << i;
+        }
+        unsigned pass = 0;
+        if (cand) {
+            // staged like the per-word kernel: the first layers reject most non-codewords
+            constexpr int LS = L > 2 ? 2 : L;
+            pass = cand & ~cta_or_lanes(qc_rows_unsat_lanes<DT, EXACT, 0, LS, POW2>(Q, appb, k) & cand, &s_bad[par][0]);
+            if (LS < L && pass)
+                pass &= ~cta_or_lanes(qc_rows_unsat_lanes<DT, EXACT, LS, L, POW2>(Q, appb, k) & pass, &s_bad[par][1]);
+        }
+        const unsigned done = pass | limit;
+        if (done) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if (!((done >> i) & 1u)) continue;
+                const long long f = s_frame[i];
+                qc_store_lane(J, apph, Q.n, f, i);
+                if (k == 0 && J.iters_out) J.iters_out[f] = (int32_t)((itp >> (8 * i)) & 0xffu);
+            }
+            if (async16) asm volatile("cp.async.wait_all;" ::: "memory");
+            __syncthreads();  // staged frames landed; decisions and s_frame read before they are replaced
+            const int head = s_head;
+            const int nd = __popc(done);
+            if (k == 0) {
+                // done lanes take the staged frames in order (the earliest first)
+                int c = 0;
+                for (int i = 0; i < 4; i++)
+                    if ((done >> i) & 1u) {
+                        const int sl = (head + c++) % QC_STAGE;
+                        s_src[i] = sl;
+                        s_frame[i] = s_slot[sl];
+                    }
+            }
+            __syncthreads();
+            uint32_t keep0 = 0xffffffffu, keep1 = 0xffffffffu;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if (!((done >> i) & 1u)) continue;
+                if (s_frame[i] >= 0)
+                    qc_put_lane<false>(stage + (size_t)s_src[i] * Q.n, apph, Q.n, i);
+                else
+                    act &= ~(1u << i);
+                itp &= ~(0xffu << (8 * i));
+                if (i < 2)
+                    keep0 &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
+                else
+                    keep1 &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
+            }
+            if (!act) break;
+            __syncthreads();  // the taken slots are read before new frames are copied into them
+            if (k == 0) s_head = (head + nd) % QC_STAGE;
+            for (int c = 0; c < nd; c++) {
+                const int sl = (head + c) % QC_STAGE;
+                const long long f = next < frames ? next : -1;
+                next += G;
+                if (k == 0) s_slot[sl] = f;  // read again only after the next refill's barriers
+                if (f >= 0) qc_stage_frame(J, stage + (size_t)sl * Q.n, Q.n, f, async16);
+            }
+#pragma unroll
+            for (int l = 0; l < L; l++)
+#pragma unroll
+                for (int j = 0; j < DT; j++) {
+                    msg[0][l][j] &= keep0;
+                    msg[1][l][j] &= keep1;
+                }
+        }
+        par ^= 1;
+    }
+}
+
 }  // namespace ldpc

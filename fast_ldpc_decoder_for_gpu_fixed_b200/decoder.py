@@ -75,7 +75,9 @@ def _ptr(x):
 class Decoder:
     """One ldpc_decoder: ``kind`` in MS/OMS/NMS/2NMS/XMS/LEARNED, ``nb_frames`` 32-bit
     lanes (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8;
-    ``early_stop`` sets LDPC_FLAG_EARLY_STOP (syndrome early stop per word)."""
+    ``early_stop`` sets LDPC_FLAG_EARLY_STOP (syndrome early stop per word), or with
+    ``early_stop="frame"`` LDPC_FLAG_EARLY_STOP_FRAMES (per frame, finished frames'
+    slots refilled; iteration counts per frame)."""
 
     def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO", early_stop=False):
         if isinstance(code, str):
@@ -87,9 +89,11 @@ class Decoder:
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().ldpc_decoder_create(
             ctypes.byref(h), self.native.handle, _lib.KINDS[self.kind], self.nb_frames,
-            _lib.PACKS[pack.upper()], _lib.FLAG_EARLY_STOP if early_stop else 0))
+            _lib.PACKS[pack.upper()], _lib.FLAG_EARLY_STOP_FRAMES if early_stop == "frame"
+            else (_lib.FLAG_EARLY_STOP if early_stop else 0)))
         self.handle = h
         self.early_stop = bool(early_stop)
+        self.per_frame = early_stop == "frame"
         self.early_slack = _lib.EARLY_STOP_DEFAULT_SLACK
 
     def info(self):

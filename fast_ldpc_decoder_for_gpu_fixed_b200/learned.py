@@ -193,7 +193,8 @@ def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewor
     (with LDPC_LEARNED ``constants`` = (offsets, scales)) at ``ebn0`` dB over at
     least ``frames`` frames of seeded random codewords: channel kernel, decode
     with per-word iteration counts, error-count kernel.  Errors are counted over
-    all n bits.  Returns dict(frames, bit_errors, frame_errors, fer, ber, mean_iters)."""
+    all n bits.  ``early_stop="frame"``: the per-frame early stop, and mean_iters is
+    per frame.  Returns dict(frames, bit_errors, frame_errors, fer, ber, mean_iters)."""
     import torch
     words = min(words_per_call, max(1, (frames + 3) // 4))
     dec = Decoder(code, kind, nb_frames=words, pack=pack, early_stop=early_stop)
@@ -202,7 +203,8 @@ def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewor
     cw = torch.from_numpy(random_codewords(code, n_codewords, seed + 3)).cuda()
     llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
     hard = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")
-    its = torch.zeros(words, dtype=torch.int32, device="cuda")
+    per_frame = early_stop == "frame"  # iteration counts per frame, not per word
+    its = torch.zeros(4 * words if per_frame else words, dtype=torch.int32, device="cuda")
     it_sum = torch.zeros(1, dtype=torch.int64, device="cuda")
     counts = torch.zeros(3, dtype=torch.int64, device="cuda")
     s = sigma_for(ebn0, code.n_info / code.n)
@@ -219,7 +221,7 @@ def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewor
     dec.close()
     f, be, fe = (int(x) for x in counts.cpu().tolist())
     return {"frames": f, "bit_errors": be, "frame_errors": fe, "fer": fe / f, "ber": be / (f * code.n),
-            "mean_iters": float(it_sum.item()) / (calls * words)}
+            "mean_iters": float(it_sum.item()) / (calls * its.numel())}
 
 
 def save_constants(path, offsets, scales, **meta):

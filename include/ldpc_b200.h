@@ -131,12 +131,23 @@ void ldpc_code_destroy(ldpc_code* code);
 #define LDPC_FLAG_EARLY_STOP 1
 #define LDPC_EARLY_STOP_DEFAULT_SLACK 128
 
+/* Per-frame early stop (implies LDPC_FLAG_EARLY_STOP): the rule above applied to
+ * each frame alone (its own odd rows against `slack`, its own syndrome), and a
+ * frame that stops frees its slot for the next frame.  Decoder path 5: the QC
+ * register kernel with 4 frames per CTA (ldpc_code_create_qc, the regular 8x16
+ * base with Z a power of two, every kind but 2NMS) run as persistent CTAs that
+ * refill finished frame slots with prefetched frames; with LDPC_PACK_FRAME (path 3)
+ * it is that path's own rule.  Other decoders fail with LDPC_ERR_UNSUPPORTED.  On
+ * path 5: d_iters_out receives one count per frame (4*n_words entries), iters <= 255,
+ * no state dumps and no ldpc_simulate. */
+#define LDPC_FLAG_EARLY_STOP_FRAMES 4
+
 /* nb_frames counts 32-bit lanes like the reference's constructor argument:
  * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
  * Unlike the reference (decoder_oms/CGPU_Decoder_OMS_SIMD.cu:101-105), any
  * nb_frames >= 1 is accepted.  The decoder owns its device buffers; the code
  * may be destroyed after this call.  pack = LDPC_PACK_*; flags = 0 or
- * LDPC_FLAG_EARLY_STOP. */
+ * LDPC_FLAG_EARLY_STOP, LDPC_FLAG_EARLY_STOP_FRAMES. */
 int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* code, int kind, size_t nb_frames,
                         int pack, int flags);
 
@@ -232,7 +243,8 @@ size_t ldpc_train_stash_bytes(const ldpc_decoder* dec, size_t frames, int iters)
 
 /* Turns the syndrome early stop on or off and sets its slack (default
  * LDPC_EARLY_STOP_DEFAULT_SLACK).  Turning it on for a decoder created without
- * LDPC_FLAG_EARLY_STOP fails for the 2-frames-per-CTA kernel (path 2). */
+ * LDPC_FLAG_EARLY_STOP fails for the 2-frames-per-CTA kernel (path 2).  On path 5
+ * turning it off keeps the per-frame scheduling: every frame runs `iters`. */
 int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
 
 /* info[0..7] = kind, pack, nb_frames (words), threads per CTA, shared bytes
@@ -240,7 +252,8 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
  * scheduled, 1 = QC register-message, 2 = level scheduled with 2 frames per
  * CTA: LDPC_PACK_F16X2 for every kind but 2NMS, 3 = one frame per CTA with
  * packed row state: LDPC_PACK_FRAME, 4 = QC register-message with 2 frames per
- * CTA, see LDPC_PACK_F16X2) */
+ * CTA, see LDPC_PACK_F16X2, 5 = QC register-message with per-frame early stop,
+ * see LDPC_FLAG_EARLY_STOP_FRAMES) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);

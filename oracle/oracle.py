@@ -76,7 +76,8 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     device layouts (n*nframes and e*nframes bytes).  ``early_stop``: the
     syndrome early stop of LDPC_FLAG_EARLY_STOP (per 4-frame word) with
     ``early_slack`` (ldpc_decoder_set_early_stop); ``per_frame``: every frame
-    stops on its own and ``iters`` has one entry per frame (LDPC_PACK_FRAME);
+    stops on its own and ``iters`` has one entry per frame (LDPC_PACK_FRAME,
+    LDPC_FLAG_EARLY_STOP_FRAMES);
     ``pairs``: frames 4g, 4g+1 and 4g+2, 4g+3 stop as pairs and ``iters`` has the
     larger count of each word (the 2-frame QC kernel, decoder path 4).
     """
