@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--ebn0", type=float, default=None, help="default 2.25 dB (learned), 2.0 (oms, table), 1.4 (ira)")
     ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira", "batch"])
     ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
+    ap.add_argument("--per-frame", action="store_true",
+                    help="early stop per frame with slot refill (LDPC_FLAG_EARLY_STOP_FRAMES) instead of per 4-frame word")
     ap.add_argument("--fer-frames", type=int, default=1 << 20)
     ap.add_argument("--no-sweep", dest="sweep", action="store_false",
                     help="skip the learned-vs-plain ratio over Eb/N0 1.5..2.5 dB")
@@ -379,13 +381,14 @@ def main():
     early = args.workload in ("learned", "ira")
     constants = load_constants(TRAINED)[:2] if learned else None
     kind = "LEARNED" if learned else args.kind
-    dec = Decoder(code, kind, nb_frames=words, pack=args.pack, early_stop=early)
+    es = ("frame" if args.per_frame else True) if early else False
+    dec = Decoder(code, kind, nb_frames=words, pack=args.pack, early_stop=es)
     if constants is not None:
         dec.set_learned(*constants)
     if early and args.slack is not None:
         dec.set_early_stop(True, args.slack)
     info = dec.info()
-    per_frame = info["path"] == 3
+    per_frame = info["path"] in (3, 5)  # iteration counts per frame
     stream = torch.cuda.current_stream()
     d_llr = torch.from_numpy(llr.reshape(-1)).cuda()
     d_out = torch.empty(args.frames * code.n, dtype=torch.uint8, device="cuda")
@@ -446,7 +449,7 @@ def main():
     # equal-FER evidence on more frames (untimed)
     fer_cmp = None
     if learned and rank == 0 and args.fer_frames > 0:
-        fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=True)
+        fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=es)
         fp = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames)
         fer_cmp = {"frames": fl["frames"], "ebn0_db": args.ebn0,
                    "learned_early_stop": {"fer": fl["fer"], "frame_errors": fl["frame_errors"], "ber": fl["ber"],
@@ -460,11 +463,12 @@ def main():
 
     # roofline of the decode kernel (one launch per step), from the iterations it executed
     int_peak = _int_peak()
+    one_lane = info["path"] == 3  # one frame per thread lane: one int32 op per frame-edge-update
     if per_frame:
         edge_updates = float(d_its.sum().item()) * code.e
     else:
         edge_updates = float(d_its.sum().item()) * 4 * code.e if early else float(args.frames) * code.e * args.iters
-    alg_ops = (1.0 if per_frame else 2.0) * edge_updates
+    alg_ops = (1.0 if one_lane else 2.0) * edge_updates
     achieved = alg_ops / (ms_step * 1e-3) / 1e12
     hbm_bytes = args.frames * code.n * 2  # int8 LLRs in + 0/1 bytes out
     peaks = _measured_peaks()
@@ -482,7 +486,8 @@ def main():
 
     if rank == 0:
         kernel = {0: "level_scheduled", 1: "qc_register_messages", 2: "level_scheduled_2f",
-                  3: "frame_per_cta_packed_rows"}[info["path"]]
+                  3: "frame_per_cta_packed_rows", 4: "qc_register_messages_2f",
+                  5: "qc_register_messages_per_frame_refill"}[info["path"]]
         workload = workload_name(args)
         line = {
             "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s", "n_gpus": world,
@@ -490,7 +495,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic (seeded codewords, AWGN, reference quantiser)",
             "config": {"workload": workload, "kind": kind, "pack": info["pack"], "frames_per_gpu": args.frames,
-                       "max_iterations": args.iters, "early_stop": early, "mean_iterations": mean_iters,
+                       "max_iterations": args.iters, "early_stop": ("per_frame" if per_frame else "per_word") if early
+                       else False, "mean_iterations": mean_iters,
                        "ebn0_db": args.ebn0, "batch_fer": fer, "batch_ber": ber,
                        "l2": ("inputs %d MB: L2 flushed (256 MB write) between steps, outside the timed spans" % (
                            llr.nbytes // 2**20)) if flush else
@@ -505,7 +511,7 @@ def main():
             "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
                          "frac": achieved / int_peak, "traffic": None,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
-                         "ops_per_edge_update": 1.0 if per_frame else 2.0,
+                         "ops_per_edge_update": 1.0 if one_lane else 2.0,
                          "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, all SMs)"},
             "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
                              "unit": "GB/s", "frac": (hbm_bytes / (ms_step * 1e-3) / 1e9) / peaks["hbm_gbs"]
@@ -533,8 +539,9 @@ def _sweep(code, constants, args, stream):
     cw = torch.from_numpy(random_codewords(code, 64, 77)).cuda()
     llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
     out = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")
-    its = torch.zeros(words, dtype=torch.int32, device="cuda")
-    ldec = Decoder(code, "LEARNED", nb_frames=words, early_stop=True)
+    es = "frame" if args.per_frame else True
+    its = torch.zeros(4 * words if args.per_frame else words, dtype=torch.int32, device="cuda")
+    ldec = Decoder(code, "LEARNED", nb_frames=words, early_stop=es)
     ldec.set_learned(*constants)
     pdec = Decoder(code, "OMS", nb_frames=words)
     rows = []
@@ -549,7 +556,7 @@ def _sweep(code, constants, args, stream):
                 st()
             ms = _timed(st, 10, stream, False) / 10
             r = evaluate(code, "LEARNED" if d_its is not None else "OMS", args.iters, e, 1 << 18,
-                         constants=constants if d_its is not None else None, early_stop=d_its is not None)
+                         constants=constants if d_its is not None else None, early_stop=es if d_its is not None else False)
             row[name] = {"gbps": 4 * words * code.n_info / (ms * 1e-3) / 1e9, "fer": r["fer"],
                          "frame_errors": r["frame_errors"], "mean_iters": r["mean_iters"]}
         row["ratio"] = row["learned_early_stop"]["gbps"] / row["plain_oms"]["gbps"]
