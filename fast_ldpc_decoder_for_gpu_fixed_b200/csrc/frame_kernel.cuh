@@ -141,11 +141,6 @@ __device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const 
     return bad;
 }
 
-__device__ __forceinline__ int sat8(int x) { return min(max(x, -128), 127); }
-
-// One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134)
-// with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
-// sign bit j set when edge j's message is positive.  Returns the new state.
 // The row a thread updates in one level: its record (columns, degree, class;
 // see Plan::rowrec) and its index.  Records do not depend on the frame's
 // state, so they are loaded two levels ahead: with one CTA per SM nothing else
@@ -186,39 +181,86 @@ __device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow& x)
 // with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
 // sign bit j set when edge j's message is positive.  D: the row's degree (fully
 // unrolled).  Returns the new state.
+//
+// Two edges per 32-bit word: edges 2p and 2p+1 are the fp16 halves of pair p, in the
+// biased negated form of the F16X2 packing (b = 127 - x in [0, 255], integer-valued,
+// so every step is exact; see namespace h2).  Each half keeps its own running
+// (min1, min2, sign parity) over its edges; the halves are merged once per row.  An
+// odd degree's last pair carries a dummy edge x = -127 with no message: |u| = 127
+// equals the initial min1 and min2 and its sign is positive, so it changes nothing.
+// All edges whose |t| equals min1 get c1 (as in the reference); ties give c1 = c2 for
+// every kind served here, so the stored index (the first such edge) is exact.
 template <int KIND, int D>
 __device__ __forceinline__ uint32_t frame_row(int8_t* app, const FrameRow& row, uint32_t st, bool first, bool noclip,
                                               int& odd, const uint16_t* lut)
 {
-    int t[D];
-    const int oc1 = st & 0x7f, oc2 = (st >> 7) & 0x7f, oi = (st >> 14) & 0xf;
-    int mn1 = 127, mn2 = 127, i1 = 0, par = 0;
+    using namespace h2;
+    constexpr int NP = (D + 1) / 2;
+    uint32_t bt[NP], ut[NP];
+    // old messages: magnitude oc1 on edge oi, oc2 on the others, as fp16 pairs
+    const uint32_t oc1 = st & 0x7f, oc2 = (st >> 7) & 0x7f, oi = (st >> 14) & 0xf;
+    const uint32_t h22 = add(0x64006400u | oc2 | (oc2 << 16), CNEG1024);
+    const uint32_t h12 = add(0x64006400u | oc1 | (oc2 << 16), CNEG1024);
+    const uint32_t h21 = add(0x64006400u | oc2 | (oc1 << 16), CNEG1024);
+    uint32_t mn1 = C127, mn2 = C127;
 #pragma unroll
-    for (int j = 0; j < D; j++) {
-        int x = app[row.col(j)];
+    for (int p = 0; p < NP; p++) {
+        const int j0 = 2 * p, j1 = 2 * p + 1;
+        // bytes x of the two edges; 127 - x as an unsigned byte is x ^ 0x7f (Access<PackF16x2>::pair)
+        uint32_t w = (uint32_t)(uint8_t)app[row.col(j0)];
+        w |= (j1 < D ? (uint32_t)(uint8_t)app[row.col(j1)] : 0x81u) << 16;
+        const uint32_t b = add((w ^ 0x007f007fu) | 0x64006400u, CNEG1024);
+        uint32_t m = 0;  // negated old messages (h2 convention: t = clamp(b - m))
         if (!first) {
-            const int mag = j == oi ? oc1 : oc2;
-            x = sat8(x - (((st >> (18 + j)) & 1) ? mag : -mag));
+            const uint32_t sb = st >> (18 + j0);  // bit 0: edge j0's message positive, bit 1: edge j1's
+            m = (oi == (uint32_t)j0 ? h12 : (oi == (uint32_t)j1 ? h21 : h22)) | ((sb & 1u) << 15) | ((sb & 2u) << 30);
+            if (j1 >= D) m &= 0xffffu;
         }
-        t[j] = x;
-        const int a = abs(x);  // 128 for -128, like vabs4
-        if (a < mn1) i1 = j;
-        mn2 = min(mn2, max(a, mn1));
-        mn1 = min(mn1, a);
-        par ^= x > 0;
+        bt[p] = hmin(fma_relu(m, NEG1, b), C255);
+        ut[p] = add(bt[p], CNEG127);
+        const uint32_t mx = max_xs(ut[p], mn1);
+        mn1 = min_xs(mn1, ut[p]);
+        mn2 = min_xs(mn2, mx);
     }
-    int c1, c2;
-    PackI8::mags<KIND>(mn1, mn2, noclip, c1, c2, lut);
-    uint32_t signs = 0;
+    // merge the halves: min1 of both, min2 = min(max of the two min1s, both min2s), parity of both
+    const uint32_t s1 = __byte_perm(mn1, 0, 0x1032), s2 = __byte_perm(mn2, 0, 0x1032);
+    const uint32_t m1 = min_xs(mn1, s1);  // |min1| in both halves, sign: the row's parity
+    const uint32_t m2 = min_xs(min_xs(mn2, s2), max_xs(mn1, s1));
+    const uint32_t a1 = habs(m1), a2 = habs(m2);
+    uint32_t c1, c2, ic1, ic2;
+    if (KIND == KIND_LEARNED) {
+        // the integer tables of the I8 packing (any constants): c1 = lut[min2], c2 = lut[min1]
+        ic1 = lut[add(a2, C1024) & 0x7fu];
+        ic2 = lut[add(a1, C1024) & 0x7fu];
+        c1 = add(0x64006400u | ic1 | (ic1 << 16), CNEG1024);
+        c2 = add(0x64006400u | ic2 | (ic2 << 16), CNEG1024);
+    } else {
+        h2::mags<KIND>(a1, a2, noclip, c1, c2, 0u, 0u);
+        ic1 = add(c1, C1024) & 0x7fu;
+        ic2 = add(c2, C1024) & 0x7fu;
+    }
+    const uint32_t c1s = c1 | (m1 & SIGN), c2s = c2 | (m1 & SIGN);
+    const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
+    uint32_t notmin = 0, sgn = 0;
 #pragma unroll
-    for (int j = 0; j < D; j++) {
-        const int s = par ^ (t[j] > 0);  // 1: positive message
-        const int mag = j == i1 ? c1 : c2;
-        app[row.col(j)] = (int8_t)sat8(t[j] + (s ? mag : -mag));
-        signs |= (uint32_t)s << j;
+    for (int p = 0; p < NP; p++) {
+        const int j0 = 2 * p, j1 = 2 * p + 1;
+        const uint32_t fl = add_sat(habs(ut[p]), na1);  // 0.0 on minimum edges, 1.0 elsewhere
+        const uint32_t mo = fma(fl, dcs, c1s) ^ (ut[p] & SIGN);
+        const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[p]), C255), C1024);  // 1024 + b: b in the low byte
+        app[row.col(j0)] = (int8_t)(bn ^ 0x7fu);
+        notmin |= ((fl >> 13) & 1u) << j0;
+        sgn |= ((mo >> 15) & 1u) << j0;  // the message -mo is positive
+        if (j1 < D) {
+            app[row.col(j1)] = (int8_t)((bn >> 16) ^ 0x7fu);
+            notmin |= ((fl >> 29) & 1u) << j1;
+            sgn |= (mo >> 31) << j1;
+        }
     }
-    odd += par;
-    return (uint32_t)c1 | ((uint32_t)c2 << 7) | ((uint32_t)i1 << 14) | (signs << 18);
+    const uint32_t mins = ~notmin & ((1u << D) - 1u);
+    const uint32_t i1 = mins ? (uint32_t)(__ffs(mins) - 1) : 0u;
+    odd += (m1 >> 15) & 1u;
+    return ic1 | (ic2 << 7) | (i1 << 14) | (sgn << 18);
 }
 
 // Dispatches a row to the unrolled update for its degree.  Rows of a level are
@@ -240,8 +282,10 @@ __device__ __forceinline__ uint32_t frame_row_any(int8_t* app, const FrameRow& r
     return st;  // not reached: degrees are 1..FRAME_MAX_DEGREE
 }
 
+// Launched with at most FRAME_MAX_THREADS (512) threads, so 128 registers a thread always
+// fit; a plain launch bound let the compiler settle at 64 and spill the degree-14 update.
 template <int KIND, int DT, bool EXACT, bool ET>
-__global__ void __launch_bounds__(FRAME_MAX_THREADS) decode_frame_kernel(const Plan P, const Job J)
+__global__ void __maxnreg__(128) decode_frame_kernel(const Plan P, const Job J)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                                  // [npad]

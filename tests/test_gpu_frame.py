@@ -57,6 +57,24 @@ def test_frame_early_stop_per_frame(cuda, name, slack):
     assert len(set(its.tolist())) > 3
 
 
+@pytest.mark.parametrize("llr_kind", ["uniform", "extreme"])
+@pytest.mark.parametrize("kind", ["MS", "OMS", "NMS", "LEARNED"])
+def test_frame_saturated_inputs(cuda, kind, llr_kind):
+    """Every int8 value (uniform) or the saturation edges -128/127 with many ties
+    (extreme): the wrapped |-128|, equal minima and odd row degrees (a dummy edge in
+    the last fp16 pair) on the 4000x2000 table (degrees 6 and 7)."""
+    code = load_table("4000x2000")
+    words = 6
+    llr = make_llr(llr_kind, 4 * words * code.n, 19)
+    constants = None
+    if kind == "LEARNED":
+        constants = (np.array([[1, -2], [0, 3]], dtype=np.int8), np.array([[200, 128], [96, 71]], dtype=np.uint8))
+        oracle.set_learned(*constants)
+    ref = oracle.decode(code, kind, llr, 8)
+    hard, _ = _decode(code, kind, llr, 8, words, constants=constants)
+    assert np.array_equal(hard, ref["hard"])
+
+
 def test_frame_learned(cuda):
     code = load_table("1944x972")
     words = 4
