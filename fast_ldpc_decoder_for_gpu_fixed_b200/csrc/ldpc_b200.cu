@@ -493,7 +493,13 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (early && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     const int pack_req = pack;
-    if (pack == LDPC_PACK_AUTO) pack = LDPC_PACK_SIMD4;
+    // AUTO: the QC register kernel where one fits (below); otherwise fp16x2 with 2 frames per
+    // CTA for the fixed-iteration MS / OMS / NMS / xMS decoders (the fastest level kernel where
+    // it applies), else SIMD4 (early stop; 2NMS; LEARNED, whose SIMD4 tables take any constants)
+    if (pack == LDPC_PACK_AUTO)
+        pack = !early && (kind == LDPC_MS || kind == LDPC_OMS || kind == LDPC_NMS || kind == LDPC_XMS)
+                   ? LDPC_PACK_F16X2
+                   : LDPC_PACK_SIMD4;
     if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_FRAME) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
     bool frame = pack == LDPC_PACK_FRAME;
     if (frame) pack = LDPC_PACK_I8;  // the arithmetic of that path
@@ -509,7 +515,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     QCParams probe;
-    bool qc_ok = (pack == LDPC_PACK_SIMD4 && pack_req == LDPC_PACK_AUTO) || pack == LDPC_PACK_F16X2;
+    bool qc_ok = pack_req == LDPC_PACK_AUTO || pack == LDPC_PACK_F16X2;
     int probe_wpt = 2;
     qc_ok = qc_ok && qc_kernel_for(c, kind, probe, false, &probe_wpt) && qc_smem(c, probe_wpt) + 512 <= (size_t)smem_max;
     // the 2-frame QC kernel is an explicit LDPC_PACK_F16X2 choice: AUTO keeps the level kernels

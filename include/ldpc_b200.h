@@ -56,6 +56,10 @@ extern "C" {
 #define LDPC_LEARNED_MAX_ITERS 32
 
 /* frame packing of the on-chip decoder state */
+/* LDPC_PACK_AUTO: the QC register kernel when the code is QC and one fits (info path 1);
+ * else LDPC_PACK_F16X2 (2 frames per CTA, path 2) for MS / OMS / NMS / xMS without early
+ * stop; else LDPC_PACK_SIMD4; LDPC_PACK_FRAME when no 4-frame state fits.  Every packing
+ * gives the same decisions. */
 #define LDPC_PACK_AUTO (-1)
 #define LDPC_PACK_SIMD4 0 /* 4 frames per 32-bit word, saturating byte lanes      */
 /* 2 frames per 32-bit word, integer-valued fp16 lanes.  On a QC code (ldpc_code_create_qc)
