@@ -1016,6 +1016,11 @@ struct ldpc_batch {
     std::vector<uintptr_t> key;     // what the captured graph was made for
     std::vector<uintptr_t> staged;  // what the staged records describe
     cudaEvent_t done = nullptr;  // the last launch (h_codes may be rewritten after it)
+    // per-code strategy: the codes' launches run side by side, forked from and joined back to
+    // the caller's stream (inside a graph capture too), so one code's early-stop tail overlaps
+    // the others' work
+    std::vector<cudaStream_t> side;  // one per code after the first
+    std::vector<cudaEvent_t> fork;   // [0]: the fork point, [i]: code i's end
 };
 
 static void batch_free(ldpc_batch* b)
@@ -1028,6 +1033,8 @@ static void batch_free(ldpc_batch* b)
     cudaFree(b->d_lut);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->done) cudaEventDestroy(b->done);
+    for (auto x : b->side) cudaStreamDestroy(x);
+    for (auto x : b->fork) cudaEventDestroy(x);
     delete b;
 }
 
@@ -1139,6 +1146,16 @@ extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_codes, batch_code_bytes() * n_codes);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    for (int i = 0; i < n_codes && e == cudaSuccess; i++) {
+        cudaEvent_t ev = nullptr;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) b->fork.push_back(ev);
+        if (e == cudaSuccess && i > 0) {
+            cudaStream_t sx = nullptr;
+            e = cudaStreamCreateWithFlags(&sx, cudaStreamNonBlocking);
+            if (e == cudaSuccess) b->side.push_back(sx);
+        }
+    }
     if (e != cudaSuccess) {
         batch_free(b);
         return fail(LDPC_ERR_CUDA, "ldpc_batch_create: %s", cudaGetErrorString(e));
@@ -1256,8 +1273,12 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
     void* args[] = {(void*)&codes, (void*)&n, (void*)&counter, (void*)&total, (void*)&J};
     auto enqueue = [&]() -> cudaError_t {
         if (b->per_code) {
-            for (int i = 0; i < n; i++) {
+            cudaError_t e = cudaEventRecord(b->fork[0], st);
+            for (int i = 0; i < n && e == cudaSuccess; i++) {
                 if (n_words[i] == 0) continue;
+                cudaStream_t si = i == 0 ? st : b->side[i - 1];
+                if (i > 0) e = cudaStreamWaitEvent(si, b->fork[0], 0);
+                if (e != cudaSuccess) break;
                 Job Jc = J;
                 Jc.llr = d_llr[i];
                 Jc.out = d_out[i];
@@ -1266,11 +1287,12 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
                 Jc.total_words = (long long)n_words[i];
                 Plan P = b->plans[i]->plan;
                 void* a[] = {(void*)&P, (void*)&Jc};
-                cudaError_t e = cudaLaunchKernel(b->pc_kfn[i], dim3((unsigned)n_words[i]), dim3(b->pc_threads[i]), a,
-                                                 b->pc_smem[i], st);
-                if (e != cudaSuccess) return e;
+                e = cudaLaunchKernel(b->pc_kfn[i], dim3((unsigned)n_words[i]), dim3(b->pc_threads[i]), a,
+                                     b->pc_smem[i], si);
+                if (e == cudaSuccess && i > 0) e = cudaEventRecord(b->fork[i], si);
+                if (e == cudaSuccess && i > 0) e = cudaStreamWaitEvent(st, b->fork[i], 0);
             }
-            return cudaSuccess;
+            return e;
         }
         cudaError_t e = cudaMemcpyAsync(b->d_codes, b->h_codes, batch_code_bytes() * n, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st);
