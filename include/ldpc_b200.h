@@ -297,7 +297,8 @@ int ldpc_batch_autotune(ldpc_batch* batch, const int8_t* const* d_llr, void* con
 
 /* Sets the strategy by hand: per_code = 0: the persistent kernel with this pack,
  * CTA width (32..256) and resident CTAs per SM (0 = as many as fit); per_code = 1:
- * one launch of each code's own kernel with this pack. */
+ * one launch of each code's own kernel with this pack, the launches forked onto the
+ * batch's own streams from `stream` and joined back to it (they run side by side). */
 int ldpc_batch_configure(ldpc_batch* batch, int per_code, int pack, int threads, int ctas_per_sm);
 
 /* LDPC_LEARNED constants of the batch (all codes), as ldpc_decoder_set_learned. */
