@@ -31,6 +31,27 @@ def test_header_symbols_exported():
     assert set(names) == set(_lib.SIGNATURES), "python binding out of sync with the header"
 
 
+def test_header_constants_match_python():
+    """Every status code, kind, packing, flag and output format the header defines has
+    the same value in the Python binding."""
+    txt = open(HEADER).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define\s+(LDPC_[A-Z0-9_]+)\s+\(?(-?\d+)\)?", txt)}
+    expect = {"LDPC_OK": _lib.LDPC_OK, "LDPC_OUT_BYTES": _lib.OUT_BYTES, "LDPC_OUT_PACKED": _lib.OUT_PACKED,
+              "LDPC_FLAG_EARLY_STOP": _lib.FLAG_EARLY_STOP,
+              "LDPC_FLAG_EARLY_STOP_FRAMES": _lib.FLAG_EARLY_STOP_FRAMES,
+              "LDPC_BATCH_GRAPH": _lib.BATCH_GRAPH,
+              "LDPC_EARLY_STOP_DEFAULT_SLACK": _lib.EARLY_STOP_DEFAULT_SLACK,
+              "LDPC_TRAIN_QUANTIZED": _lib.TRAIN_QUANTIZED, "LDPC_TRAIN_FRAME_LOSS": _lib.TRAIN_FRAME_LOSS}
+    expect.update({v: k for k, v in _lib.ERRORS.items()})
+    expect.update({"LDPC_" + k: v for k, v in _lib.KINDS.items() if k != "FMS"})
+    expect.update({"LDPC_PACK_" + k: v for k, v in _lib.PACKS.items()})
+    for name, value in expect.items():
+        assert defs.get(name) == value, (name, defs.get(name), value)
+    # the flags are distinct bits
+    flags = [defs["LDPC_FLAG_EARLY_STOP"], defs["LDPC_FLAG_EARLY_STOP_FRAMES"], defs["LDPC_BATCH_GRAPH"]]
+    assert all(f & (f - 1) == 0 for f in flags) and len(set(flags)) == 3
+
+
 def test_version_and_error_string():
     assert _lib.lib().ldpc_version() >= 1
     assert isinstance(_lib.last_error(), str)
