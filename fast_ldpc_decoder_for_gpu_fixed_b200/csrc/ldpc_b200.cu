@@ -317,10 +317,10 @@ const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
 }
 
-// shared memory of the QC kernel: the APP of 4 frames, 8 bytes per variable
+// shared memory of the QC kernel: the APP, 4 bytes per variable per pair of frames
+// (wpt = 2: 4 frames, 8 bytes per variable)
 static size_t qc_smem(const ldpc_code* c, int wpt) { return (size_t)c->n * 4 * wpt; }
 
-// QC register-message kernel, when the code is QC and a matching instantiation exists
 // The QC register-message kernel for the code, or null: 4 frames per CTA (*wpt = 2)
 // when an instantiation matches the code's shape, else 2 frames per CTA (*wpt = 1)
 // with the smallest instantiated row degree that holds it.  Fills q for that layout.
