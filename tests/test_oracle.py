@@ -119,3 +119,28 @@ def test_layered_order_matters():
     app = out["app"].reshape(3, 1, 4)[:, 0, 0].tolist()
     # row0: t=(10,-2): msgs (-2, 10) -> app (8, 8); row1 over (v1=8, v2=20): msgs (20->min 20, 8) -> (28, 28)
     assert app == [8, 28, 28]
+
+
+@pytest.mark.parametrize("kind", ["OMS", "NMS"])
+def test_early_stop_groups_agree_on_copied_frames(kind):
+    """The early-stop groupings (per frame, per frame pair, per 4-frame word) agree when a
+    group's frames are copies of one frame and the slack scales with the group: the group's
+    odd-row count is then the frame's times the group size and its syndrome is the
+    frame's, so every frame stops at the same iteration in all three modes."""
+    code = load_table("576x288")
+    frames = 48
+    base = np.concatenate([llr_gen.llr("awgn", frames * code.n // 3, 31 + i, sigma=llr_gen.sigma_for(e, 0.5))
+                           for i, e in enumerate((1.5, 2.5, 4.0))]).reshape(frames, code.n)
+    for slack in (0, 5, 40):
+        per_frame = oracle.decode(code, kind, base.reshape(-1), 25, early_stop=True, early_slack=slack,
+                                  per_frame=True)
+        words = np.repeat(base, 4, axis=0)                     # word g = 4 copies of frame g
+        per_word = oracle.decode(code, kind, words.reshape(-1), 25, early_stop=True, early_slack=4 * slack)
+        assert np.array_equal(per_word["iters"], per_frame["iters"])
+        assert np.array_equal(per_word["hard"][::4], per_frame["hard"])
+        pairs = np.repeat(base, 2, axis=0)                     # pair p = 2 copies of frame p
+        per_pair = oracle.decode(code, kind, pairs.reshape(-1), 25, early_stop=True, early_slack=2 * slack,
+                                 pairs=True)
+        assert np.array_equal(per_pair["iters"], np.maximum(per_frame["iters"][0::2], per_frame["iters"][1::2]))
+        assert np.array_equal(per_pair["hard"][::2], per_frame["hard"])
+    assert len(set(per_frame["iters"].tolist())) > 3
