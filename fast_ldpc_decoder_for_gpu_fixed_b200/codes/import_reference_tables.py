@@ -75,4 +75,6 @@ def main(matrix_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/matrix")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python import_reference_tables.py <reference src/matrix directory>")
+    main(sys.argv[1])

@@ -7,13 +7,22 @@
 # oracle/_ref/src_<code>/ made of symbolic links into the reference plus a
 # generated matrix/code.h; no reference file is copied or edited.
 #
-# usage: oracle/build_ref.sh [code ...]     (default: the codes the tests use)
+# usage: oracle/build_ref.sh [--if-present] [code ...]
+#   (default codes: those of tests/golden/make_golden.py; the reference's src directory
+#   is $REF_SRC, by default where this machine keeps the reference tree; --if-present
+#   exits 0 quietly when it is absent, as on machines that only run the built files)
 set -euo pipefail
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then IF_PRESENT=1; shift; fi
 REF=${REF_SRC:-/root/reference/src}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 NVCC=${NVCC:-nvcc}
-[ -d "$REF" ] || { echo "reference sources not found at $REF" >&2; exit 1; }
+if [ ! -d "$REF" ]; then
+    [ $IF_PRESENT = 1 ] && exit 0
+    echo "reference sources not found at $REF (set REF_SRC)" >&2
+    exit 1
+fi
 mkdir -p "$OUT"
 
 dir_of() {
@@ -28,21 +37,36 @@ dir_of() {
 }
 
 CODES=("$@")
-[ ${#CODES[@]} -gt 0 ] || CODES=(4000)
+[ ${#CODES[@]} -gt 0 ] || CODES=(4000 576 1944 2304 816)
 
 for CODE in "${CODES[@]}"; do
     D=$(dir_of "$CODE")
     S=$OUT/src_$CODE
     mkdir -p "$S/matrix"
+    # Real directories holding one symbolic link per file (cp -rs), never a link to a
+    # whole directory: the kernels include "../../matrix/constantes_gpu.h", and through
+    # a directory link that path resolves inside the reference tree, whose own
+    # matrix/code.h (CODE 4000) would then select the table instead of this tree's.
     for d in decoder_ms decoder_oms decoder_nms decoder_2nms decoder_oms_v2 transpose; do
-        ln -sfn "$REF/$d" "$S/$d"
+        rm -rf "$S/$d"
+        cp -rs "$REF/$d" "$S/$d"
     done
     ln -sf "$REF/matrix/constantes_gpu.h" "$S/matrix/constantes_gpu.h"
     ln -sf "$REF/matrix/constantes_decoder.cpp" "$S/matrix/constantes_decoder.cpp"
     ln -sfn "$REF/matrix/$D" "$S/matrix/$D"
     echo "#define CODE $CODE" > "$S/matrix/code.h"
+    # every unit must see this tree's table: the kernels' array bounds carry _N
+    WANT=${D%%x*}
+    for u in decoder_ms/cuda/CUDA_MS_SIMD.cu decoder_oms/cuda/CUDA_OMS_SIMD.cu decoder_nms/cuda/CUDA_NMS_SIMD.cu \
+             decoder_2nms/cuda/CUDA_2NMS_SIMD.cu decoder_oms_v2/cuda/CUDA_OMS_SIMD_v2.cu; do
+        GOT=$($NVCC -E -w -I"$S" "$S/$u" 2>/dev/null | grep -o 'var_nodes\[[0-9]*\]' | head -1 | tr -dc 0-9)
+        if [ "$GOT" != "$WANT" ]; then
+            echo "$u sees _N=$GOT, expected $WANT for $D: the shadow tree leaks another table" >&2
+            exit 1
+        fi
+    done
     LIB=$OUT/libref_$CODE.so
-    if [ -f "$LIB" ] && [ "$LIB" -nt "$HERE/ref_harness.cu" ]; then
+    if [ -f "$LIB" ] && [ "$LIB" -nt "$HERE/ref_harness.cu" ] && [ "$LIB" -nt "$0" ]; then
         echo "up to date: $LIB"
         continue
     fi

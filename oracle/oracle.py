@@ -45,6 +45,8 @@ def lib():
         L.oracle_decode_batch.argtypes = [i, i, P, P, P, i, i, i, i, P, P, i]
         L.oracle_decode_batch.restype = i
         L.oracle_batch_supported.restype = i
+        L.oracle_batch_isa.restype = i
+        L.oracle_batch_force_avx2.argtypes = [i]
         L.oracle_byte_op.argtypes = [i, i, i]
         L.oracle_byte_op.restype = i
         L.oracle_interleave.argtypes = [i, i, P, P]
@@ -108,8 +110,31 @@ def batch_supported():
     return bool(lib().oracle_batch_supported())
 
 
+def batch_isa():
+    """The vector ISA decode_batch uses on this CPU: "avx512bw", "avx2" or None."""
+    return {2: "avx512bw", 1: "avx2"}.get(lib().oracle_batch_isa())
+
+
+def force_avx2(on):
+    """Makes decode_batch use its AVX2 path even where AVX-512BW exists (tests)."""
+    lib().oracle_batch_force_avx2(int(bool(on)))
+
+
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def decode_batch(code, kind, llr, iters, interleaved=None, nthreads=None):
-    """AVX2 lock-step decoder (same results as decode(); 32-frame groups)."""
+    """Lock-step vector decoder (same results as decode()): 64-frame groups with
+    AVX-512BW, 32-frame groups with AVX2; frames must be a multiple of 32."""
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
         interleaved = (k == KINDS["XMS"])

@@ -9,7 +9,7 @@ in the reference's device layouts.  It also runs the CPU oracle on the same
 inputs and records whether it agreed (informational; the tests re-check).
 
     python tests/golden/make_golden.py [--out tests/golden/reference_decoder.json]
-    python tests/golden/make_golden.py --time gpurun_out/ref_kernel_times.json
+    python tests/golden/make_golden.py --time ref_kernel_times.json
 """
 import argparse
 import ctypes
@@ -31,12 +31,13 @@ from oracle import oracle  # noqa: E402
 from fast_ldpc_decoder_for_gpu_fixed_b200.codes import load_table  # noqa: E402
 
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
-# Only the reference's default table (src/matrix/code.h: CODE 4000).  Its build for the
-# two-degree 576x288 table stopped with cudaErrorInvalidAddressSpace (717) inside the
-# reference decoder kernel on a B200, on inputs checked in bounds, so the reference's
-# kernels are not run on the other tables; those are covered by the CPU oracle, which
-# these 4000x2000 cases pin.
-CODES = {4000: "4000x2000"}
+# The reference's default table (src/matrix/code.h: CODE 4000, one degree group of 6),
+# the three tables with two degree groups (576x288: 7 and 6, 1944x972: 8 and 7,
+# 2304x1152: 7 and 6), whose second group runs the separate DEG_2 row loops, the OMS
+# first-iteration no-clip (decoder_oms/cuda/CUDA_OMS_SIMD.cu:115-116) and xMS's
+# LDPC_Sched_Stage_1_MS_SIMD_Two_CN_Degs, and 816x408 (one group of degree 10).
+# Each library is built by oracle/build_ref.sh for its own table.
+CODES = {4000: "4000x2000", 576: "576x288", 1944: "1944x972", 2304: "2304x1152", 816: "816x408"}
 KINDS = ["MS", "OMS", "NMS", "2NMS", "XMS"]
 
 
@@ -70,9 +71,12 @@ def xms_supported(ref):
 
 
 def cases():
+    """The default table's 24 cases (unchanged seeds), then those of the other tables."""
     out = []
     seed = 1000
     for cid, name in CODES.items():
+        if cid != 4000:
+            continue
         code = load_table(name)
         rate = code.n_info / code.n
         inputs = [
@@ -101,6 +105,33 @@ def cases():
         out.append({"code": name, "lib": cid, "kind": "2NMS", "iters": 30, "W": 32,
                     "input": {"type": "awgn", "ebn0": 3.5, "sigma": llr_gen.sigma_for(3.5, rate),
                               "seed": seed, "tile": True}})
+    seed = 5000
+    for cid, name in CODES.items():
+        if cid == 4000:
+            continue
+        code = load_table(name)
+        rate = code.n_info / code.n
+        lo = {"type": "awgn", "ebn0": 1.0, "sigma": llr_gen.sigma_for(1.0, rate)}
+        hi = {"type": "awgn", "ebn0": 2.5, "sigma": llr_gen.sigma_for(2.5, rate)}
+        plan = []
+        for kind in ("MS", "OMS", "NMS", "XMS"):
+            for inp in (lo, hi, {"type": "uniform"}):
+                plan.append((kind, 20, inp, False))
+        for kind in ("MS", "OMS"):
+            plan.append((kind, 20, {"type": "extreme"}, False))
+        # OMS after 1, 2 and 3 iterations: the first iteration's second-group rows keep
+        # magnitudes above 31, which uniform and extreme inputs reach
+        for iters in (1, 2, 3):
+            plan.append(("OMS", iters, {"type": "uniform"}, False))
+        plan.append(("OMS", 1, {"type": "extreme"}, False))
+        plan.append(("XMS", 2, {"type": "uniform"}, False))
+        for inp in (lo, hi):
+            plan.append(("2NMS", 20, inp, True))
+        for kind, iters, inp, tile in plan:
+            seed += 1
+            extra = {"tile": True} if tile else {}
+            out.append({"code": name, "lib": cid, "kind": kind, "iters": iters, "W": 32,
+                        "input": dict(inp, seed=seed, **extra)})
     return out
 
 
@@ -117,13 +148,14 @@ def main():
     ap.add_argument("--limit", type=int, default=0, help="stop after this many cases (0 = all)")
     ap.add_argument("--codes", default="", help="comma-separated subset of codes")
     args = ap.parse_args()
-    refs = {cid: RefLib(cid) for cid in CODES}
+    wanted = [name for name in CODES.values() if not args.codes or name in args.codes.split(",")]
+    refs = {cid: RefLib(cid) for cid, name in CODES.items() if name in wanted}
     if args.time:
         return time_kernels(refs, args.time)
     results = []
     mism = 0
     t_start = time.time()
-    todo = [c for c in cases() if not args.codes or c["code"] in args.codes.split(",")]
+    todo = [c for c in cases() if c["code"] in wanted]
     if args.limit:
         todo = todo[:args.limit]
     for case in todo:

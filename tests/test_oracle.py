@@ -10,16 +10,28 @@ from oracle import oracle
 from fast_ldpc_decoder_for_gpu_fixed_b200 import Code, load_table
 
 
+@pytest.mark.parametrize("isa", ["best", "avx2"])
 @pytest.mark.parametrize("name", ["4000x2000", "576x288", "1944x972", "2048x384"])
 @pytest.mark.parametrize("kind", ["MS", "OMS", "NMS", "XMS"])
-def test_batch_equals_scalar(name, kind):
+def test_batch_equals_scalar(name, kind, isa):
+    """Both vector paths (AVX-512BW 64-frame groups where the CPU has it, and AVX2);
+    96 frames = one 64-frame group plus a 32-frame tail on the AVX-512BW path."""
     if not oracle.batch_supported():
         pytest.skip("host without AVX2")
     code = load_table(name)
-    llr = llr_gen.llr("uniform", 64 * code.n, 3)
+    llr = llr_gen.llr("uniform", 96 * code.n, 3)
     a = oracle.decode(code, kind, llr, 7)["hard"]
-    b = oracle.decode_batch(code, kind, llr, 7)
+    oracle.force_avx2(isa == "avx2")
+    try:
+        b = oracle.decode_batch(code, kind, llr, 7)
+    finally:
+        oracle.force_avx2(False)
     assert np.array_equal(a, b)
+
+
+def test_batch_isa_reported():
+    assert oracle.batch_isa() in ("avx512bw", "avx2", None)
+    assert oracle.cpu_model() is None or isinstance(oracle.cpu_model(), str)
 
 
 def test_interleave_roundtrip():
