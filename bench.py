@@ -12,9 +12,12 @@ Default workload (the metric: learned-offset decoder vs plain OMS at equal FER):
                syndrome early stop per 4-frame word), kernel only, LLRs resident in HBM
   plain_oms  : the plain 8-bit OMS kernel (offset 1, 10 fixed iterations) on the same
                batch and GPU; vs_plain_oms = value / plain_oms.value
+  oms_early_stop : plain OMS with the same early stop; early_stop_gain = its value /
+               plain_oms, learned_gain = value / its value
   fer        : both decoders on 2^20 further frames at the same Eb/N0 (untimed)
   e2e        : the learned decoder through the reference-facing host call
-               (ldpc_decode_host: pinned host LLRs in, 0/1 bytes out, copies timed)
+               (ldpc_decode_host: pinned host LLRs in, 0/1 bytes out, copies timed);
+               e2e_packed the same through ldpc_decode_host_ex with packed bits out
 Other workloads: --workload oms (plain OMS, fixed iterations), --table NAME (a
 reference H table, all-zero codeword), --workload ira (N=64800 IRA code, one frame
 per CTA, early stop, at most 50 iterations, 2048 frames).
@@ -209,8 +212,8 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic (seeded QC codewords, AWGN)",
             "config": {"workload": workload_name(args), "l2": "host CPU run", "kind": kind},
-            "cpu_baseline": {"value": value, "unit": "Gbit/s", "cores": cores, "kind": "port",
-                             "sample": samples[-1]},
+            "cpu_baseline": dict({"value": value, "unit": "Gbit/s", "cores": cores, "kind": "port",
+                                  "sample": samples[-1]}, **_cpu_info()),
             "e2e": {"value": value, "unit": "Gbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -446,14 +449,39 @@ def main():
         del ref_bits, perr, hard
         pdec.close()
 
+    # plain OMS with the same syndrome early stop: splits vs_plain_oms into the early-stop
+    # gain (oms_early_stop / plain_oms) and the learned constants' gain (value / oms_early_stop)
+    oms_es = None
+    if learned:
+        edec = Decoder(code, "OMS", nb_frames=words, pack=args.pack, early_stop=es)
+        if args.slack is not None:
+            edec.set_early_stop(True, args.slack)
+        e_its = torch.zeros(args.frames if per_frame else words, dtype=torch.int32, device="cuda")
+
+        def estep():
+            edec.decode_device(d_llr, d_out, words, args.iters, _lib.OUT_BYTES, e_its, stream)
+
+        for _ in range(args.warmup):
+            estep()
+        torch.cuda.synchronize()
+        ems = replicas.max_over_ranks(_timed(estep, args.steps, stream, flush), device="cuda")
+        launches += args.steps
+        oms_es = {"value": world * info_bits * args.steps / (ems * 1e-3) / 1e9, "unit": "Gbit/s",
+                  "ms_per_step": ems / args.steps, "mean_iterations": float(e_its.float().mean()),
+                  "early_stop": "per_frame" if per_frame else "per_word"}
+        edec.close()
+
     # equal-FER evidence on more frames (untimed)
     fer_cmp = None
     if learned and rank == 0 and args.fer_frames > 0:
         fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=es)
         fp = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames)
+        fe = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames, early_stop=es)
         fer_cmp = {"frames": fl["frames"], "ebn0_db": args.ebn0,
                    "learned_early_stop": {"fer": fl["fer"], "frame_errors": fl["frame_errors"], "ber": fl["ber"],
                                           "mean_iters": fl["mean_iters"]},
+                   "oms_early_stop": {"fer": fe["fer"], "frame_errors": fe["frame_errors"], "ber": fe["ber"],
+                                      "mean_iters": fe["mean_iters"]},
                    "plain_oms": {"fer": fp["fer"], "frame_errors": fp["frame_errors"], "ber": fp["ber"]}}
 
     # the ratio across the config-2 Eb/N0 range (untimed by the caller: extra lines of evidence)
@@ -473,16 +501,17 @@ def main():
     hbm_bytes = args.frames * code.n * 2  # int8 LLRs in + 0/1 bytes out
     peaks = _measured_peaks()
 
-    e2e = None
+    e2e = e2e_packed = None
     if not args.no_e2e:
         e2e = _e2e(dec, llr, args, info_bits, world)
+        e2e_packed = _e2e(dec, llr, args, info_bits, world, packed=True)
 
     cpu = None
     if rank == 0 and world == 1:
         ckind = "OMS" if learned else args.kind
         v, cores, sample = cpu_baseline(code, llr, min(args.iters, 10) if args.workload == "ira" else args.iters,
                                         ckind, args.cpu_seconds, enc.k)
-        cpu = {"value": v, "unit": "Gbit/s", "cores": cores, "kind": "port", "sample": sample}
+        cpu = dict({"value": v, "unit": "Gbit/s", "cores": cores, "kind": "port", "sample": sample}, **_cpu_info())
 
     if rank == 0:
         kernel = {0: "level_scheduled", 1: "qc_register_messages", 2: "level_scheduled_2f",
@@ -506,18 +535,24 @@ def main():
                        "kernel": kernel},
             "plain_oms": plain,
             "vs_plain_oms": value / plain["value"] if plain else None,
+            "oms_early_stop": oms_es,
+            "early_stop_gain": oms_es["value"] / plain["value"] if oms_es else None,
+            "learned_gain": value / oms_es["value"] if oms_es else None,
             "fer": fer_cmp,
             "ebn0_sweep": sweep,
             "roofline": {"bound": "int", "achieved": achieved, "peak": int_peak, "unit": "Tops/s (int32 word-ops)",
-                         "frac": achieved / int_peak, "traffic": None,
+                         "frac": achieved / int_peak, "traffic": _traffic(info["path"], args),
+                         "peak_nominal": NOMINAL_INT_TOPS, "frac_nominal": achieved / NOMINAL_INT_TOPS,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
                          "ops_per_edge_update": 1.0 if one_lane else 2.0,
-                         "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, all SMs)"},
+                         "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, "
+                                        "all SMs; profiles/int_peak.md); peak_nominal: 148 SMs x 128 lanes x 1.965 GHz"},
             "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
                              "unit": "GB/s", "frac": (hbm_bytes / (ms_step * 1e-3) / 1e9) / peaks["hbm_gbs"]
                              if peaks.get("hbm_gbs") else None, "alg_bytes_per_launch": hbm_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_packed": e2e_packed,
             "gpu_launches": launches,
             "clocks": clocks,
         }
@@ -575,8 +610,8 @@ def _measured_peaks():
 
 
 def _int_peak():
-    """INT32 lane-op peak of one B200 in T ops/s: measured issue rate of independent
-    LOP3/IADD3 chains (profiles/int_peak.md) x 148 SMs x the max SM clock."""
+    """INT32 lane-op peak of one B200 in T ops/s: the best measured issue rate of
+    independent LOP3 / IADD3 chains on all SMs (ldpc_probe_int_peak; profiles/int_peak.md)."""
     from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
     import ctypes
     v = ctypes.c_double()
@@ -584,25 +619,57 @@ def _int_peak():
     return v.value / 1e12
 
 
-def _e2e(dec, llr, args, info_bits, world):
-    """Host-buffer decode through the reference-facing call, copies inside the timed region."""
+def _e2e(dec, llr, args, info_bits, world, packed=False):
+    """Host-buffer decode through the reference-facing call (ldpc_decode_host: 0/1 bytes out,
+    like the reference's decode()), or with packed=True through ldpc_decode_host_ex with
+    LDPC_OUT_PACKED (n/8 bytes per frame back); copies inside the timed region."""
     import torch
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
     n = llr.shape[1]
+    out_bytes = args.frames * ((n + 7) // 8 if packed else n)
     h_in = torch.from_numpy(llr.reshape(-1)).pin_memory()
-    h_out = torch.empty(args.frames * n, dtype=torch.uint8).pin_memory()
+    h_out = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
     a_in, a_out = h_in.numpy(), h_out.numpy()
     steps = max(3, min(args.steps, 10))
+
+    def call():
+        if packed:
+            dec.decode_host_ex(a_in, a_out, args.iters, out_format=_lib.OUT_PACKED)
+        else:
+            dec.decode_host(a_in, a_out, args.iters)
+
     for _ in range(2):
-        dec.decode_host(a_in, a_out, args.iters)
+        call()
     t = time.perf_counter()
     for _ in range(steps):
-        dec.decode_host(a_in, a_out, args.iters)
+        call()
     dt = time.perf_counter() - t
     chunks = min(8, max(1, (args.frames // 4) // 256))
     return {"value": world * info_bits * steps / dt / 1e9, "unit": "Gbit/s", "ms_per_step": dt * 1e3 / steps,
-            "h2d_bytes_per_step": int(llr.size), "d2h_bytes_per_step": int(llr.size),
+            "h2d_bytes_per_step": int(llr.size), "d2h_bytes_per_step": int(out_bytes),
+            "output": "packed bits (ldpc_decode_host_ex)" if packed else "0/1 bytes (ldpc_decode_host)",
             "host_buffers": "pinned", "gpu_launches_per_step": chunks, "steps": steps}
 
+
+# nominal INT32 rate of one B200: 148 SMs x 128 lanes x 1.965 GHz (T lane-ops/s)
+NOMINAL_INT_TOPS = 148 * 128 * 1.965e9 / 1e12
+
+# DRAM bytes (read + write) per frame of the dominant decode kernel, from one ncu capture
+# of a smaller batch of the same workload, scaled here by the frames of a launch
+# (profiles/decode_qc_learned_early_stop_qc3x6_n4096_32768f.md: 134.5 MB + 92.3 MB for
+# 32 768 frames; the kernel streams each frame's LLRs once and writes its decisions once,
+# so the traffic grows with the frames)
+TRAFFIC_PER_FRAME = {1: (134.5e6 + 92.3e6) / 32768}
+
+
+def _traffic(path, args):
+    per = TRAFFIC_PER_FRAME.get(path) if args.workload == "learned" else None
+    return None if per is None else per * args.frames
+
+
+def _cpu_info():
+    from oracle import oracle
+    return {"nproc": os.cpu_count(), "cpu_model": oracle.cpu_model(), "isa": oracle.batch_isa()}
 
 if __name__ == "__main__":
     sys.exit(main())

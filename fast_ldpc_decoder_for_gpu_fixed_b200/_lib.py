@@ -34,14 +34,15 @@ SIGNATURES = {
     "ldpc_code_destroy": (None, [_P]),
     "ldpc_decoder_create": (_I, [ctypes.POINTER(_P), _P, _I, _SZ, _I, _I]),
     "ldpc_decode_host": (_I, [_P, _P, _P, _I]),
-    "ldpc_decode_device": (_I, [_P, _P, _P, _SZ, _I, _I, _P, _P]),
+    "ldpc_decode_host_ex": (_I, [_P, _P, _P, _I, _I, _P, _P]),
+    "ldpc_decode_device": (_I, [_P, _P, _P, _SZ, _I, _I, _P, _P, _P]),
     "ldpc_decode_device_state": (_I, [_P, _P, _P, _SZ, _I, _P, _P, _P, _P]),
     "ldpc_decoder_info": (_I, [_P, _P]),
     "ldpc_decoder_set_learned": (_I, [_P, _I, _P, _P]),
     "ldpc_decoder_set_early_stop": (_I, [_P, _I, _I]),
     "ldpc_decoder_destroy": (_I, [_P]),
     "ldpc_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I, _I, _I]),
-    "ldpc_batch_decode": (_I, [_P, _P, _P, _P, _I, _I, _P, _P]),
+    "ldpc_batch_decode": (_I, [_P, _P, _P, _P, _I, _I, _P, _P, _P]),
     "ldpc_batch_autotune": (_I, [_P, _P, _P, _P, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "ldpc_batch_set_learned": (_I, [_P, _I, _P, _P]),
     "ldpc_batch_configure": (_I, [_P, _I, _I, _I, _I]),

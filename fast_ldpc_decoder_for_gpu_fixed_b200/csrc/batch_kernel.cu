@@ -18,6 +18,7 @@ struct BatchCode {
     const int8_t* llr;      // frame-major int8, 4 * words frames
     void* out;              // 0/1 bytes (or packed bits), frame-major
     int32_t* iters_out;     // [words] or null
+    uint8_t* synd_out;      // [4 * words] per-frame syndrome flags or null
     long long words;
     long long first_item;   // items of the codes before this one
     int quirk;              // OMS first-iteration quirk (row classes of this code)
@@ -47,6 +48,7 @@ __global__ void __launch_bounds__(256) decode_batch_kernel(const BatchCode* __re
         J.out = bc.out;
         J.out_packed = bc.out_packed;
         J.iters_out = bc.iters_out;
+        J.synd_out = bc.synd_out;
         J.total_words = bc.words;
         J.word0 = 0;
         J.quirk = bc.quirk;
@@ -81,10 +83,11 @@ const void* kernel_table_batch(int pack, int kind, int variant)
 size_t batch_code_bytes() { return sizeof(BatchCode); }
 
 // fills one BatchCode record on the host (the struct stays private to this file)
-void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, long long words,
-                     long long first_item, int quirk, int out_packed, int variant)
+void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, uint8_t* synd_out,
+                     long long words, long long first_item, int quirk, int out_packed, int variant)
 {
     BatchCode* b = reinterpret_cast<BatchCode*>(rec);
+    b->synd_out = synd_out;
     b->variant = variant;
     b->plan = plan;
     b->llr = llr;

@@ -56,6 +56,7 @@ struct Job {
     int early;            // 1: syndrome early stop per word (LDPC_FLAG_EARLY_STOP)
     unsigned early_slack;  // evaluate the syndrome when at most this many (row, frame) pairs were odd
     int32_t* iters_out;   // [words] or null
+    uint8_t* synd_out;    // [4 * words] per-frame syndrome flags (1: every check satisfied) or null
     int8_t* app_out;      // state dumps (reference device layouts) or null
     int8_t* msg_out;
     // fused simulation (llr == null): the channel generates the LLRs in the
@@ -373,6 +374,36 @@ __device__ __forceinline__ bool rows_unsatisfied(const typename PK::S* app, cons
     return bad;
 }
 
+// Per-byte odd-parity mask of the CTA's checks: byte k is nonzero in some thread when
+// frame k has a check of odd hard-decision parity (x > 0 is bit 1); get(v) returns the
+// 4-frame byte word (values as x) of variable v.  Rows are spread over the CTA's threads.
+template <class F>
+__device__ __forceinline__ uint32_t rows_odd_mask(const Plan& P, F get)
+{
+    uint32_t bad = 0;
+    for (int r = threadIdx.x; r < P.m; r += blockDim.x) {
+        const int d = __ldg(P.rowdeg + r);
+        uint32_t acc = 0;
+        for (int j = 0; j < d; j++) acc ^= __vcmpgts4(get(__ldg(P.cols + j * P.m + r)), 0u);
+        bad |= acc;
+    }
+    return bad;
+}
+
+// Writes the syndrome flags of frames first + k (k in kmask): 1 when no thread saw an odd
+// check of frame k in its `bad` mask (byte k, or bit k with bits set).  Every thread of the
+// CTA calls it (one barrier per frame of kmask).
+__device__ __forceinline__ void write_syndrome_flags(const Job& J, long long first, uint32_t bad, int kmask,
+                                                     bool bits = false)
+{
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (!((kmask >> k) & 1)) continue;
+        const int odd = __syncthreads_or(bits ? (bad >> k) & 1u : (bad >> (8 * k)) & 0xffu);
+        if (threadIdx.x == 0) J.synd_out[first + k] = odd ? 0 : 1;
+    }
+}
+
 // ---- one check row over all storage words of the group ----
 
 template <class PK, int KIND, int DT, bool EXACT>
@@ -432,6 +463,7 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
     __syncthreads();
 
     int executed = 0;
+    bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
     for (int it = 0; it < J.iters; it++) {
         R ov = 0;
         const bool first = (it == 0);
@@ -451,12 +483,19 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
             if (!__syncthreads_or(ov != 0)) break;
         }
         if (KIND != KIND_2NMS && J.early) {
-            if (odd_rows_within_slack(J, ov, it, s_odd) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) break;
+            if (odd_rows_within_slack(J, ov, it, s_odd) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) {
+                passed = true;
+                break;
+            }
         }
     }
 
     write_group(P, J, g, [&](int v) { return Access<PK>::get(app, P.npad, v); });
     if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
+    if (J.synd_out) {
+        const uint32_t bad = passed ? 0u : rows_odd_mask(P, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+        write_syndrome_flags(J, 4 * (g - J.word0), bad, 0xF);
+    }
     if (J.app_out) {
         uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
         for (int v = threadIdx.x; v < P.n; v += blockDim.x)
@@ -517,6 +556,9 @@ __global__ void __launch_bounds__(256) decode_levels_half_kernel(const Plan P, c
     const int kmask = 3 << (2 * h);
     write_group(P, J, g, [&](int v) { return AccessHalf::get(app, v, h); }, kmask);
     if (J.iters_out && threadIdx.x == 0 && h == 0) J.iters_out[g - J.word0] = J.iters;
+    if (J.synd_out)
+        write_syndrome_flags(J, 4 * (g - J.word0), rows_odd_mask(P, [&](int v) { return AccessHalf::get(app, v, h); }),
+                             kmask);
     if (J.app_out) {
         uint8_t* ao = reinterpret_cast<uint8_t*>(J.app_out);
         for (int v = threadIdx.x; v < P.n; v += blockDim.x) {

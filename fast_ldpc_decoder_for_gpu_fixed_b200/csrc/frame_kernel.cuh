@@ -305,6 +305,7 @@ __global__ void __maxnreg__(128) decode_frame_kernel(const Plan P, const Job J)
     fetch_row(P, nl > 1 ? 1 : 0, next2);
     int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
     int executed = 0;
+    bool passed = false;  // stopped by the syndrome early stop: every check holds
     for (int it = 0; it < J.iters; it++) {
         int odd = 0;
         if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
@@ -330,13 +331,20 @@ __global__ void __maxnreg__(128) decode_frame_kernel(const Plan P, const Job J)
         }
         executed = it + 1;
         if (ET) {
-            if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) && !__syncthreads_or(frame_rows_unsatisfied(app, P)))
+            if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) && !__syncthreads_or(frame_rows_unsatisfied(app, P))) {
+                passed = true;
                 break;
+            }
         }
     }
 
     write_frame(P, J, f, [&](int v) { return (int)app[v]; });
     if (J.iters_out && threadIdx.x == 0) J.iters_out[lf] = executed;
+    if (J.synd_out) {
+        int odd = 0;
+        if (!passed) odd = __syncthreads_or(frame_rows_unsatisfied(app, P));
+        if (threadIdx.x == 0) J.synd_out[lf] = odd ? 0 : 1;
+    }
 }
 
 }  // namespace ldpc

@@ -96,6 +96,7 @@ struct ldpc_decoder {
     int32_t* d_edge_orig = nullptr;
     int8_t* d_in = nullptr;    // staging for decode_host (reference: d_MSG_C_2_V as input staging)
     uint8_t* d_out = nullptr;  // staging for decode_host (reference: d_MSG_C_2_V as output staging)
+    void* d_aux = nullptr;     // staging of iteration counts and syndrome flags for ldpc_decode_host_ex
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
@@ -424,6 +425,7 @@ static void decoder_free(ldpc_decoder* d)
     cudaFree(d->d_edge_orig);
     cudaFree(d->d_in);
     cudaFree(d->d_out);
+    cudaFree(d->d_aux);
     cudaFree(d->d_lut);
     if (d->s_comp) cudaStreamDestroy(d->s_comp);
     if (d->s_h2d) cudaStreamDestroy(d->s_h2d);
@@ -729,7 +731,7 @@ extern "C" int ldpc_decoder_destroy(ldpc_decoder* d)
 
 static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed, long long word0, long long words,
                   long long total_words, int iters, int32_t* iters_out, int8_t* app_out, int8_t* msg_out,
-                  cudaStream_t st, const Job* sim = nullptr)
+                  cudaStream_t st, const Job* sim = nullptr, uint8_t* synd_out = nullptr)
 {
     Job J{};
     if (sim) J = *sim;
@@ -749,6 +751,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.early = d->early ? 1 : 0;
     J.early_slack = d->early_slack;
     J.iters_out = iters_out;
+    J.synd_out = synd_out;
     J.app_out = app_out;
     J.msg_out = msg_out;
     if (d->path == 4 && iters_out)  // each 2-frame CTA raises its word's count with atomicMax
@@ -777,7 +780,7 @@ static int check_decode_args(ldpc_decoder* d, const void* in, const void* out, s
 }
 
 extern "C" int ldpc_decode_device(ldpc_decoder* d, const int8_t* d_llr, void* d_out, size_t n_words, int iters,
-                                  int out_format, int32_t* d_iters_out, void* stream)
+                                  int out_format, int32_t* d_iters_out, uint8_t* d_syndrome_ok, void* stream)
 {
     int rc = check_decode_args(d, d_llr, d_out, n_words, iters);
     if (rc) return rc;
@@ -785,7 +788,7 @@ extern "C" int ldpc_decode_device(ldpc_decoder* d, const int8_t* d_llr, void* d_
         return fail(LDPC_ERR_ARG, "decode: unknown out_format %d", out_format);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_out, out_format == LDPC_OUT_PACKED, 0, (long long)n_words, (long long)n_words, iters,
-                  d_iters_out, nullptr, nullptr, (cudaStream_t)stream);
+                  d_iters_out, nullptr, nullptr, (cudaStream_t)stream, nullptr, d_syndrome_ok);
 }
 
 extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, uint8_t* d_hard, size_t n_words,
@@ -828,17 +831,28 @@ extern "C" int ldpc_simulate(ldpc_decoder* d, size_t n_words, int iters, float s
                   (cudaStream_t)stream, &J);
 }
 
-extern "C" int ldpc_decode_host(ldpc_decoder* d, const int8_t* llr, uint8_t* hard, int iters)
+// Host-buffer decode of all nb_words words: the H2D copy of chunk i+1 and the D2H copy of
+// chunk i-1 overlap the decoding of chunk i (three streams).  out_format selects 0/1 bytes
+// (the reference's) or packed bits; iters_out / synd_out (host, nullable) receive the
+// iteration counts (per word, or per frame on paths 3 and 5) and the syndrome flags.
+static int decode_host_impl(ldpc_decoder* d, const int8_t* llr, void* out, int iters, int out_format,
+                            int32_t* iters_out, uint8_t* synd_out)
 {
-    if (!d) return fail(LDPC_ERR_ARG, "decode: null decoder");
-    int rc = check_decode_args(d, llr, hard, d->nb_words, iters);
+    int rc = check_decode_args(d, llr, out, d->nb_words, iters);
     if (rc) return rc;
+    if (out_format != LDPC_OUT_BYTES && out_format != LDPC_OUT_PACKED)
+        return fail(LDPC_ERR_ARG, "decode: unknown out_format %d", out_format);
     CUDA_TRY(cudaSetDevice(d->device));
-    const size_t W = d->nb_words, fb = 4 * (size_t)d->n;  // bytes per word-group of frames
+    const size_t W = d->nb_words, fb = 4 * (size_t)d->n;  // LLR bytes per word-group of frames
+    const size_t ob = out_format == LDPC_OUT_PACKED ? 4 * (size_t)((d->n + 7) / 8) : fb;  // output bytes per word
+    const size_t ipw = (d->path == 3 || d->path == 5) ? 4 : 1;  // iteration counts per word
     if (!d->d_in) {
         CUDA_TRY(cudaMalloc(&d->d_in, W * fb));
         CUDA_TRY(cudaMalloc(&d->d_out, W * fb));
     }
+    if ((iters_out || synd_out) && !d->d_aux) CUDA_TRY(cudaMalloc(&d->d_aux, W * 4 * (sizeof(int32_t) + 1)));
+    int32_t* d_its = iters_out ? reinterpret_cast<int32_t*>(d->d_aux) : nullptr;
+    uint8_t* d_syn = synd_out ? reinterpret_cast<uint8_t*>(d->d_aux) + W * 4 * sizeof(int32_t) : nullptr;
     // chunks of words: copy-in of chunk i+1 and copy-out of chunk i-1 overlap decoding of chunk i
     size_t chunks = (d->kind == LDPC_XMS) ? 1 : std::min<size_t>(8, std::max<size_t>(1, W / 256));
     size_t per = (W + chunks - 1) / chunks;
@@ -859,18 +873,38 @@ extern "C" int ldpc_decode_host(ldpc_decoder* d, const int8_t* llr, uint8_t* har
         CUDA_TRY(cudaEventRecord(a, d->s_h2d));
         CUDA_TRY(cudaStreamWaitEvent(d->s_comp, a, 0));
         const int8_t* src = (d->kind == LDPC_XMS) ? d->d_in : d->d_in + c0 * fb;
-        rc = launch(d, src, d->d_out + c0 * fb, 0, (long long)c0, (long long)words, (long long)W, iters, nullptr,
-                    nullptr, nullptr, d->s_comp);
+        rc = launch(d, src, d->d_out + c0 * ob, out_format == LDPC_OUT_PACKED, (long long)c0, (long long)words,
+                    (long long)W, iters, d_its ? d_its + c0 * ipw : nullptr, nullptr, nullptr, d->s_comp, nullptr,
+                    d_syn ? d_syn + 4 * c0 : nullptr);
         if (rc) return rc;
         CUDA_TRY(cudaEventRecord(b, d->s_comp));
         CUDA_TRY(cudaStreamWaitEvent(d->s_d2h, b, 0));
-        CUDA_TRY(cudaMemcpyAsync(hard + c0 * fb, d->d_out + c0 * fb, words * fb, cudaMemcpyDeviceToHost, d->s_d2h));
+        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(out) + c0 * ob, d->d_out + c0 * ob, words * ob,
+                                 cudaMemcpyDeviceToHost, d->s_d2h));
+        if (d_its)
+            CUDA_TRY(cudaMemcpyAsync(iters_out + c0 * ipw, d_its + c0 * ipw, words * ipw * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, d->s_d2h));
+        if (d_syn)
+            CUDA_TRY(cudaMemcpyAsync(synd_out + 4 * c0, d_syn + 4 * c0, words * 4, cudaMemcpyDeviceToHost, d->s_d2h));
     }
     cudaError_t e = cudaStreamSynchronize(d->s_d2h);
     for (auto ev : ev_in) cudaEventDestroy(ev);
     for (auto ev : ev_dec) cudaEventDestroy(ev);
     if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "decode_host: %s", cudaGetErrorString(e));
     return LDPC_OK;
+}
+
+extern "C" int ldpc_decode_host(ldpc_decoder* d, const int8_t* llr, uint8_t* hard, int iters)
+{
+    if (!d) return fail(LDPC_ERR_ARG, "decode: null decoder");
+    return decode_host_impl(d, llr, hard, iters, LDPC_OUT_BYTES, nullptr, nullptr);
+}
+
+extern "C" int ldpc_decode_host_ex(ldpc_decoder* d, const int8_t* llr, void* out, int iters, int out_format,
+                                   int32_t* iters_out, uint8_t* syndrome_ok)
+{
+    if (!d) return fail(LDPC_ERR_ARG, "decode: null decoder");
+    return decode_host_impl(d, llr, out, iters, out_format, iters_out, syndrome_ok);
 }
 
 // ------------------------------------------------------------------------
@@ -973,22 +1007,14 @@ extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
 }
 
 // ------------------------------------------------------------------------
-// Decoding without any allocation
-// ------------------------------------------------------------------------
-//
-// Some callers may not allocate device memory once they are running: real-time
-// receive chains and plugin hosts that reserve all GPU memory at start-up, where
-// cudaMalloc can stall for milliseconds, cudaFree synchronises the whole device,
-// and a framework-owned memory pool may refuse the request outright.  For them,
-// ------------------------------------------------------------------------
 // batches of several codes: one persistent kernel (batch_kernel.cu)
 // ------------------------------------------------------------------------
 
 namespace ldpc {
 const void* kernel_table_batch(int pack, int kind, int variant);
 size_t batch_code_bytes();
-void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, long long words,
-                     long long first_item, int quirk, int out_packed, int variant);
+void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, uint8_t* synd_out,
+                     long long words, long long first_item, int quirk, int out_packed, int variant);
 }  // namespace ldpc
 
 struct ldpc_batch {
@@ -1219,7 +1245,8 @@ extern "C" int ldpc_batch_set_early_stop(ldpc_batch* b, int enabled, int slack)
 }
 
 extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
-                                 int iters, int out_format, int32_t* const* d_iters_out, void* stream)
+                                 int iters, int out_format, int32_t* const* d_iters_out,
+                                 uint8_t* const* d_syndrome_ok, void* stream)
 {
     if (!b || !d_llr || !d_out || !n_words) return fail(LDPC_ERR_ARG, "ldpc_batch_decode: null pointer");
     if (iters < 1) return fail(LDPC_ERR_ARG, "ldpc_batch_decode: iterations must be >= 1 (got %d)", iters);
@@ -1240,6 +1267,7 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
         recs.push_back((uintptr_t)d_out[i]);
         recs.push_back((uintptr_t)n_words[i]);
         recs.push_back((uintptr_t)(d_iters_out ? d_iters_out[i] : nullptr));
+        recs.push_back((uintptr_t)(d_syndrome_ok ? d_syndrome_ok[i] : nullptr));
     }
     if (total == 0) return LDPC_OK;
     std::vector<uintptr_t> key = recs;
@@ -1256,7 +1284,8 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
         long long first = 0;
         for (int i = 0; i < n; i++) {
             batch_code_fill(static_cast<char*>(b->h_codes) + i * batch_code_bytes(), b->plans[i]->plan, d_llr[i],
-                            d_out[i], d_iters_out ? d_iters_out[i] : nullptr, (long long)n_words[i], first,
+                            d_out[i], d_iters_out ? d_iters_out[i] : nullptr,
+                            d_syndrome_ok ? d_syndrome_ok[i] : nullptr, (long long)n_words[i], first,
                             b->kind == LDPC_OMS, out_format == LDPC_OUT_PACKED, b->cls[i]);
             first += (long long)n_words[i];
         }
@@ -1284,6 +1313,7 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
                 Jc.out = d_out[i];
                 Jc.out_packed = out_format == LDPC_OUT_PACKED;
                 Jc.iters_out = d_iters_out ? d_iters_out[i] : nullptr;
+                Jc.synd_out = d_syndrome_ok ? d_syndrome_ok[i] : nullptr;
                 Jc.total_words = (long long)n_words[i];
                 Plan P = b->plans[i]->plan;
                 void* a[] = {(void*)&P, (void*)&Jc};
@@ -1351,12 +1381,12 @@ extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, vo
                     if (half && ctas == b->ctas_per_sm) continue;
                     if (batch_configure(b, p, t, ctas)) continue;
                 }
-                int rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, stream);
+                int rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, nullptr, stream);
                 if (rc) continue;
                 float ms = 0.f;
                 cudaEventRecord(e0, st);
                 for (int r = 0; r < 3 && !rc; r++)
-                    rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, stream);
+                    rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, nullptr, stream);
                 cudaEventRecord(e1, st);
                 if (rc || cudaEventSynchronize(e1) != cudaSuccess) continue;
                 cudaEventElapsedTime(&ms, e0, e1);
@@ -1412,19 +1442,50 @@ extern "C" int ldpc_batch_destroy(ldpc_batch* b)
     return LDPC_OK;
 }
 
+// ------------------------------------------------------------------------
+// Decoding without any allocation
+// ------------------------------------------------------------------------
+//
+// Some callers may not allocate device memory once they are running: real-time
+// receive chains and plugin hosts that reserve all GPU memory at start-up, where
+// cudaMalloc can stall for milliseconds, cudaFree synchronises the whole device,
+// and a framework-owned memory pool may refuse the request outright.  For them,
 // ldpc_decode_noalloc decodes with the level-scheduled kernel and no allocation:
 // the per-code tables that ldpc_decoder_create puts in its own device buffers
-// (column table, row degrees, row groups, level list) go instead into the
-// fixed array below, which every GPU that loads this library holds until exit.
+// (column table, row degrees, row groups, level list) go instead into the fixed
+// array below, which every GPU that loads this library holds until exit.
+//
+// The tables reach that array as kernel parameters (chunks of kNoallocChunk bytes
+// copied by noalloc_upload_kernel), not by a copy from host memory: a launch takes
+// its parameters by value when it is issued, so nothing refers to a host buffer after
+// the call returns, and the host never waits for earlier work in the stream.
 
 #define LDPC_NOALLOC_SCRATCH_BYTES (256 * 1024)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[LDPC_NOALLOC_SCRATCH_BYTES];
 
-// host image of the tables, filled per call, copied into the device array
+// 30 KiB per launch: kernel parameters may hold up to 32764 bytes (CUDA 12.1 and later)
+static const unsigned kNoallocChunk = 30 * 1024;
+
+struct NoallocChunk {
+    unsigned offset;  // byte offset in g_noalloc_scratch (a multiple of 4)
+    unsigned words;   // 32-bit words in data
+    uint32_t data[kNoallocChunk / 4];
+};
+
+__global__ void noalloc_upload_kernel(const __grid_constant__ NoallocChunk c)
+{
+    uint32_t* dst = reinterpret_cast<uint32_t*>(g_noalloc_scratch + c.offset);
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < c.words; i += gridDim.x * blockDim.x)
+        dst[i] = c.data[i];
+}
+
+// host image of the tables and the parameter block, filled per call under the mutex
 static unsigned char g_noalloc_host[LDPC_NOALLOC_SCRATCH_BYTES];
+static NoallocChunk g_noalloc_chunk;
 static std::mutex g_noalloc_mutex;
 static const int kNoallocMaxDevices = 64;
+// device address of g_noalloc_scratch, looked up once per device by the first call there
 static void* g_noalloc_dev_ptr[kNoallocMaxDevices];
 
 extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const int8_t* d_llr, uint8_t* d_hard,
@@ -1458,7 +1519,8 @@ extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const
     if (!kfn) return fail(LDPC_ERR_UNSUPPORTED, "ldpc_decode_noalloc: no kernel for this pack/kind");
 
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    // first call on this device: the device address of the static array
+    // set-up, once per device with that device current: the device address of the array
+    // (in host code the array's name is only a host-side stand-in)
     if (!g_noalloc_dev_ptr[dev]) {
         void* p = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -1470,7 +1532,8 @@ extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const
     uint8_t* hdeg = g_noalloc_host + off_deg;
     uint8_t* hcls = g_noalloc_host + off_cls;
     int2* hlev = reinterpret_cast<int2*>(g_noalloc_host + off_lev);
-    memset(g_noalloc_host, 0, bytes);
+    const size_t padded = (bytes + 3) / 4 * 4;
+    memset(g_noalloc_host, 0, padded);
     for (int rp = 0; rp < m; rp++) {
         const int r = c->order[rp], b = c->row_ptr[r], dg = c->row_ptr[r + 1] - b;
         hdeg[rp] = (uint8_t)dg;
@@ -1479,8 +1542,15 @@ extern "C" int ldpc_decode_noalloc(const ldpc_code* c, int kind, int pack, const
     }
     for (int l = 0; l < nlev; l++) hlev[l] = c->levels[l];
     cudaStream_t st = (cudaStream_t)stream;
-    // pageable source: the call returns once the host image has been consumed
-    CUDA_TRY(cudaMemcpyAsync(base, g_noalloc_host, bytes, cudaMemcpyHostToDevice, st));
+    for (size_t off = 0; off < padded; off += kNoallocChunk) {
+        const size_t len = std::min<size_t>(kNoallocChunk, padded - off);
+        g_noalloc_chunk.offset = (unsigned)off;
+        g_noalloc_chunk.words = (unsigned)(len / 4);
+        memcpy(g_noalloc_chunk.data, g_noalloc_host + off, len);
+        void* ua[] = {(void*)&g_noalloc_chunk};
+        const unsigned blocks = (unsigned)std::min<size_t>(32, (len / 4 + 255) / 256);
+        CUDA_TRY(cudaLaunchKernel((const void*)noalloc_upload_kernel, dim3(blocks), dim3(256), ua, 0, st));
+    }
 
     Plan P{};
     P.n = c->n;

@@ -22,6 +22,7 @@ namespace ldpc {
 
 constexpr int QC_MAX_LAYERS = 16;
 constexpr int QC_MAX_DEG = 24;
+constexpr int QC_LUT_ITS = 32;  // LDPC_LEARNED iteration rows (LDPC_LEARNED_MAX_ITERS)
 
 struct QCParams {
     int z;                   // circulant size = threads per CTA
@@ -80,6 +81,37 @@ __device__ __noinline__ bool qc_rows_unsatisfied(const QCParams& Q, const char* 
     return bad;
 }
 
+// bit i set when the CTA's frame i (lanes of the pair-words: WPT = 2: frames 0..3 of the
+// word; WPT = 1: frames 2h, 2h + 1 in bits 0, 1) has a row of odd hard-decision parity
+// among rows k of layers [L0, L1)
+template <int DT, bool EXACT, int L0, int L1, bool POW2, int WPT>
+__device__ __noinline__ unsigned qc_rows_unsat_mask(const QCParams& Q, const char* appb, int k)
+{
+    uint32_t bad0 = 0, bad1 = 0;
+    const int kb = 4 * WPT * k;
+#pragma unroll
+    for (int l = L0; l < L1; l++) {
+        const int d = EXACT ? DT : Q.deg[l];
+        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                const int off = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb);
+                if (WPT == 2) {
+                    const uint2 v = *reinterpret_cast<const uint2*>(appb + off);
+                    acc0 ^= qc_zero_bits(v.x);
+                    acc1 ^= qc_zero_bits(v.y);
+                } else {
+                    acc0 ^= qc_zero_bits(*reinterpret_cast<const uint32_t*>(appb + off));
+                }
+            }
+        }
+        bad0 |= acc0;
+        if (WPT == 2) bad1 |= acc1;
+    }
+    return ((bad0 >> 15) & 1u) | ((bad0 >> 30) & 2u) | ((bad1 >> 13) & 4u) | ((bad1 >> 28) & 8u);
+}
+
 // ET: the syndrome early stop compiled in (J.early is then always set); without
 // it the extrinsic-parity count is dead code for every kind but 2NMS
 template <int KIND, int DT, bool EXACT, int L, bool POW2, bool ET, int WPT>
@@ -89,12 +121,17 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     uint2* app = reinterpret_cast<uint2*>(smem_raw);     // WPT = 2: [n] (pair-word 0, pair-word 1)
     uint32_t* app1 = reinterpret_cast<uint32_t*>(smem_raw);  // WPT = 1: [n] pair-word of frames 2h, 2h+1
     char* appb = reinterpret_cast<char*>(smem_raw);
-    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + (size_t)Q.n * 4 * WPT);  // KIND_LEARNED
     const long long g = J.word0 + (WPT == 2 ? blockIdx.x : blockIdx.x >> 1);
     const int h = WPT == 2 ? 0 : (blockIdx.x & 1);
     const int k = threadIdx.x;
     __shared__ unsigned s_odd[2];
+    // KIND_LEARNED: the (k, k) and (b, b) words of every iteration and row group, loaded
+    // once (the head of each [iteration][group] table, see ldpc_decoder_set_learned), so
+    // that no iteration waits on a global load and a barrier for its constants
+    __shared__ uint2 s_kb[KIND == KIND_LEARNED ? QC_LUT_ITS : 1][2];
     if (k < 2) s_odd[k] = 0;
+    if (KIND == KIND_LEARNED && k < 2 * J.lut_its)
+        s_kb[k >> 1][k & 1] = *reinterpret_cast<const uint2*>(J.lut + (k >> 1) * 256 + (k & 1) * 128);
 
     Plan P;  // only n is used by the shared prologue / epilogue helpers
     P.n = Q.n;
@@ -115,9 +152,10 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
             for (int j = 0; j < DT; j++) msg[w][l][j] = 0;
 
     int executed = 0;
+    bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
     for (int it = 0; it < J.iters; it++) {
         uint32_t ov = 0;
-        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
+        const int lt = KIND == KIND_LEARNED ? min(it, J.lut_its - 1) : 0;  // constants of this iteration
 #pragma unroll
         for (int l = 0; l < L; l++) {
             const int d = EXACT ? DT : Q.deg[l];
@@ -142,8 +180,12 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                     }
                 }
             }
-            uint32_t lk, lb;  // LEARNED constants of this layer's class (registers only within the layer)
-            h2::learned_kb<KIND>(slut + 128 * Q.cls[l], lk, lb);
+            uint32_t lk = 0, lb = 0;  // LEARNED constants of this layer's class (registers only within the layer)
+            if (KIND == KIND_LEARNED) {
+                const uint2 kb = s_kb[lt][Q.cls[l]];
+                lk = kb.x;
+                lb = kb.y;
+            }
             h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov, lk, lb);
             if (WPT == 2) h2::row<KIND, DT, EXACT>(b1, msg[WPT - 1][l], d, noclip, ov, lk, lb);
 #pragma unroll
@@ -173,7 +215,10 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                 bool done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, 0, LS, POW2, WPT>(Q, appb, k));
                 if (LS < L && done)
                     done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, LS, L, POW2, WPT>(Q, appb, k));
-                if (done) break;
+                if (done) {
+                    passed = true;
+                    break;
+                }
             }
         }
     }
@@ -183,10 +228,18 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
         // (the host zeroes d_iters_out before the launch)
         write_group(P, J, g, [&](int v) { return AccessHalf::get(app1, v, h); }, 3 << (2 * h));
         if (J.iters_out && threadIdx.x == 0) atomicMax(J.iters_out + (g - J.word0), executed);
+        if (J.synd_out) {
+            const unsigned bad = passed ? 0u : qc_rows_unsat_mask<DT, EXACT, 0, L, POW2, 1>(Q, appb, k);
+            write_syndrome_flags(J, 4 * (g - J.word0) + 2 * h, bad, 3, true);
+        }
         return;
     }
     write_group(P, J, g, [&](int v) { uint2 a = app[v]; return Access<PackF16x2>::unbias(a.x, a.y); });
     if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
+    if (J.synd_out) {
+        const unsigned bad = passed ? 0u : qc_rows_unsat_mask<DT, EXACT, 0, L, POW2, 2>(Q, appb, k);
+        write_syndrome_flags(J, 4 * (g - J.word0), bad, 0xF, true);
+    }
     if (J.app_out) {
         uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
         for (int v = threadIdx.x; v < Q.n; v += blockDim.x) {
@@ -233,33 +286,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
 // early-stop rule (odd rows within the slack, then the syndrome) applied to that
 // frame only.
 
-constexpr int QC_LUT_ITS = 32;  // LDPC_LEARNED iteration rows (LDPC_LEARNED_MAX_ITERS)
 constexpr int QC_STAGE = 4;     // staged frames per CTA (a refill takes at most 4)
-
-// bit i set when lane i's frame has a row of odd hard-decision parity among rows k
-// of layers [L0, L1)
-template <int DT, bool EXACT, int L0, int L1, bool POW2>
-__device__ __noinline__ unsigned qc_rows_unsat_lanes(const QCParams& Q, const char* appb, int k)
-{
-    uint32_t bad0 = 0, bad1 = 0;
-    const int kb = 8 * k;
-#pragma unroll
-    for (int l = L0; l < L1; l++) {
-        const int d = EXACT ? DT : Q.deg[l];
-        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
-#pragma unroll
-        for (int j = 0; j < DT; j++) {
-            if (EXACT || j < d) {
-                const uint2 v = *reinterpret_cast<const uint2*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb));
-                acc0 ^= qc_zero_bits(v.x);
-                acc1 ^= qc_zero_bits(v.y);
-            }
-        }
-        bad0 |= acc0;
-        bad1 |= acc1;
-    }
-    return ((bad0 >> 15) & 1u) | ((bad0 >> 30) & 2u) | ((bad1 >> 13) & 4u) | ((bad1 >> 28) & 8u);
-}
 
 // CTA-wide OR of a lane mask through the shared slot *s (zero on entry); every thread calls it
 __device__ __forceinline__ unsigned cta_or_lanes(unsigned m, unsigned* s)
@@ -494,18 +521,29 @@ __global__ void __launch_bounds__(256, 2) decode_qc_refill_kernel(const __grid_c
         if (cand) {
             // staged like the per-word kernel: the first layers reject most non-codewords
             constexpr int LS = L > 2 ? 2 : L;
-            pass = cand & ~cta_or_lanes(qc_rows_unsat_lanes<DT, EXACT, 0, LS, POW2>(Q, appb, k) & cand, &s_bad[par][0]);
+            pass = cand & ~cta_or_lanes(qc_rows_unsat_mask<DT, EXACT, 0, LS, POW2, 2>(Q, appb, k) & cand, &s_bad[par][0]);
             if (LS < L && pass)
-                pass &= ~cta_or_lanes(qc_rows_unsat_lanes<DT, EXACT, LS, L, POW2>(Q, appb, k) & pass, &s_bad[par][1]);
+                pass &= ~cta_or_lanes(qc_rows_unsat_mask<DT, EXACT, LS, L, POW2, 2>(Q, appb, k) & pass, &s_bad[par][1]);
         }
         const unsigned done = pass | limit;
         if (done) {
+            // syndrome flags: lanes that passed the check satisfy every row; lanes stopped by
+            // the iteration limit alone are checked here (uniform: limit and pass are)
+            unsigned unsat = 0;
+            const unsigned chk = J.synd_out ? limit & ~pass : 0u;
+            if (chk) {
+                const unsigned lm = qc_rows_unsat_mask<DT, EXACT, 0, L, POW2, 2>(Q, appb, k) & chk;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    if (((chk >> i) & 1u) && __syncthreads_or((lm >> i) & 1u)) unsat |= 1u << i;
+            }
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 if (!((done >> i) & 1u)) continue;
                 const long long f = s_frame[i];
                 qc_store_lane(J, apph, Q.n, f, i);
                 if (k == 0 && J.iters_out) J.iters_out[f] = (int32_t)((itp >> (8 * i)) & 0xffu);
+                if (k == 0 && J.synd_out) J.synd_out[f] = ((unsat >> i) & 1u) ? 0 : 1;
             }
             if (async16) asm volatile("cp.async.wait_all;" ::: "memory");
             __syncthreads();  // staged frames landed; decisions and s_frame read before they are replaced

@@ -124,12 +124,27 @@ class Decoder:
         _lib.check(_lib.lib().ldpc_decode_host(self.handle, _ptr(llr), _ptr(hard), int(iters)))
         return hard
 
-    def decode_device(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None):
+    def decode_host_ex(self, llr, out, iters, out_format=_lib.OUT_BYTES, iters_out=None, syndrome_ok=None):
+        """Host-buffer decode of all 4*nb_frames codewords with packed output and the
+        per-word iteration counts / per-frame syndrome flags (ldpc_decode_host_ex)."""
+        n_bytes = 4 * self.nb_frames * self.code.n
+        o_bytes = 4 * self.nb_frames * ((self.code.n + 7) // 8 if out_format == _lib.OUT_PACKED else self.code.n)
+        if llr.nbytes < n_bytes or out.nbytes < o_bytes:
+            raise ValueError("buffers must hold %d and %d bytes" % (n_bytes, o_bytes))
+        if syndrome_ok is not None and syndrome_ok.nbytes < 4 * self.nb_frames:
+            raise ValueError("syndrome_ok must hold %d bytes" % (4 * self.nb_frames))
+        _lib.check(_lib.lib().ldpc_decode_host_ex(self.handle, _ptr(llr), _ptr(out), int(iters), int(out_format),
+                                                  _ptr(iters_out), _ptr(syndrome_ok)))
+        return out
+
+    def decode_device(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None,
+                      d_syndrome=None):
         """Asynchronous device-buffer decode of 4*n_words codewords on ``stream`` (a raw
-        cudaStream_t value, a torch stream or None for the legacy default stream)."""
+        cudaStream_t value, a torch stream or None for the legacy default stream);
+        ``d_syndrome`` (4*n_words bytes) receives the per-frame syndrome flags."""
         st = getattr(stream, "cuda_stream", stream)
         _lib.check(_lib.lib().ldpc_decode_device(self.handle, _ptr(d_llr), _ptr(d_out), int(n_words), int(iters),
-                                                 int(out_format), _ptr(d_iters), st))
+                                                 int(out_format), _ptr(d_iters), _ptr(d_syndrome), st))
 
     def decode_device_state(self, d_llr, d_hard, n_words, iters, d_iters=None, d_app=None, d_msg=None,
                             stream=None):
@@ -200,10 +215,13 @@ class Batch:
         its = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_iters]) if d_iters is not None else None
         return llr, out, words, its
 
-    def decode(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None):
+    def decode(self, d_llr, d_out, n_words, iters, out_format=_lib.OUT_BYTES, d_iters=None, stream=None,
+               d_syndrome=None):
         st = getattr(stream, "cuda_stream", stream)
         llr, out, words, its = self._arrays(d_llr, d_out, n_words, d_iters)
-        _lib.check(_lib.lib().ldpc_batch_decode(self.handle, llr, out, words, int(iters), int(out_format), its, st))
+        syn = (ctypes.c_void_p * len(d_llr))(*[_ptr(x) for x in d_syndrome]) if d_syndrome is not None else None
+        _lib.check(_lib.lib().ldpc_batch_decode(self.handle, llr, out, words, int(iters), int(out_format), its, syn,
+                                                st))
 
     def autotune(self, d_llr, d_out, n_words, iters, d_iters=None, stream=None):
         """Picks the fastest packing / CTA width / residency on these inputs; returns ms per decode."""

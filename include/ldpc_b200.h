@@ -163,12 +163,27 @@ int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* code, int kind, siz
  * may be pageable or pinned; copies are pipelined with the decoding. */
 int ldpc_decode_host(ldpc_decoder* dec, const int8_t* llr, uint8_t* hard, int iters);
 
+/* Like ldpc_decode_host, with the outputs the device call offers (no reference
+ * counterpart beyond decode()): out_format = LDPC_OUT_PACKED returns ceil(n/8) bytes
+ * per frame instead of n (an eighth of the copy back to the host); iters_out (host,
+ * nullable) receives what d_iters_out of ldpc_decode_device would, for all nb_frames
+ * words; syndrome_ok (host, nullable) the 4*nb_frames per-frame syndrome flags. */
+int ldpc_decode_host_ex(ldpc_decoder* dec, const int8_t* llr, void* out, int iters, int out_format,
+                        int32_t* iters_out, uint8_t* syndrome_ok);
+
 /* Asynchronous decode between device buffers on `stream` (a cudaStream_t,
  * 0 = legacy default stream).  n_words <= nb_frames words (4*n_words
  * codewords) starting at llr; out_format = LDPC_OUT_*.  iters_out (nullable,
- * device, n_words int32) receives the iterations executed per word. */
+ * device, n_words int32) receives the iterations executed per word.
+ * d_syndrome_ok (nullable, device, 4*n_words bytes) receives per frame 1 when
+ * its hard decisions (x > 0 is bit 1) satisfy every check, else 0: the test the
+ * reference's error analyser makes against the transmitted word
+ * (src/ber_analyzer/CErrorAnalyzer.cpp:142-158), made without it.  Frames that
+ * stopped early by the syndrome have passed it already; the others get one
+ * syndrome pass in the kernel's epilogue. */
 int ldpc_decode_device(ldpc_decoder* dec, const int8_t* d_llr, void* d_out, size_t n_words,
-                       int iters, int out_format, int32_t* d_iters_out, void* stream);
+                       int iters, int out_format, int32_t* d_iters_out, uint8_t* d_syndrome_ok,
+                       void* stream);
 
 /* Like ldpc_decode_device, plus the final decoder state in the reference's
  * device layouts (nullable): d_app = device_V, n*n_words 32-bit words
@@ -190,18 +205,29 @@ int ldpc_simulate(ldpc_decoder* dec, size_t n_words, int iters, float sigma, uin
                   uint64_t offset, const uint8_t* d_codewords, size_t n_codewords, int n_vars,
                   int64_t* d_counts, uint8_t* d_hard, void* stream);
 
-/* Decode with no allocation at all, for callers that may not call cudaMalloc
- * once running (real-time receive chains, plugin hosts whose memory pool owns
- * the GPU: an allocation can stall, cudaFree synchronises the device, a pool
- * may refuse).  No counterpart in the reference.  Same arguments and results
- * as ldpc_decode_device with LDPC_OUT_BYTES for a decoder of `kind` and `pack`
- * on `code` (level-scheduled kernel), but nothing is allocated: the code's
- * device tables go into a static 256 KiB array inside the library that every
- * GPU loading it keeps until exit.  Codes whose tables exceed it return
- * LDPC_ERR_UNSUPPORTED.  The first call on a device looks up that array's
- * device address, so make it before any stream capture.  Every call rewrites
- * the array: calls that overlap on the GPU (different streams, no ordering)
- * race; issue them on one stream or synchronise between them. */
+/* Decode with no allocation at all.  No counterpart in the reference.  For callers
+ * that may not call cudaMalloc once running: real-time receive chains, which cannot
+ * afford the stall of an allocation or the device-wide synchronisation of cudaFree,
+ * and plugin hosts whose memory pool owns the GPU and may refuse a request.  The
+ * caller passes `code`, the decoder `kind` and `pack` (LDPC_PACK_SIMD4 / F16X2 / I8;
+ * AUTO means SIMD4) and its own device buffers: d_llr (frame-major int8, 4*n_words
+ * frames; LDPC_XMS: word-interleaved) and d_hard (frame-major 0/1 bytes).  The hard
+ * decisions equal those of ldpc_decode_device (LDPC_OUT_BYTES) for a decoder of the
+ * same kind on the same code, since every packing decides identically; this entry
+ * point always runs the 4-frame level-scheduled kernel of `pack`, which needs
+ * 4*(n rounded up to 16 + max row degree * checks) bytes of shared memory (twice that
+ * for LDPC_PACK_F16X2) and refuses larger codes with LDPC_ERR_UNSUPPORTED.  No early
+ * stop, iteration counts or state dumps.
+ * Instead of decoder-owned buffers the code's tables go into one static 256 KiB
+ * device array inside the library, which every GPU that loads the library holds until
+ * exit; codes whose tables exceed it return LDPC_ERR_UNSUPPORTED.  The tables travel
+ * as kernel parameters, so the call neither reads host memory later nor waits for
+ * earlier work in `stream`.  The first call on a device looks up the array's device
+ * address (once per device, kept for the life of the process): make that first call
+ * before any stream capture, and do not reset the device (cudaDeviceReset) between
+ * calls.  Every call rewrites the array, so calls that overlap on the GPU (different
+ * streams with no ordering between them) race: issue them on one stream or
+ * synchronise between them. */
 int ldpc_decode_noalloc(const ldpc_code* code, int kind, int pack, const int8_t* d_llr,
                         uint8_t* d_hard, size_t n_words, int iters, void* stream);
 
@@ -281,10 +307,12 @@ int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes, int n_cod
 
 /* Decodes n_words[c] 4-frame words of every code c: d_llr[c] frame-major int8
  * LLRs, d_out[c] hard decisions (LDPC_OUT_BYTES or LDPC_OUT_PACKED), optional
- * d_iters_out[c] (iterations per word) or d_iters_out null.  Asynchronous on
- * `stream`. */
+ * d_iters_out[c] (iterations per word) or d_iters_out null, optional
+ * d_syndrome_ok[c] (per-frame syndrome flags, as ldpc_decode_device) or
+ * d_syndrome_ok null.  Asynchronous on `stream`. */
 int ldpc_batch_decode(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
-                      int iters, int out_format, int32_t* const* d_iters_out, void* stream);
+                      int iters, int out_format, int32_t* const* d_iters_out,
+                      uint8_t* const* d_syndrome_ok, void* stream);
 
 /* Times, on these inputs (outputs are overwritten), the two strategies: the
  * persistent kernel for each packing (SIMD4, F16X2, I8), CTA width (64, 128,

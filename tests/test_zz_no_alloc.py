@@ -40,8 +40,13 @@ def _noalloc(native, kind, pack, d_llr, words, iters):
 
 def test_noalloc_matches_regular_entry_point_twice(cuda):
     import torch
-    cases = [("4000x2000", "OMS", "SIMD4", 37, 20), ("576x288", "2NMS", "F16X2", 21, 15)]
-    for name, kind, pack, words, iters in cases:  # two calls in a row, different codes
+    # consecutive calls with different codes, kinds and packings; the regular decoder
+    # takes other kernels for some of them (F16X2 OMS / xMS: 2 frames per CTA), which
+    # must decide identically
+    cases = [("4000x2000", "OMS", "SIMD4", 37, 20), ("576x288", "2NMS", "F16X2", 21, 15),
+             ("1944x972", "OMS", "F16X2", 9, 12), ("4000x2000", "XMS", "F16X2", 5, 10),
+             ("576x288", "MS", "I8", 13, 8), ("2304x1152", "NMS", "I8", 6, 7)]
+    for name, kind, pack, words, iters in cases:
         code = load_table(name)
         native = NativeCode(code)
         llr = llr_gen.llr("awgn", 4 * words * code.n, 17 + words, sigma=llr_gen.sigma_for(2.0, 0.5))
