@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--table", default=None,
                     help="decode a reference H table (e.g. 4000x2000) with the all-zero codeword instead of the QC workload")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    ap.add_argument("--constants", default=TRAINED, help="trained LDPC_LEARNED constants (learned workload)")
     a = ap.parse_args()
     if a.table:
         a.workload = "oms"
@@ -382,7 +383,7 @@ def main():
     words = args.frames // 4
     learned = args.workload == "learned"
     early = args.workload in ("learned", "ira")
-    constants = load_constants(TRAINED)[:2] if learned else None
+    constants = load_constants(args.constants)[:2] if learned else None
     kind = "LEARNED" if learned else args.kind
     es = ("frame" if args.per_frame else True) if early else False
     dec = Decoder(code, kind, nb_frames=words, pack=args.pack, early_stop=es)

@@ -72,6 +72,9 @@ struct Job {
     // KIND_LEARNED: magnitude tables [lut_its][2 row groups][128] (see packs.cuh)
     const uint16_t* lut;
     int lut_its;
+    // one-frame-per-CTA decoder: message scratch of fslots CTA slots (frame_kernel.cuh)
+    uint2* fmsg;
+    long long fslots;
 };
 
 // KIND_LEARNED: loads the tables of iteration `it` into shared memory (256 entries);

@@ -1,22 +1,15 @@
 // Row-layered decoder for long codes (DVB-S2 size, N = 64800): one frame per CTA,
-// everything on chip.
+// its APP in shared memory, its c->v messages in a global scratch.
 //
 // The 4-frame state of a long code does not fit in one CTA's shared memory
-// (N = 64800 needs 259 KB of APP alone for 4 frames), and per-edge c->v messages
-// would add E bytes per frame (194 KB for the rate-1/2 IRA code).  But every
-// message of a min-sum check row is a function of four row quantities: the
-// magnitude c1 sent on the minimum edge, the magnitude c2 sent on the others,
-// the index of the minimum edge and one sign bit per edge.  Stored as one
-// 32-bit word per row (7 + 7 + 4 + 14 bits: degree <= 14, magnitudes <= 127,
-// which every kind but 2NMS satisfies), a frame's whole decoder state is
-// N + 4M bytes: 194 KB for N = 64800, M = 32400, inside one SM's shared memory.
-// No message crosses HBM; the prologue reads N LLR bytes and the epilogue
-// writes the hard decisions.
-//
-// The state reproduces the reference's per-edge messages exactly: edges whose
-// |t| equals min1 receive c1 in the reference (CUDA_OMS_SIMD.cu:73-90), and
-// when two edges tie at min1, min2 = min1 and c1 = c2, so one stored index
-// suffices.
+// (N = 64800 needs 259 KB of APP alone for 4 frames).  One frame's APP as int8 is
+// N bytes (64.8 KB), so two CTAs, two frames, fit on an SM.  The frame's E
+// messages (194 K for the rate-1/2 IRA code) go to the decoder's scratch in global
+// memory, one byte per edge, 8 bytes per check row for its edges 0-7 (and 8 more for
+// edges 8-15): the thread that updates a row reads and writes its row words
+// coalesced with the other rows of the level, two levels ahead of their use, so the
+// latency hides behind the levels in between.  Per frame and iteration that is 2E
+// bytes of message traffic, the HBM-bound case of this decoder.
 //
 // Early stop (ET) is per frame: the frame stops after an iteration in which at
 // most J.early_slack of its rows had odd extrinsic parity and its hard decisions
@@ -141,13 +134,14 @@ __device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const 
     return bad;
 }
 
-// The row a thread updates in one level: its record (columns, degree, class;
-// see Plan::rowrec) and its index.  Records do not depend on the frame's
-// state, so they are loaded two levels ahead: with one CTA per SM nothing else
-// hides the L2 latency of a table too large for L1 (1 MB for M = 32400).
+// The row a thread updates in one level: its record (columns, degree, class; see
+// Plan::rowrec), its index, and its c->v messages.  Records and messages do not depend
+// on the frame's APP, so they are loaded two levels ahead: the record table (1 MB for
+// M = 32400) lives in L2 and the messages in the decoder's scratch in HBM.
 struct FrameRow {
     uint4 c0, c1;
-    int r, end;  // row, end of its level
+    uint2 m0, m1;  // messages of edges 0-7 and 8-15, one byte each (see frame_row)
+    int r, end;    // row, end of its level
     __device__ __forceinline__ int deg() const { return (c1.w >> 16) & 0xff; }
     __device__ __forceinline__ int cls() const { return c1.w >> 24; }
     __device__ __forceinline__ int col(int j) const  // j a compile-time constant after unrolling
@@ -157,6 +151,18 @@ struct FrameRow {
         const uint32_t w = k == 0 ? q.x : (k == 1 ? q.y : (k == 2 ? q.z : q.w));
         return (j & 1) ? (int)(w >> 16) : (int)(w & 0xffff);
     }
+    // the 32-bit word of the messages that holds edges 2p and 2p+1 (bytes 2(p&1), +1)
+    __device__ __forceinline__ uint32_t& mword(int p)
+    {
+        return p < 4 ? ((p >> 1) ? m0.y : m0.x) : ((p >> 1) & 1 ? m1.y : m1.x);
+    }
+};
+
+// The decoder's message scratch: one slot per resident CTA, M rows of 8 bytes for edges
+// 0-7 and, for row degrees above 8, a second array of M rows for edges 8-15.
+struct FrameMsgs {
+    uint2* lo;
+    uint2* hi;
 };
 
 __device__ __forceinline__ void load_row(const Plan& P, int r, FrameRow& x)
@@ -165,22 +171,43 @@ __device__ __forceinline__ void load_row(const Plan& P, int r, FrameRow& x)
     x.c1 = __ldg(P.rowrec + 2 * r + 1);
 }
 
-__device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow& x)
+template <int DT>
+__device__ __forceinline__ void load_msgs(const FrameMsgs& M, FrameRow& x)
+{
+    x.m0 = M.lo[x.r];
+    if (DT > 8) x.m1 = M.hi[x.r];
+}
+
+template <int DT>
+__device__ __forceinline__ void store_msgs(const FrameMsgs& M, const FrameRow& x)
+{
+    M.lo[x.r] = x.m0;
+    if (DT > 8) M.hi[x.r] = x.m1;
+}
+
+// the row of level l this thread updates first (records and, with msgs, messages)
+template <int DT>
+__device__ __forceinline__ void fetch_row(const Plan& P, const FrameMsgs& M, int l, FrameRow& x, bool msgs)
 {
     const int2 lv = __ldg(P.levels + l);
     x.r = lv.x + threadIdx.x;
     x.end = lv.x + lv.y;
     if (x.r < x.end) {
         load_row(P, x.r, x);
+        if (msgs) load_msgs<DT>(M, x);
     } else {
         x.c1.w = 0;  // degree 0: no row for this thread
     }
 }
 
-// One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134)
-// with its messages held as the packed row state st: c1 | c2 << 7 | i1 << 14 | signs << 18,
-// sign bit j set when edge j's message is positive.  D: the row's degree (fully
-// unrolled).  Returns the new state.
+// f16x2 of 1152 and -1152: a message byte y = 128 + u (u the negated message, |u| <= 127)
+// under the byte 0x64 is the fp16 1024 + y, so adding -1152 gives u, and adding 1152 to u
+// puts y back in the low byte
+constexpr uint32_t FRAME_C1152 = 0x64806480u, FRAME_CNEG1152 = 0xe480e480u;
+
+// One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134):
+// APP bytes in shared memory, this row's messages in row.m0 / row.m1 (in / out), one byte
+// per edge holding 128 - msg.  D: the row's degree (fully unrolled).
 //
 // Two edges per 32-bit word: edges 2p and 2p+1 are the fp16 halves of pair p, in the
 // biased negated form of the F16X2 packing (b = 127 - x in [0, 255], integer-valued,
@@ -188,20 +215,13 @@ __device__ __forceinline__ void fetch_row(const Plan& P, int l, FrameRow& x)
 // (min1, min2, sign parity) over its edges; the halves are merged once per row.  An
 // odd degree's last pair carries a dummy edge x = -127 with no message: |u| = 127
 // equals the initial min1 and min2 and its sign is positive, so it changes nothing.
-// All edges whose |t| equals min1 get c1 (as in the reference); ties give c1 = c2 for
-// every kind served here, so the stored index (the first such edge) is exact.
 template <int KIND, int D>
-__device__ __forceinline__ uint32_t frame_row(int8_t* app, const FrameRow& row, uint32_t st, bool first, bool noclip,
-                                              int& odd, const uint16_t* lut)
+__device__ __forceinline__ void frame_row(int8_t* app, FrameRow& row, bool first, bool noclip, int& odd,
+                                          const uint16_t* lut)
 {
     using namespace h2;
     constexpr int NP = (D + 1) / 2;
-    uint32_t bt[NP], ut[NP];
-    // old messages: magnitude oc1 on edge oi, oc2 on the others, as fp16 pairs
-    const uint32_t oc1 = st & 0x7f, oc2 = (st >> 7) & 0x7f, oi = (st >> 14) & 0xf;
-    const uint32_t h22 = add(0x64006400u | oc2 | (oc2 << 16), CNEG1024);
-    const uint32_t h12 = add(0x64006400u | oc1 | (oc2 << 16), CNEG1024);
-    const uint32_t h21 = add(0x64006400u | oc2 | (oc1 << 16), CNEG1024);
+    uint32_t bt[NP];  // the extrinsics t = 127 - bt are recomputed where needed (registers)
     uint32_t mn1 = C127, mn2 = C127;
 #pragma unroll
     for (int p = 0; p < NP; p++) {
@@ -210,16 +230,15 @@ __device__ __forceinline__ uint32_t frame_row(int8_t* app, const FrameRow& row, 
         uint32_t w = (uint32_t)(uint8_t)app[row.col(j0)];
         w |= (j1 < D ? (uint32_t)(uint8_t)app[row.col(j1)] : 0x81u) << 16;
         const uint32_t b = add((w ^ 0x007f007fu) | 0x64006400u, CNEG1024);
-        uint32_t m = 0;  // negated old messages (h2 convention: t = clamp(b - m))
+        uint32_t u = 0;  // negated old messages (h2 convention: t = clamp(b - u))
         if (!first) {
-            const uint32_t sb = st >> (18 + j0);  // bit 0: edge j0's message positive, bit 1: edge j1's
-            m = (oi == (uint32_t)j0 ? h12 : (oi == (uint32_t)j1 ? h21 : h22)) | ((sb & 1u) << 15) | ((sb & 2u) << 30);
-            if (j1 >= D) m &= 0xffffu;
+            u = add(__byte_perm(row.mword(p), 0x64646464u, (p & 1) ? 0x4342 : 0x4140), FRAME_CNEG1152);
+            if (j1 >= D) u &= 0xffffu;
         }
-        bt[p] = hmin(fma_relu(m, NEG1, b), C255);
-        ut[p] = add(bt[p], CNEG127);
-        const uint32_t mx = max_xs(ut[p], mn1);
-        mn1 = min_xs(mn1, ut[p]);
+        bt[p] = hmin(fma_relu(u, NEG1, b), C255);
+        const uint32_t ut = add(bt[p], CNEG127);
+        const uint32_t mx = max_xs(ut, mn1);
+        mn1 = min_xs(mn1, ut);
         mn2 = min_xs(mn2, mx);
     }
     // merge the halves: min1 of both, min2 = min(max of the two min1s, both min2s), parity of both
@@ -227,123 +246,127 @@ __device__ __forceinline__ uint32_t frame_row(int8_t* app, const FrameRow& row, 
     const uint32_t m1 = min_xs(mn1, s1);  // |min1| in both halves, sign: the row's parity
     const uint32_t m2 = min_xs(min_xs(mn2, s2), max_xs(mn1, s1));
     const uint32_t a1 = habs(m1), a2 = habs(m2);
-    uint32_t c1, c2, ic1, ic2;
+    uint32_t c1, c2;
     if (KIND == KIND_LEARNED) {
         // the integer tables of the I8 packing (any constants): c1 = lut[min2], c2 = lut[min1]
-        ic1 = lut[add(a2, C1024) & 0x7fu];
-        ic2 = lut[add(a1, C1024) & 0x7fu];
+        const uint32_t ic1 = lut[add(a2, C1024) & 0x7fu];
+        const uint32_t ic2 = lut[add(a1, C1024) & 0x7fu];
         c1 = add(0x64006400u | ic1 | (ic1 << 16), CNEG1024);
         c2 = add(0x64006400u | ic2 | (ic2 << 16), CNEG1024);
     } else {
         h2::mags<KIND>(a1, a2, noclip, c1, c2, 0u, 0u);
-        ic1 = add(c1, C1024) & 0x7fu;
-        ic2 = add(c2, C1024) & 0x7fu;
     }
     const uint32_t c1s = c1 | (m1 & SIGN), c2s = c2 | (m1 & SIGN);
     const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
-    uint32_t notmin = 0, sgn = 0;
 #pragma unroll
     for (int p = 0; p < NP; p++) {
         const int j0 = 2 * p, j1 = 2 * p + 1;
-        const uint32_t fl = add_sat(habs(ut[p]), na1);  // 0.0 on minimum edges, 1.0 elsewhere
-        const uint32_t mo = fma(fl, dcs, c1s) ^ (ut[p] & SIGN);
-        const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[p]), C255), C1024);  // 1024 + b: b in the low byte
-        app[row.col(j0)] = (int8_t)(bn ^ 0x7fu);
-        notmin |= ((fl >> 13) & 1u) << j0;
-        sgn |= ((mo >> 15) & 1u) << j0;  // the message -mo is positive
-        if (j1 < D) {
-            app[row.col(j1)] = (int8_t)((bn >> 16) ^ 0x7fu);
-            notmin |= ((fl >> 29) & 1u) << j1;
-            sgn |= (mo >> 31) << j1;
-        }
+        const uint32_t ut = add(bt[p], CNEG127);
+        const uint32_t fl = add_sat(habs(ut), na1);  // 0.0 on minimum edges, 1.0 elsewhere
+        const uint32_t mo = fma(fl, dcs, c1s) ^ (ut & SIGN);
+        const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[p]), C255), C1024) ^ 0x007f007fu;  // x bytes
+        app[row.col(j0)] = (int8_t)bn;
+        if (j1 < D) app[row.col(j1)] = (int8_t)(bn >> 16);
+        uint32_t& mw = row.mword(p);
+        mw = __byte_perm(mw, add(mo, FRAME_C1152), (p & 1) ? 0x6410 : 0x3264);
     }
-    const uint32_t mins = ~notmin & ((1u << D) - 1u);
-    const uint32_t i1 = mins ? (uint32_t)(__ffs(mins) - 1) : 0u;
     odd += (m1 >> 15) & 1u;
-    return ic1 | (ic2 << 7) | (i1 << 14) | (sgn << 18);
 }
 
 // Dispatches a row to the unrolled update for its degree.  Rows of a level are
 // sorted by degree, so the warps of a level mostly take one case.
 template <int KIND, int DT, bool EXACT>
-__device__ __forceinline__ uint32_t frame_row_any(int8_t* app, const FrameRow& row, uint32_t st, bool first,
-                                                  bool noclip, int& odd, const uint16_t* lut)
+__device__ __forceinline__ void frame_row_any(int8_t* app, FrameRow& row, bool first, bool noclip, int& odd,
+                                              const uint16_t* lut)
 {
-    if (EXACT) return frame_row<KIND, DT>(app, row, st, first, noclip, odd, lut);
-#define LDPC_FRAME_CASE(D) \
-    case D:                \
-        if (D <= DT) return frame_row<KIND, (D <= DT ? D : DT)>(app, row, st, first, noclip, odd, lut);
+    if (EXACT) return frame_row<KIND, DT>(app, row, first, noclip, odd, lut);
+#define LDPC_FRAME_CASE(D)                                                                        \
+    case D:                                                                                       \
+        if (D <= DT) frame_row<KIND, (D <= DT ? D : DT)>(app, row, first, noclip, odd, lut);      \
+        return;
     switch (row.deg()) {
         LDPC_FRAME_CASE(1) LDPC_FRAME_CASE(2) LDPC_FRAME_CASE(3) LDPC_FRAME_CASE(4) LDPC_FRAME_CASE(5)
         LDPC_FRAME_CASE(6) LDPC_FRAME_CASE(7) LDPC_FRAME_CASE(8) LDPC_FRAME_CASE(9) LDPC_FRAME_CASE(10)
         LDPC_FRAME_CASE(11) LDPC_FRAME_CASE(12) LDPC_FRAME_CASE(13) LDPC_FRAME_CASE(14)
     }
 #undef LDPC_FRAME_CASE
-    return st;  // not reached: degrees are 1..FRAME_MAX_DEGREE
 }
 
-// Launched with at most FRAME_MAX_THREADS (512) threads, so 128 registers a thread always
-// fit; a plain launch bound let the compiler settle at 64 and spill the degree-14 update.
+// Persistent CTAs: CTA c decodes frames c, c + G, c + 2G, ... of the launch (G = gridDim.x),
+// one at a time, with slot c of the message scratch (J.fmsg: J.fslots slots of P.m rows,
+// then as many again for edges 8-15 when DT > 8).  Shared memory: the frame's APP
+// (npad bytes) and, for KIND_LEARNED, the iteration's tables.
 template <int KIND, int DT, bool EXACT, bool ET>
-__global__ void __maxnreg__(128) decode_frame_kernel(const Plan P, const Job J)
+__global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J, long long frames)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                                  // [npad]
-    uint32_t* state = reinterpret_cast<uint32_t*>(smem_raw + P.npad);                   // [m]
-    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad + 4 * (size_t)P.m);  // KIND_LEARNED
+    int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                     // [npad]
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad);       // KIND_LEARNED
     __shared__ unsigned s_odd[2];
-    const long long lf = blockIdx.x;
-    const long long f = 4 * J.word0 + lf;
-
-    read_frame(P, J, f, [&](int v, int x) { app[v] = (int8_t)x; });
-    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
-    __syncthreads();
-
+    const FrameMsgs M = {J.fmsg + (long long)blockIdx.x * P.m, J.fmsg + (J.fslots + blockIdx.x) * (long long)P.m};
     const int nl = P.nlevels;
-    FrameRow next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
-    fetch_row(P, 0, next1);
-    fetch_row(P, nl > 1 ? 1 : 0, next2);
-    int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
-    int executed = 0;
-    bool passed = false;  // stopped by the syndrome early stop: every check holds
-    for (int it = 0; it < J.iters; it++) {
-        int odd = 0;
-        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
-        for (int l = 0; l < nl; l++) {
-            const FrameRow cur = next1;
-            next1 = next2;
-            fetch_row(P, lf2, next2);
-            lf2 = lf2 + 1 == nl ? 0 : lf2 + 1;
-            if (cur.r < cur.end) {
-                const bool noclip = J.quirk && it == 0 && cur.cls();
-                state[cur.r] = frame_row_any<KIND, DT, EXACT>(app, cur, it == 0 ? 0u : state[cur.r], it == 0, noclip,
-                                                              odd, slut + 128 * cur.cls());
-            }
-            // levels wider than the CTA: the remaining rows load their records directly
-            for (int r = cur.r + blockDim.x; r < cur.end; r += blockDim.x) {
-                FrameRow x;
-                load_row(P, r, x);
-                const bool noclip = J.quirk && it == 0 && x.cls();
-                state[r] = frame_row_any<KIND, DT, EXACT>(app, x, it == 0 ? 0u : state[r], it == 0, noclip, odd,
-                                                          slut + 128 * x.cls());
-            }
-            __syncthreads();
-        }
-        executed = it + 1;
-        if (ET) {
-            if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) && !__syncthreads_or(frame_rows_unsatisfied(app, P))) {
-                passed = true;
-                break;
-            }
-        }
-    }
+    // messages are fetched with the records two levels ahead; a row's messages are written
+    // back when its level is updated, so with fewer than 3 levels per iteration the fetch
+    // would come before that write: such codes load them when the row is updated
+    const bool pf = nl >= 3;
+    for (long long lf = blockIdx.x; lf < frames; lf += gridDim.x) {
+        const long long f = 4 * J.word0 + lf;
+        if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+        read_frame(P, J, f, [&](int v, int x) { app[v] = (int8_t)x; });
+        __syncthreads();
 
-    write_frame(P, J, f, [&](int v) { return (int)app[v]; });
-    if (J.iters_out && threadIdx.x == 0) J.iters_out[lf] = executed;
-    if (J.synd_out) {
-        int odd = 0;
-        if (!passed) odd = __syncthreads_or(frame_rows_unsatisfied(app, P));
-        if (threadIdx.x == 0) J.synd_out[lf] = odd ? 0 : 1;
+        FrameRow next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
+        fetch_row<DT>(P, M, 0, next1, pf);
+        fetch_row<DT>(P, M, nl > 1 ? 1 : 0, next2, pf);
+        int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
+        int executed = 0;
+        bool passed = false;  // stopped by the syndrome early stop: every check holds
+        for (int it = 0; it < J.iters; it++) {
+            int odd = 0;
+            const bool first = it == 0, keep = it + 1 < J.iters;  // the last iteration's messages are not needed
+            if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
+            for (int l = 0; l < nl; l++) {
+                FrameRow cur = next1;
+                next1 = next2;
+                fetch_row<DT>(P, M, lf2, next2, pf);
+                lf2 = lf2 + 1 == nl ? 0 : lf2 + 1;
+                if (cur.r < cur.end) {
+                    if (!pf && !first) load_msgs<DT>(M, cur);
+                    const bool noclip = J.quirk && first && cur.cls();
+                    frame_row_any<KIND, DT, EXACT>(app, cur, first, noclip, odd, slut + 128 * cur.cls());
+                    if (keep) store_msgs<DT>(M, cur);
+                }
+                // levels wider than the CTA: the remaining rows load their records directly
+                for (int r = cur.r + blockDim.x; r < cur.end; r += blockDim.x) {
+                    FrameRow x;
+                    x.r = r;
+                    x.end = cur.end;
+                    load_row(P, r, x);
+                    if (!first) load_msgs<DT>(M, x);
+                    const bool noclip = J.quirk && first && x.cls();
+                    frame_row_any<KIND, DT, EXACT>(app, x, first, noclip, odd, slut + 128 * x.cls());
+                    if (keep) store_msgs<DT>(M, x);
+                }
+                __syncthreads();
+            }
+            executed = it + 1;
+            if (ET) {
+                if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) &&
+                    !__syncthreads_or(frame_rows_unsatisfied(app, P))) {
+                    passed = true;
+                    break;
+                }
+            }
+        }
+
+        write_frame(P, J, f, [&](int v) { return (int)app[v]; });
+        if (J.iters_out && threadIdx.x == 0) J.iters_out[lf] = executed;
+        if (J.synd_out) {
+            int odd = 0;
+            if (!passed) odd = __syncthreads_or(frame_rows_unsatisfied(app, P));
+            if (threadIdx.x == 0) J.synd_out[lf] = odd ? 0 : 1;
+        }
+        __syncthreads();  // the APP is refilled by the next frame
     }
 }
 

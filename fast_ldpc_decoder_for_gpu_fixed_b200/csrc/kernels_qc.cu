@@ -1,7 +1,7 @@
 // Instantiations of the QC register-message decoder for the code shapes in use,
 // each with and without the syndrome early stop compiled in:
 //   4 frames per CTA (WPT = 2): the regular (3,6) rate-1/2 8x16 base (row degree 6,
-//     8 layers, Z a power of two);
+//     8 layers, Z a power of two), every kind and the offset-only learned kind;
 //   2 frames per CTA (WPT = 1): 24-column irregular bases (802.11n-like) at rates
 //     1/2, 2/3, 3/4, 5/6, i.e. 12, 8, 6, 4 layers of row degree up to 10, 14, 18, 24,
 //     any Z.  Not for 2NMS, whose early termination is per 4-frame word;
@@ -15,9 +15,10 @@ namespace ldpc {
     if (kind == KIND && dt == D && exact == EX && layers == L && pow2 == P2 && wpt == W)                \
         return et ? (const void*)decode_qc_kernel<KIND, D, EX, L, P2, true, W>                          \
                   : (const void*)decode_qc_kernel<KIND, D, EX, L, P2, false, W>;
-#define LDPC_QC_KINDS(D, EX, L, P2) \
-    LDPC_QC(KIND_MS, D, EX, L, P2, 2) LDPC_QC(KIND_OMS, D, EX, L, P2, 2) \
-    LDPC_QC(KIND_NMS, D, EX, L, P2, 2) LDPC_QC(KIND_2NMS, D, EX, L, P2, 2) LDPC_QC(KIND_LEARNED, D, EX, L, P2, 2)
+#define LDPC_QC_KINDS(D, EX, L, P2)                                                                    \
+    LDPC_QC(KIND_MS, D, EX, L, P2, 2) LDPC_QC(KIND_OMS, D, EX, L, P2, 2)                                \
+    LDPC_QC(KIND_NMS, D, EX, L, P2, 2) LDPC_QC(KIND_2NMS, D, EX, L, P2, 2) LDPC_QC(KIND_LEARNED, D, EX, L, P2, 2) \
+    LDPC_QC(KIND_LEARNED_OFS, D, EX, L, P2, 2)
 #define LDPC_QC_PAIR(D, L) \
     LDPC_QC(KIND_MS, D, false, L, false, 1) LDPC_QC(KIND_OMS, D, false, L, false, 1) \
     LDPC_QC(KIND_NMS, D, false, L, false, 1) LDPC_QC(KIND_LEARNED, D, false, L, false, 1)

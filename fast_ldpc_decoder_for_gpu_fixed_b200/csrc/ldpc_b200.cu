@@ -101,11 +101,16 @@ struct ldpc_decoder {
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
     const void* kfn_alt = nullptr;  // the same kernel with the other early-stop setting (paths 1, 3 and 4)
+    // path 1, LDPC_LEARNED: the general and the offset-only (every scale 1.0) kernels with
+    // and without the early stop; ldpc_decoder_set_learned picks from them
+    const void* kfn_lrn[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [offset-only][early stop]
     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA,
     // 3 = one frame per CTA, 4 = QC register-message, 2 frames per CTA, 5 = QC register-message with
     // per-frame early stop and lane refill (persistent CTAs)
     int path = 0;
-    int sms = 0;  // path 5: multiprocessors (grid size)
+    int sms = 0;  // paths 3 and 5: multiprocessors (grid size)
+    uint2* d_fmsg = nullptr;  // path 3: message scratch, fslots CTA slots (frame_kernel.cuh)
+    long long fslots = 0;
     int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
     uint16_t* d_lut = nullptr;  // LDPC_LEARNED magnitude tables [its][2][128]
@@ -327,7 +332,7 @@ static size_t qc_smem(const ldpc_code* c, int wpt) { return (size_t)c->n * 4 * w
 // with the smallest instantiated row degree that holds it.  Fills q for that layout.
 // refill: the per-frame early-stop kernel with lane refill (4 frames per CTA) instead.
 static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false, int* wpt_out = nullptr,
-                                 bool refill = false)
+                                 bool refill = false, bool ofs = false)
 {
     if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > (1 << 20)) return nullptr;
     int deg[QC_MAX_LAYERS], dt = 0;
@@ -344,7 +349,8 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool
         dt = std::max(dt, d);
     }
     const bool pow2 = (c->z & (c->z - 1)) == 0;
-    const int k = (kind == LDPC_XMS) ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
+    // KIND_* values equal LDPC_* values; ofs: the learned kind with every scale 1.0
+    const int k = (kind == LDPC_XMS) ? LDPC_OMS : (ofs && kind == LDPC_LEARNED ? KIND_LEARNED_OFS : kind);
     const bool e = et && kind != LDPC_2NMS;
     int wpt = 2;
     const void* f =
@@ -426,6 +432,7 @@ static void decoder_free(ldpc_decoder* d)
     cudaFree(d->d_in);
     cudaFree(d->d_out);
     cudaFree(d->d_aux);
+    cudaFree(d->d_fmsg);
     cudaFree(d->d_lut);
     if (d->s_comp) cudaStreamDestroy(d->s_comp);
     if (d->s_h2d) cudaStreamDestroy(d->s_h2d);
@@ -529,7 +536,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
                         smem, smem_max);
         frame = true;  // one frame per CTA with packed row state
     }
-    const size_t frame_smem = (size_t)npad + 4 * (size_t)c->m + lut_smem;
+    const size_t frame_smem = (size_t)npad + lut_smem;  // the APP; messages live in the decoder's scratch
     if (frame) {
         if (kind == LDPC_2NMS)
             return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: 2NMS terminates per 4-frame word; use another pack");
@@ -577,6 +584,9 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         QCParams alt;
         d->kfn = qk;
         d->kfn_alt = qc_kernel_for(c, kind, alt, !early);  // for ldpc_decoder_set_early_stop (same layout)
+        if (kind == LDPC_LEARNED && qc_wpt == 2)
+            for (int o = 0; o < 2; o++)
+                for (int e = 0; e < 2; e++) d->kfn_lrn[o][e] = qc_kernel_for(c, kind, alt, e != 0, nullptr, false, o != 0);
         d->path = qc_wpt == 2 ? 1 : 4;
         d->grid_mult = qc_wpt == 2 ? 1 : 2;
         d->pack = LDPC_PACK_F16X2;
@@ -598,7 +608,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_FRAMES: needs the QC register kernel with 4 frames per "
                                           "CTA (the regular 8x16 base, Z a power of two) or LDPC_PACK_FRAME");
     }
-    if (d->path == 5) {
+    if (d->path == 5 || d->path == 3) {
         cudaError_t ec = cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, dev);
         if (ec != cudaSuccess) {
             decoder_free(d);
@@ -607,6 +617,9 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     }
     cudaError_t e1 = ldpc_internal_raise_smem(d->kfn, d->smem);
     if (e1 == cudaSuccess && d->kfn_alt) e1 = ldpc_internal_raise_smem(d->kfn_alt, d->smem);
+    for (int o = 0; o < 2; o++)
+        for (int e = 0; e < 2; e++)
+            if (e1 == cudaSuccess && d->kfn_lrn[o][e]) e1 = ldpc_internal_raise_smem(d->kfn_lrn[o][e], d->smem);
     cudaFuncAttributes fa;
     cudaError_t e2 = cudaFuncGetAttributes(&fa, d->kfn);
     cudaError_t e3 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->ctas_per_sm, d->kfn, d->threads, d->smem);
@@ -619,6 +632,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (d->ctas_per_sm < 1) {
         decoder_free(d);
         return fail(LDPC_ERR_UNSUPPORTED, "kernel cannot be resident (smem %d B, %d threads)", d->smem, d->threads);
+    }
+    if (d->path == 3) {
+        // one message slot per resident CTA: 8 bytes per check row for edges 0-7, and as many
+        // again for edges 8-15 when a row has more than 8
+        d->fslots = (long long)d->ctas_per_sm * d->sms;
+        const size_t bytes = (size_t)d->fslots * d->m * sizeof(uint2) * (c->dmax > 8 ? 2 : 1);
+        cudaError_t ea = cudaMalloc(&d->d_fmsg, bytes);
+        if (ea != cudaSuccess) {
+            decoder_free(d);
+            return fail(ea == cudaErrorMemoryAllocation ? LDPC_ERR_NOMEM : LDPC_ERR_CUDA,
+                        "message scratch of %zu B: %s", bytes, cudaGetErrorString(ea));
+        }
     }
     cudaError_t es = cudaStreamCreateWithFlags(&d->s_comp, cudaStreamNonBlocking);
     if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&d->s_h2d, cudaStreamNonBlocking);
@@ -703,6 +728,14 @@ extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8
     if (!d->d_lut) CUDA_TRY(cudaMalloc(&d->d_lut, sizeof(uint16_t) * 256 * LDPC_LEARNED_MAX_ITERS));
     CUDA_TRY(cudaMemcpy(d->d_lut, lut.data(), lut.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
     d->lut_its = n_iters;
+    if (d->kfn_lrn[0][0]) {
+        // the QC register kernel: constants with every scale 1.0 (offsets only) take the kernel
+        // whose magnitude is min - offset, the arithmetic of OMS, without the floor step
+        bool ofs = true;
+        for (int i = 0; i < 2 * n_iters; i++) ofs = ofs && scales[i] == 128;
+        d->kfn = d->kfn_lrn[ofs][d->early];
+        d->kfn_alt = d->kfn_lrn[ofs][!d->early];
+    }
     return LDPC_OK;
 }
 
@@ -762,6 +795,16 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
         long long frames = 4 * words;
         const long long grid = std::min(words, (long long)d->ctas_per_sm * d->sms);
         void* a[] = {(void*)&d->qcp, (void*)&J, (void*)&frames};
+        CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
+        return LDPC_OK;
+    }
+    if (d->path == 3) {
+        // persistent CTAs, one message-scratch slot each
+        long long frames = 4 * words;
+        J.fmsg = d->d_fmsg;
+        J.fslots = d->fslots;
+        const long long grid = std::min(frames, d->fslots);
+        void* a[] = {(void*)&d->plan, (void*)&J, (void*)&frames};
         CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
         return LDPC_OK;
     }

@@ -37,6 +37,12 @@ namespace ldpc {
 
 enum { KIND_MS = 0, KIND_OMS = 1, KIND_NMS = 2, KIND_2NMS = 3, KIND_XMS = 4, KIND_LEARNED = 5 };
 
+// KIND_LEARNED with every scale 1.0 (a learned-offset decoder): the magnitude is
+// clamp(min - offset, 0, 31), no floor step, the arithmetic of OMS with the offset of
+// the iteration.  Used by the fp16 QC register kernel, which the host switches to it
+// when the constants allow; the (k, b) words then carry b = -offset.
+constexpr int KIND_LEARNED_OFS = 6;
+
 // KIND_LEARNED (no reference counterpart): the magnitude of a check's outgoing
 // messages is c = clamp(floor(min * scale_q7 / 128) - offset, 0, 31) with the
 // trained int8 offset and Q1.7 scale of the current iteration and row group.
@@ -210,7 +216,11 @@ template <int KIND>
 __device__ __forceinline__ void mags(uint32_t a1, uint32_t a2, bool noclip, uint32_t& c1, uint32_t& c2, uint32_t lk,
                                      uint32_t lb, uint32_t clip = C31)
 {
-    if (KIND == KIND_LEARNED) {
+    if (KIND == KIND_LEARNED_OFS) {
+        // scale 1: clamp(a - offset, 0, 31) with lb = (-offset, -offset), exact on integers
+        c1 = hmin(fma_relu(a2, ONE, lb), C31);
+        c2 = hmin(fma_relu(a1, ONE, lb), C31);
+    } else if (KIND == KIND_LEARNED) {
         // clamp(floor(a * k) - offset, 0, 31) = min(round(relu(a * k + b)), 31), b = -offset - 15/32:
         // with k on a 1/16 grid, a * k + b is exact below 64 and never within 1/32 of a tie
         // (ldpc_decoder_set_learned stores (k, k) and (b, b) at the head of the class's table)
@@ -244,23 +254,59 @@ __device__ __forceinline__ void learned_kb(const uint16_t* lut, uint32_t& lk, ui
     }
 }
 
-// LANES: ov counts odd rows per fp16 lane (bit 0 and bit 16 fields) instead of in total,
-// and clip is the per-lane OMS clip word
-template <int KIND, int DT, bool EXACT, bool LANES = false>
+// CMODE 0: ov counts odd (row, frame) pairs; 1: ov counts odd rows per fp16 lane (bit 0 and
+// bit 16 fields), and clip is the per-lane OMS clip word; 2: ov is a count_parity
+// accumulator (+1 per even row, -1 per odd row and lane, on the FMA pipe)
+template <int KIND, int DT, bool EXACT, int CMODE = 0>
 __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d, bool noclip, uint32_t& ov,
                                     uint32_t lk, uint32_t lb, uint32_t clip = C31)
 {
     uint32_t ut[DT];
     uint32_t mn1 = C127, mn2 = C127;
+    if (EXACT && DT >= 4) {
+        // Rows of a known degree: the two smallest |t| by a tournament (pairs sorted, then
+        // merged: min1 = min(m1, l), min2 = min(max(m1, l), min(m2, h))), 3.5 min/max per
+        // two edges instead of 3 per edge.  The xorsign forms carry the sign parity of
+        // the row into min1 as in the running form below.
 #pragma unroll
-    for (int j = 0; j < DT; j++) {
-        if (EXACT || j < d) {
-            uint32_t bt = hmin(fma_relu(m[j], NEG1, b[j]), C255);  // clamp(b - m, 0, 255)
+        for (int j = 0; j < DT; j++) {
+            const uint32_t bt = hmin(fma_relu(m[j], NEG1, b[j]), C255);  // clamp(b - m, 0, 255)
             b[j] = bt;
             ut[j] = add(bt, CNEG127);
-            uint32_t mx = max_xs(ut[j], mn1);
-            mn1 = min_xs(mn1, ut[j]);
+        }
+        mn1 = min_xs(ut[0], ut[1]);
+        mn2 = max_xs(ut[0], ut[1]);
+#pragma unroll
+        for (int j = 2; j + 1 < DT; j += 2) {
+            const uint32_t lo = min_xs(ut[j], ut[j + 1]), hi = max_xs(ut[j], ut[j + 1]);
+            const uint32_t m2 = min_xs(max_xs(mn1, lo), min_xs(mn2, hi));
+            mn1 = min_xs(mn1, lo);
+            mn2 = m2;
+        }
+        if (DT & 1) {
+            const uint32_t mx = max_xs(ut[DT - 1], mn1);
+            mn1 = min_xs(mn1, ut[DT - 1]);
             mn2 = min_xs(mn2, mx);
+        }
+        // The reference starts both minima at 127; |t| reaches 128 only for x = -128.  That
+        // changes a magnitude only where the magnitude is not clipped to 31 (NMS, 2NMS,
+        // LEARNED, the OMS first-iteration no-clip), so only those cap.
+        if (KIND == KIND_NMS || KIND == KIND_2NMS || KIND == KIND_LEARNED || KIND == KIND_LEARNED_OFS ||
+            (KIND == KIND_OMS && (noclip || clip != C31))) {
+            mn1 = min_xs(mn1, C127);
+            mn2 = min_xs(mn2, C127);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                uint32_t bt = hmin(fma_relu(m[j], NEG1, b[j]), C255);  // clamp(b - m, 0, 255)
+                b[j] = bt;
+                ut[j] = add(bt, CNEG127);
+                uint32_t mx = max_xs(ut[j], mn1);
+                mn1 = min_xs(mn1, ut[j]);
+                mn2 = min_xs(mn2, mx);
+            }
         }
     }
     const uint32_t a1 = habs(mn1), a2 = habs(mn2);
@@ -281,10 +327,21 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
             b[j] = hmin(fma_relu(mo, ONE, b[j]), C255);         // clamp(bt + m, 0, 255)
         }
     }
-    if (LANES)
+    if (CMODE == 1)
         ov += (mn1 & SIGN) >> 15;  // odd rows of each lane's frame
+    else if (CMODE == 2)
+        ov = add(ov, (mn1 & SIGN) | ONE);
     else
         ov += __popc(mn1 & SIGN);  // odd (row, frame) pairs
+}
+
+// The number of odd rows from a CMODE 2 accumulator of row() after `rows` rows per lane:
+// each row added +1 (even) or -1 (odd) per lane, so 2 * rows - sum is twice that number.
+__device__ __forceinline__ unsigned odd_count(uint32_t acc, int rows)
+{
+    const __half2 h = *reinterpret_cast<const __half2*>(&acc);
+    const int sum = __half2int_rn(__low2half(h)) + __half2int_rn(__high2half(h));
+    return (unsigned)((2 * rows - sum) >> 1);
 }
 }  // namespace h2
 

@@ -128,10 +128,17 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     // KIND_LEARNED: the (k, k) and (b, b) words of every iteration and row group, loaded
     // once (the head of each [iteration][group] table, see ldpc_decoder_set_learned), so
     // that no iteration waits on a global load and a barrier for its constants
-    __shared__ uint2 s_kb[KIND == KIND_LEARNED ? QC_LUT_ITS : 1][2];
+    constexpr bool LRN = KIND == KIND_LEARNED || KIND == KIND_LEARNED_OFS;
+    __shared__ uint2 s_kb[LRN ? QC_LUT_ITS : 1][2];
     if (k < 2) s_odd[k] = 0;
-    if (KIND == KIND_LEARNED && k < 2 * J.lut_its)
-        s_kb[k >> 1][k & 1] = *reinterpret_cast<const uint2*>(J.lut + (k >> 1) * 256 + (k & 1) * 128);
+    if (LRN && k < 2 * J.lut_its) {
+        uint2 kb = *reinterpret_cast<const uint2*>(J.lut + (k >> 1) * 256 + (k & 1) * 128);
+        if (KIND == KIND_LEARNED_OFS) kb.y = h2::add(kb.y, 0x37803780u);  // b + 15/32 = -offset (scale 1)
+        s_kb[k >> 1][k & 1] = kb;
+    }
+    // the odd-row count of the early stop: a +-1 accumulator on the FMA pipe (row(), CMODE 2);
+    // 2NMS keeps the exact popcount, which its own rule tests against zero
+    constexpr int CM = (ET && KIND != KIND_2NMS) ? 2 : 0;
 
     Plan P;  // only n is used by the shared prologue / epilogue helpers
     P.n = Q.n;
@@ -155,7 +162,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
     for (int it = 0; it < J.iters; it++) {
         uint32_t ov = 0;
-        const int lt = KIND == KIND_LEARNED ? min(it, J.lut_its - 1) : 0;  // constants of this iteration
+        const int lt = LRN ? min(it, J.lut_its - 1) : 0;  // constants of this iteration
 #pragma unroll
         for (int l = 0; l < L; l++) {
             const int d = EXACT ? DT : Q.deg[l];
@@ -181,13 +188,13 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                 }
             }
             uint32_t lk = 0, lb = 0;  // LEARNED constants of this layer's class (registers only within the layer)
-            if (KIND == KIND_LEARNED) {
+            if (KIND == KIND_LEARNED || KIND == KIND_LEARNED_OFS) {
                 const uint2 kb = s_kb[lt][Q.cls[l]];
                 lk = kb.x;
                 lb = kb.y;
             }
-            h2::row<KIND, DT, EXACT>(b0, msg[0][l], d, noclip, ov, lk, lb);
-            if (WPT == 2) h2::row<KIND, DT, EXACT>(b1, msg[WPT - 1][l], d, noclip, ov, lk, lb);
+            h2::row<KIND, DT, EXACT, CM>(b0, msg[0][l], d, noclip, ov, lk, lb);
+            if (WPT == 2) h2::row<KIND, DT, EXACT, CM>(b1, msg[WPT - 1][l], d, noclip, ov, lk, lb);
 #pragma unroll
             for (int j = 0; j < DT; j++) {
                 if (EXACT || j < d) {
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
         // ((b | 0x8000) - 0x57f0) has bit 15 set iff b >= 127.0, i.e. iff the
         // hard decision is 0; a row is satisfied when its count of 1s is even.
         if (KIND != KIND_2NMS && ET) {
-            if (odd_rows_within_slack(J, ov, it, s_odd)) {
+            if (odd_rows_within_slack(J, h2::odd_count(ov, L * WPT), it, s_odd)) {
                 // staged: the first layers alone reject most words that are not codewords yet
                 constexpr int LS = L > 2 ? 2 : L;
                 bool done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, 0, LS, POW2, WPT>(Q, appb, k));
@@ -486,8 +493,8 @@ __global__ void __launch_bounds__(256, 2) decode_qc_refill_kernel(const __grid_c
                 cl0 = s_clip[0];
                 cl1 = s_clip[1];
             }
-            h2::row<KIND, DT, EXACT, true>(b0, msg[0][l], d, false, ov0, lk0, lb0, cl0);
-            h2::row<KIND, DT, EXACT, true>(b1, msg[1][l], d, false, ov1, lk1, lb1, cl1);
+            h2::row<KIND, DT, EXACT, 1>(b0, msg[0][l], d, false, ov0, lk0, lb0, cl0);
+            h2::row<KIND, DT, EXACT, 1>(b1, msg[1][l], d, false, ov1, lk1, lb1, cl1);
 #pragma unroll
             for (int j = 0; j < DT; j++)
                 if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);

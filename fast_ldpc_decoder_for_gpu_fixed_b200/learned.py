@@ -64,7 +64,8 @@ class Trainer:
     """
 
     def __init__(self, code, iters=10, batch=4096, sub=512, ebn0=(1.0, 3.0), lr=0.03, seed=1,
-                 n_codewords=256, init_alpha=1.0, init_beta=1.0, weights="last", loss="bit", device="cuda"):
+                 n_codewords=256, init_alpha=1.0, init_beta=1.0, weights="last", loss="bit", device="cuda",
+                 train_scales=True):
         import torch
         if sub % n_codewords or batch % sub:
             raise ValueError("batch must be a multiple of sub, and sub a multiple of n_codewords")
@@ -92,7 +93,10 @@ class Trainer:
         self.beta = torch.full((self.T, 2), float(init_beta), dtype=torch.float32, device=dev, requires_grad=True)
         self.alpha.grad = torch.zeros_like(self.alpha)
         self.beta.grad = torch.zeros_like(self.beta)
-        self.opt = torch.optim.Adam([self.alpha, self.beta], lr=lr)
+        # train_scales=False: the scales stay at init_alpha (1.0: a learned-offset decoder, whose
+        # deployed kernel computes min - offset like OMS) and only the offsets are trained
+        self.train_scales = bool(train_scales)
+        self.opt = torch.optim.Adam([self.alpha, self.beta] if self.train_scales else [self.beta], lr=lr)
         # loss weight per iteration: "last" (the final soft output only) or "all"
         # (every iteration's soft output, which rewards early convergence)
         if isinstance(weights, str):
@@ -268,6 +272,8 @@ def main(argv=None):
     ap.add_argument("--init", default="oms", choices=("oms", "ms"))
     ap.add_argument("--qat", type=float, default=1.0, help="fraction of the steps with the quantised forward pass")
     ap.add_argument("--lr", type=float, default=0.01)
+    ap.add_argument("--offsets-only", action="store_true",
+                    help="keep every scale at 1.0 and train the offsets only (a learned-offset decoder)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--eval-ebn0", type=float, nargs="*", default=(1.75, 2.0, 2.25))
     ap.add_argument("--eval-frames", type=int, default=262144)
@@ -275,7 +281,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     code = _code_by_name(a.code)
     tr = Trainer(code, iters=a.iters, batch=a.batch, lr=a.lr, seed=a.seed, weights=a.weights, loss=a.loss,
-                 init_alpha=1.0, init_beta=1.0 if a.init == "oms" else 0.0, ebn0=tuple(a.ebn0))
+                 init_alpha=1.0, init_beta=1.0 if a.init == "oms" else 0.0, ebn0=tuple(a.ebn0),
+                 train_scales=not a.offsets_only)
     v0 = tr.validation_loss(2.0)
     t0 = time.time()
     tr.train(a.frames, qat_fraction=a.qat)
@@ -293,6 +300,7 @@ def main(argv=None):
         evals.append(row)
     meta = {"code": a.code, "iterations": a.iters, "frames": a.frames, "batch": a.batch, "ebn0_db": list(a.ebn0),
             "loss": a.loss, "weights": a.weights, "init": a.init, "qat_fraction": a.qat, "lr": a.lr, "seed": a.seed,
+            "offsets_only": bool(a.offsets_only),
             "train_seconds": round(dt, 2), "validation_loss_2db": [v0, v1],
             "evaluation": evals, "evaluation_frames": a.eval_frames}
     import json

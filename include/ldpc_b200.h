@@ -70,15 +70,16 @@ extern "C" {
  * 4g+2, 4g+3) on its own and reports per word the larger of its two pairs' counts. */
 #define LDPC_PACK_F16X2 1
 #define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
-/* 1 frame per CTA, everything in shared memory: the APP as int8 and each check
- * row's messages packed into one 32-bit word (the two magnitudes, the minimum
- * edge and the edges' signs), N + 4*M bytes per frame.  For long codes whose
- * 4-frame state exceeds shared memory (N = 64800 rate 1/2: 194 KB).  Row degree
- * <= 14.  LDPC_PACK_AUTO falls back to it when nothing else fits.  Not for
- * LDPC_2NMS (whose early termination is per 4-frame word).  With
- * LDPC_FLAG_EARLY_STOP each frame stops on its own.  On this path d_iters_out
- * always receives one count per frame (4*n_words entries), and state dumps
- * (ldpc_decode_device_state) are unsupported. */
+/* 1 frame per CTA: the frame's APP as int8 in shared memory (N bytes, two CTAs per
+ * SM at N = 64800) and its c->v messages, one byte per edge, in a message scratch
+ * the decoder allocates in device memory (8 bytes per check row and resident CTA,
+ * 16 when a row has more than 8 edges: 153 MB for N = 64800 rate 1/2 on 148 SMs).
+ * For long codes whose 4-frame state exceeds shared memory.  Row degree <= 14.
+ * LDPC_PACK_AUTO falls back to it when nothing else fits.  Not for LDPC_2NMS
+ * (whose early termination is per 4-frame word).  With LDPC_FLAG_EARLY_STOP each
+ * frame stops on its own.  On this path d_iters_out always receives one count per
+ * frame (4*n_words entries), and state dumps (ldpc_decode_device_state) are
+ * unsupported. */
 #define LDPC_PACK_FRAME 3
 
 /* output formats of ldpc_decode_device */
