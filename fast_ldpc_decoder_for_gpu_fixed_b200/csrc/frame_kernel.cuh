@@ -165,24 +165,47 @@ struct FrameMsgs {
     uint2* hi;
 };
 
+// Loads issued where they stand: the compiler may not move a volatile asm across the
+// level barriers, so a load issued two levels ahead stays two levels ahead instead of
+// being sunk next to its use to save registers.
+__device__ __forceinline__ uint4 ld_nc_v4(const uint4* p)
+{
+    uint4 v;
+    asm volatile("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p)
+                 : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint2 ld_v2(const uint2* p)
+{
+    uint2 v;
+    asm volatile("ld.global.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void load_row(const Plan& P, int r, FrameRow& x)
 {
-    x.c0 = __ldg(P.rowrec + 2 * r);
-    x.c1 = __ldg(P.rowrec + 2 * r + 1);
+    x.c0 = ld_nc_v4(P.rowrec + 2 * r);
+    x.c1 = ld_nc_v4(P.rowrec + 2 * r + 1);
 }
 
 template <int DT>
 __device__ __forceinline__ void load_msgs(const FrameMsgs& M, FrameRow& x)
 {
-    x.m0 = M.lo[x.r];
-    if (DT > 8) x.m1 = M.hi[x.r];
+    x.m0 = ld_v2(M.lo + x.r);
+    if (DT > 8) x.m1 = ld_v2(M.hi + x.r);
 }
 
 template <int DT>
 __device__ __forceinline__ void store_msgs(const FrameMsgs& M, const FrameRow& x)
 {
-    M.lo[x.r] = x.m0;
-    if (DT > 8) M.hi[x.r] = x.m1;
+    // ordered with the volatile loads of the same words (a row's words are written and
+    // read back by the same thread)
+    asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(M.lo + x.r), "r"(x.m0.x), "r"(x.m0.y) : "memory");
+    if (DT > 8)
+        asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(M.hi + x.r), "r"(x.m1.x), "r"(x.m1.y) : "memory");
 }
 
 // the row of level l this thread updates first (records and, with msgs, messages)

@@ -48,9 +48,11 @@ __device__ __forceinline__ int qc_var_off(const QCParams& Q, int idx, int kb)
     return Q.cz4[idx] + u;
 }
 
-// hard-decision parity masks of one biased pair-word: bit 15 / 31 set iff that
-// frame's decision is 0 (b >= 127.0; (b | 0x8000) - 0x57f0 has bit 15 set iff so)
-__device__ __forceinline__ uint32_t qc_zero_bits(uint32_t b) { return ((b | 0x80008000u) - 0x57f057f0u) & 0x80008000u; }
+// hard decisions of one biased pair-word as sign bits, one fp16 add for both frames on
+// the FMA pipe: the integer b is below 127 (decision 1, x > 0) exactly when b - 126.5 is
+// negative.  XORed over a row, bits 15 / 31 are the row's parity of 1s in each frame; the
+// other bits are don't-care.
+__device__ __forceinline__ uint32_t qc_one_signs(uint32_t b) { return h2::add(b, 0xd7e8d7e8u); }
 
 // true when row k of some layer in [L0, L1) has odd hard-decision parity in one of
 // the CTA's frames (see the early stop in decode_qc_kernel)
@@ -62,21 +64,21 @@ __device__ __noinline__ bool qc_rows_unsatisfied(const QCParams& Q, const char* 
 #pragma unroll
     for (int l = L0; l < L1; l++) {
         const int d = EXACT ? DT : Q.deg[l];
-        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+        uint32_t acc0 = 0, acc1 = 0;
 #pragma unroll
         for (int j = 0; j < DT; j++) {
             if (EXACT || j < d) {
                 const int off = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb);
                 if (WPT == 2) {
                     const uint2 v = *reinterpret_cast<const uint2*>(appb + off);
-                    acc0 ^= qc_zero_bits(v.x);
-                    acc1 ^= qc_zero_bits(v.y);
+                    acc0 ^= qc_one_signs(v.x);
+                    acc1 ^= qc_one_signs(v.y);
                 } else {
-                    acc0 ^= qc_zero_bits(*reinterpret_cast<const uint32_t*>(appb + off));
+                    acc0 ^= qc_one_signs(*reinterpret_cast<const uint32_t*>(appb + off));
                 }
             }
         }
-        bad |= (WPT == 2 ? (acc0 | acc1) : acc0) != 0;
+        bad |= ((WPT == 2 ? (acc0 | acc1) : acc0) & 0x80008000u) != 0;
     }
     return bad;
 }
@@ -92,23 +94,25 @@ __device__ __noinline__ unsigned qc_rows_unsat_mask(const QCParams& Q, const cha
 #pragma unroll
     for (int l = L0; l < L1; l++) {
         const int d = EXACT ? DT : Q.deg[l];
-        uint32_t acc0 = (d & 1) ? 0x80008000u : 0u, acc1 = acc0;
+        uint32_t acc0 = 0, acc1 = 0;
 #pragma unroll
         for (int j = 0; j < DT; j++) {
             if (EXACT || j < d) {
                 const int off = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb);
                 if (WPT == 2) {
                     const uint2 v = *reinterpret_cast<const uint2*>(appb + off);
-                    acc0 ^= qc_zero_bits(v.x);
-                    acc1 ^= qc_zero_bits(v.y);
+                    acc0 ^= qc_one_signs(v.x);
+                    acc1 ^= qc_one_signs(v.y);
                 } else {
-                    acc0 ^= qc_zero_bits(*reinterpret_cast<const uint32_t*>(appb + off));
+                    acc0 ^= qc_one_signs(*reinterpret_cast<const uint32_t*>(appb + off));
                 }
             }
         }
         bad0 |= acc0;
         if (WPT == 2) bad1 |= acc1;
     }
+    bad0 &= 0x80008000u;
+    bad1 &= 0x80008000u;
     return ((bad0 >> 15) & 1u) | ((bad0 >> 30) & 2u) | ((bad1 >> 13) & 4u) | ((bad1 >> 28) & 8u);
 }
 
@@ -213,8 +217,8 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
         }
         // syndrome early stop (odd_rows_within_slack): thread k checks row k of
         // every layer.  For a biased APP b (x = 127 - b, an fp16 in [0, 255]),
-        // ((b | 0x8000) - 0x57f0) has bit 15 set iff b >= 127.0, i.e. iff the
-        // hard decision is 0; a row is satisfied when its count of 1s is even.
+        // b - 126.5 is negative iff the hard decision is 1 (qc_one_signs); a row is
+        // satisfied when its count of 1s is even.
         if (KIND != KIND_2NMS && ET) {
             if (odd_rows_within_slack(J, h2::odd_count(ov, L * WPT), it, s_odd)) {
                 // staged: the first layers alone reject most words that are not codewords yet
