@@ -17,6 +17,7 @@ PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2, "FRAME": 3}
 OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
 FLAG_EARLY_STOP_FRAMES = 4
+FLAG_FLOODING = 8
 BATCH_GRAPH = 2
 EARLY_STOP_DEFAULT_SLACK = 128
 TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2
@@ -48,6 +49,8 @@ SIGNATURES = {
     "ldpc_batch_configure": (_I, [_P, _I, _I, _I, _I]),
     "ldpc_batch_set_early_stop": (_I, [_P, _I, _I]),
     "ldpc_batch_info": (_I, [_P, _P]),
+    "ldpc_batch_code_info": (_I, [_P, _I, _P]),
+    "ldpc_batch_set_code_kernel": (_I, [_P, _I, _I]),
     "ldpc_batch_destroy": (_I, [_P]),
     "ldpc_train_step": (_I, [_P, _P, _P, _P, _SZ, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ldpc_train_stash_bytes": (_SZ, [_P, _SZ, _I]),

@@ -42,6 +42,10 @@ struct Plan {
     // [m][2] 32-byte row records (dmax <= 14): u16 columns 0..13, slot 14 unused,
     // slot 15 = degree | class << 8; null when dmax > 14
     const uint4* rowrec;
+    // the flooding schedule: variable v's edges as message indices j * m + r' (schedule
+    // order), vedge[vptr[v] .. vptr[v + 1])
+    const int32_t* vptr;
+    const int32_t* vedge;
 };
 
 struct Job {
@@ -508,6 +512,122 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
         uint32_t* mo = reinterpret_cast<uint32_t*>(J.msg_out);
         const int mstride = P.dmax * P.m;
         for (int i = threadIdx.x; i < P.dmax * P.m; i += blockDim.x) {
+            const int j = i / P.m, r = i - j * P.m;
+            if (j < P.rowdeg[r])
+                mo[(long long)P.edge_orig[i] * J.total_words + g] = Access<PK>::get_msg(msg, mstride, i);
+        }
+    }
+}
+
+// ---- the flooding schedule (LDPC_FLAG_FLOODING; no reference counterpart) ----
+//
+// Every row of an iteration reads the APP of the previous iteration and stores only its
+// new messages; then every variable's APP is rebuilt from its channel value and the new
+// messages of its edges, x = sat8(LLR + sum of messages), the sum exact (integer-valued
+// fp16 below 2048) and saturated once.  Two barriers per iteration whatever the level
+// structure.  PackF16x2 only (4 frames, two pair-words): APP [2][npad], messages
+// [2][dmax*m], the channel values [2][npad] (biased like the APP), then the LEARNED table.
+
+template <int KIND, int DT, bool EXACT>
+__device__ __forceinline__ void row_update_flood(uint32_t* app, uint32_t* msg, const Plan& P, int r, int d,
+                                                 bool noclip, uint32_t& ov, const uint16_t* lut)
+{
+    int v[DT];
+#pragma unroll
+    for (int j = 0; j < DT; j++)
+        if (EXACT || j < d) v[j] = __ldg(P.cols + j * P.m + r);
+    const int mstride = P.dmax * P.m;
+#pragma unroll
+    for (int w = 0; w < 2; w++) {
+        const uint32_t* A = app + w * P.npad;
+        uint32_t* M = msg + w * mstride;
+        uint32_t x[DT], mm[DT];
+#pragma unroll
+        for (int j = 0; j < DT; j++) {
+            if (EXACT || j < d) {
+                x[j] = A[v[j]];
+                mm[j] = M[j * P.m + r];
+            }
+        }
+        PackF16x2::update<KIND, DT, EXACT>(x, mm, d, noclip, ov, lut);
+#pragma unroll
+        for (int j = 0; j < DT; j++)
+            if (EXACT || j < d) M[j * P.m + r] = mm[j];
+    }
+}
+
+template <int KIND, int DT, bool EXACT>
+__global__ void __launch_bounds__(256) decode_flood_kernel(const Plan P, const Job J)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_odd[2];
+    using PK = PackF16x2;
+    const long long g = J.word0 + blockIdx.x;
+    const int mstride = P.dmax * P.m;
+    uint32_t* app = reinterpret_cast<uint32_t*>(smem_raw);
+    uint32_t* msg = app + 2 * P.npad;
+    uint32_t* llrb = msg + 2 * mstride;
+    uint16_t* slut = reinterpret_cast<uint16_t*>(llrb + 2 * P.npad);
+    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+
+    read_group(P, J, g, [&](int v, uint32_t w) {
+        Access<PK>::put(app, P.npad, v, w);
+        Access<PK>::put(llrb, P.npad, v, w);
+    });
+    for (int i = threadIdx.x; i < 2 * mstride; i += blockDim.x) msg[i] = 0;
+    __syncthreads();
+
+    int executed = 0;
+    bool passed = false;
+    for (int it = 0; it < J.iters; it++) {
+        uint32_t ov = 0;
+        const bool first = (it == 0);
+        if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
+        for (int r = threadIdx.x; r < P.m; r += blockDim.x) {
+            const int d = EXACT ? DT : __ldg(P.rowdeg + r);
+            const int cls = __ldg(P.rowcls + r);
+            const bool noclip = J.quirk && first && cls;
+            row_update_flood<KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov, slut + 128 * cls);
+        }
+        __syncthreads();
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x) {
+            const int e0 = __ldg(P.vptr + v), e1 = __ldg(P.vptr + v + 1);
+            uint32_t a0 = llrb[v], a1 = llrb[P.npad + v];
+            for (int e = e0; e < e1; e++) {
+                const int i = __ldg(P.vedge + e);
+                a0 = h2::add(a0, msg[i]);
+                a1 = h2::add(a1, msg[mstride + i]);
+            }
+            app[v] = h2::hmin(h2::fma_relu(a0, h2::ONE, 0u), h2::C255);
+            app[P.npad + v] = h2::hmin(h2::fma_relu(a1, h2::ONE, 0u), h2::C255);
+        }
+        __syncthreads();
+        executed = it + 1;
+        if (KIND == KIND_2NMS && it >= 1) {
+            if (!__syncthreads_or(ov != 0)) break;
+        }
+        if (KIND != KIND_2NMS && J.early) {
+            if (odd_rows_within_slack(J, ov, it, s_odd) && !__syncthreads_or(rows_unsatisfied<PK>(app, P))) {
+                passed = true;
+                break;
+            }
+        }
+    }
+
+    write_group(P, J, g, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+    if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
+    if (J.synd_out) {
+        const uint32_t bad = passed ? 0u : rows_odd_mask(P, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+        write_syndrome_flags(J, 4 * (g - J.word0), bad, 0xF);
+    }
+    if (J.app_out) {
+        uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
+        for (int v = threadIdx.x; v < P.n; v += blockDim.x)
+            ao[(long long)v * J.total_words + g] = Access<PK>::get(app, P.npad, v);
+    }
+    if (J.msg_out) {
+        uint32_t* mo = reinterpret_cast<uint32_t*>(J.msg_out);
+        for (int i = threadIdx.x; i < mstride; i += blockDim.x) {
             const int j = i / P.m, r = i - j * P.m;
             if (j < P.rowdeg[r])
                 mo[(long long)P.edge_orig[i] * J.total_words + g] = Access<PK>::get_msg(msg, mstride, i);

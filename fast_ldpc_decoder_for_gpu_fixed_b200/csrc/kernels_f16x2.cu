@@ -16,4 +16,16 @@ const void* kernel_table_f16x2(int kind, int variant)
     return table[kind][variant];
 }
 
+// the flooding schedule (decode_flood_kernel), same table shape
+#define LDPC_FLOOD_ENTRY(PK, KIND, D, EX) (const void*)decode_flood_kernel<KIND, D, EX>,
+#define LDPC_FLOOD_ROW(KIND) {LDPC_DEGREE_VARIANTS(LDPC_FLOOD_ENTRY, PackF16x2, KIND)},
+
+const void* kernel_table_flood(int kind, int variant)
+{
+    static const void* table[5][5] = {LDPC_FLOOD_ROW(KIND_MS) LDPC_FLOOD_ROW(KIND_OMS) LDPC_FLOOD_ROW(KIND_NMS)
+                                      LDPC_FLOOD_ROW(KIND_2NMS) LDPC_FLOOD_ROW(KIND_LEARNED)};
+    if (kind < 0 || kind > 4 || variant < 0 || variant > 4) return nullptr;
+    return table[kind][variant];
+}
+
 }  // namespace ldpc

@@ -94,6 +94,8 @@ struct ldpc_decoder {
     uint8_t* d_rowcls = nullptr;
     int2* d_levels = nullptr;
     int32_t* d_edge_orig = nullptr;
+    int32_t* d_vptr = nullptr;   // flooding: variable -> message indices (Plan::vptr / vedge)
+    int32_t* d_vedge = nullptr;
     int8_t* d_in = nullptr;    // staging for decode_host (reference: d_MSG_C_2_V as input staging)
     uint8_t* d_out = nullptr;  // staging for decode_host (reference: d_MSG_C_2_V as output staging)
     void* d_aux = nullptr;     // staging of iteration counts and syndrome flags for ldpc_decode_host_ex
@@ -321,6 +323,7 @@ const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2,
 const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
+const void* kernel_table_flood(int kind, int variant);
 }
 
 // shared memory of the QC kernel: the APP, 4 bytes per variable per pair of frames
@@ -429,6 +432,8 @@ static void decoder_free(ldpc_decoder* d)
     cudaFree(d->d_rowcls);
     cudaFree(d->d_levels);
     cudaFree(d->d_edge_orig);
+    cudaFree(d->d_vptr);
+    cudaFree(d->d_vedge);
     cudaFree(d->d_in);
     cudaFree(d->d_out);
     cudaFree(d->d_aux);
@@ -474,6 +479,20 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
     CUDA_TRY(cudaMemcpy(d->d_rowdeg, deg.data(), m, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(d->d_rowcls, cls.data(), m, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(d->d_levels, c->levels.data(), c->levels.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    {
+        // variable -> message indices j * m + r' (the flooding schedule's APP rebuild)
+        std::vector<int32_t> vptr(c->n + 1, 0), vedge(c->e);
+        for (int rp = 0; rp < m; rp++)
+            for (int j = 0; j < deg[rp]; j++) vptr[cols[(size_t)j * m + rp] + 1]++;
+        for (int v = 0; v < c->n; v++) vptr[v + 1] += vptr[v];
+        std::vector<int32_t> fill(vptr.begin(), vptr.end() - 1);
+        for (int rp = 0; rp < m; rp++)
+            for (int j = 0; j < deg[rp]; j++) vedge[fill[cols[(size_t)j * m + rp]]++] = j * m + rp;
+        CUDA_TRY(cudaMalloc(&d->d_vptr, vptr.size() * sizeof(int32_t)));
+        CUDA_TRY(cudaMalloc(&d->d_vedge, vedge.size() * sizeof(int32_t)));
+        CUDA_TRY(cudaMemcpy(d->d_vptr, vptr.data(), vptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(d->d_vedge, vedge.data(), vedge.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
     Plan& P = d->plan;
     P.n = c->n;
     P.npad = (c->n + 15) / 16 * 16;
@@ -486,6 +505,8 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
     P.levels = d->d_levels;
     P.edge_orig = d->d_edge_orig;
     P.rowrec = reinterpret_cast<const uint4*>(d->d_rowrec);
+    P.vptr = d->d_vptr;
+    P.vedge = d->d_vedge;
     return LDPC_OK;
 }
 
@@ -495,9 +516,13 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (!out || !c) return fail(LDPC_ERR_ARG, "ldpc_decoder_create: null pointer");
     if (kind < LDPC_MS || kind > LDPC_LEARNED) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
     if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
-    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES))
+    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES | LDPC_FLAG_FLOODING))
         return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
     const bool per_frame = flags & LDPC_FLAG_EARLY_STOP_FRAMES;
+    const bool flood = flags & LDPC_FLAG_FLOODING;
+    if (flood && (per_frame || (pack != LDPC_PACK_AUTO && pack != LDPC_PACK_F16X2)))
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_FLOODING: the flooding schedule runs on the 4-frame "
+                                          "LDPC_PACK_F16X2 level kernel, per-word early stop only");
     const bool early = (flags & LDPC_FLAG_EARLY_STOP) || per_frame;
     if (early && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
@@ -506,7 +531,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     // CTA for the fixed-iteration MS / OMS / NMS / xMS decoders (the fastest level kernel where
     // it applies), else SIMD4 (early stop; 2NMS; LEARNED, whose SIMD4 tables take any constants)
     if (pack == LDPC_PACK_AUTO)
-        pack = !early && (kind == LDPC_MS || kind == LDPC_OMS || kind == LDPC_NMS || kind == LDPC_XMS)
+        pack = flood || (!early && (kind == LDPC_MS || kind == LDPC_OMS || kind == LDPC_NMS || kind == LDPC_XMS))
                    ? LDPC_PACK_F16X2
                    : LDPC_PACK_SIMD4;
     if (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_FRAME) return fail(LDPC_ERR_ARG, "unknown pack %d", pack);
@@ -515,8 +540,9 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (c->dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", c->dmax, kMaxDegree);
     int npad = (c->n + 15) / 16 * 16;
     // fp16x2 without early termination: 2 frames per CTA (half the shared memory)
-    const bool half = pack == LDPC_PACK_F16X2 && kind != LDPC_2NMS && !early;
+    const bool half = pack == LDPC_PACK_F16X2 && kind != LDPC_2NMS && !early && !flood;
     size_t smem = half ? 4 * ((size_t)npad + (size_t)c->dmax * c->m) : smem_bytes(pack, npad, c->dmax, c->m);
+    if (flood) smem += 8 * (size_t)npad;  // the channel values the flooding APP is rebuilt from
     const size_t lut_smem = kind == LDPC_LEARNED ? 512 : 0;  // the iteration's magnitude tables
     smem += lut_smem;
     int dev = 0;
@@ -524,14 +550,14 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     QCParams probe;
-    bool qc_ok = pack_req == LDPC_PACK_AUTO || pack == LDPC_PACK_F16X2;
+    bool qc_ok = !flood && (pack_req == LDPC_PACK_AUTO || pack == LDPC_PACK_F16X2);
     int probe_wpt = 2;
     qc_ok = qc_ok && qc_kernel_for(c, kind, probe, false, &probe_wpt) && qc_smem(c, probe_wpt) + 512 <= (size_t)smem_max;
     // the 2-frame QC kernel is an explicit LDPC_PACK_F16X2 choice: AUTO keeps the level kernels
     // for those shapes (faster on some, slower on others, and a different early-stop unit)
     qc_ok = qc_ok && (probe_wpt == 2 || pack_req == LDPC_PACK_F16X2);
     if (!frame && smem > (size_t)smem_max && !qc_ok) {
-        if (pack_req != LDPC_PACK_AUTO || kind == LDPC_2NMS)
+        if (pack_req != LDPC_PACK_AUTO || kind == LDPC_2NMS || flood)
             return fail(LDPC_ERR_UNSUPPORTED, "decoder state of one frame group needs %zu B of shared memory (> %d)",
                         smem, smem_max);
         frame = true;  // one frame per CTA with packed row state
@@ -561,7 +587,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return rc;
     }
     int qc_wpt = 2;
-    const void* qk = !frame && (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2)
+    const void* qk = !frame && !flood && (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2)
                          ? qc_kernel_for(c, kind, d->qcp, early, &qc_wpt)
                          : nullptr;
     if (qc_wpt == 1 && pack_req != LDPC_PACK_F16X2) qk = nullptr;
@@ -592,6 +618,12 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->pack = LDPC_PACK_F16X2;
         d->smem = (int)(qc_smem(c, qc_wpt) + lut_smem);
         d->threads = c->z;
+    } else if (flood) {
+        // every row per iteration: as many threads as rows, up to 256
+        d->kfn = kernel_table_flood(kind == LDPC_XMS ? LDPC_OMS : (kind == LDPC_LEARNED ? 4 : kind), degree_variant(c));
+        d->path = 6;
+        d->smem = (int)smem;
+        d->threads = std::min(256, std::max(32, (c->m + 31) / 32 * 32));
     } else if (half) {
         d->kfn = kernel_table_f16x2h(kind == LDPC_XMS ? LDPC_OMS : (kind == LDPC_LEARNED ? 3 : kind), degree_variant(c));
         d->path = 2;
@@ -839,7 +871,7 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
-    if (d->path >= 3 && (d_app || d_msg))
+    if (d->path >= 3 && d->path != 6 && (d_app || d_msg))
         return fail(LDPC_ERR_UNSUPPORTED, "this decoder (path %d) has no state dumps", d->path);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
@@ -1068,10 +1100,13 @@ struct ldpc_batch {
     std::vector<int> cls;              // degree class of each code: 0 <= 8, 1 <= 16, 2 <= 32
     std::vector<int> dvar;             // its variant of the per-code kernels (degree_variant)
     std::vector<int> widest;           // its widest level
-    // per-code strategy: each code's own level kernel, one launch per code
+    // per-code strategy: one launch per code of that code's own decoder, chosen per code
+    // among the candidate kernels (BatchCand) by ldpc_batch_autotune or set uniformly by
+    // ldpc_batch_configure
     bool per_code = false;
-    std::vector<const void*> pc_kfn;
-    std::vector<int> pc_threads, pc_smem;
+    std::vector<ldpc_code> codes;                      // copies (the caller may destroy its codes)
+    std::vector<std::vector<ldpc_decoder*>> pc_dec;    // [code][candidate], created on first use
+    std::vector<int> pc_choice;                        // [code] candidate
     void* d_codes = nullptr;           // BatchCode[n]
     void* h_codes = nullptr;           // pinned staging of the same
     unsigned long long* d_counter = nullptr;
@@ -1092,10 +1127,19 @@ struct ldpc_batch {
     std::vector<cudaEvent_t> fork;   // [0]: the fork point, [i]: code i's end
 };
 
+// Kernels the per-code strategy can give a code: the layered level kernels of the three
+// packings, the QC register kernel (QC codes only: 4 frames per CTA on the regular base,
+// path 1, else 2 frames per CTA with early stop per frame pair, path 4) and the flooding
+// schedule (path 6)
+enum BatchCand { CAND_SIMD4 = 0, CAND_F16X2 = 1, CAND_I8 = 2, CAND_QC = 3, CAND_FLOOD = 4, CAND_COUNT = 5 };
+
 static void batch_free(ldpc_batch* b)
 {
     if (!b) return;
     for (auto* d : b->plans) decoder_free(d);
+    for (auto& v : b->pc_dec)
+        for (auto* d : v)
+            if (d) decoder_free(d);
     cudaFree(b->d_codes);
     cudaFreeHost(b->h_codes);
     cudaFree(b->d_counter);
@@ -1127,6 +1171,54 @@ static int batch_lut(ldpc_batch* b, int pack)
     return LDPC_OK;
 }
 
+// Frees the per-code decoders (they are re-created on use); a captured graph that refers
+// to their tables is dropped with them
+static void batch_drop_decoders(ldpc_batch* b)
+{
+    cudaDeviceSynchronize();
+    for (auto& v : b->pc_dec)
+        for (auto*& d : v)
+            if (d) {
+                decoder_free(d);
+                d = nullptr;
+            }
+    b->key.clear();
+}
+
+// The decoder of candidate `cand` for code i (created on first use, then kept), with the
+// batch's kind, early stop and learned constants.  Fails when the candidate cannot serve the
+// code (shared memory, row degree, not a QC code, constants off the fp16 grid).
+static int batch_code_decoder(ldpc_batch* b, int i, int cand, ldpc_decoder** out)
+{
+    ldpc_decoder*& d = b->pc_dec[i][cand];
+    if (!d) {
+        ldpc_code c = b->codes[i];
+        int pack = cand == CAND_SIMD4 ? LDPC_PACK_SIMD4 : (cand == CAND_I8 ? LDPC_PACK_I8 : LDPC_PACK_F16X2);
+        if (cand != CAND_QC) c.qc = false;  // the level kernels, also for a QC code
+        else if (!c.qc) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d is not quasi-cyclic", i);
+        const int flags = (b->early ? LDPC_FLAG_EARLY_STOP : 0) | (cand == CAND_FLOOD ? LDPC_FLAG_FLOODING : 0);
+        // nb_frames only bounds the words of a call; the batch passes its own counts
+        int rc = ldpc_decoder_create(&d, &c, b->kind, (size_t)1 << 40, pack, flags);
+        if (rc) return rc;
+        if (cand == CAND_QC && d->path != 1 && d->path != 4) {
+            decoder_free(d);
+            d = nullptr;
+            return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d has no QC register kernel", i);
+        }
+        if (b->kind == LDPC_LEARNED && !b->off.empty()) {
+            rc = ldpc_decoder_set_learned(d, b->lut_its, b->off.data(), b->sc.data());
+            if (rc) {
+                decoder_free(d);
+                d = nullptr;
+                return rc;
+            }
+        }
+    }
+    d->early_slack = b->slack;
+    if (out) *out = d;
+    return LDPC_OK;
+}
+
 // selects the strategy: one persistent kernel with this packing, CTA width and
 // resident CTAs per SM (0 = as many as fit), or (per_code) one launch of each
 // code's own level kernel with this packing
@@ -1136,24 +1228,12 @@ static int batch_configure(ldpc_batch* b, int pack, int threads, int ctas_per_sm
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
     const size_t lut = b->kind == LDPC_LEARNED ? 512 : 0;
     if (per_code) {
-        std::vector<const void*> kf;
-        std::vector<int> th, sm;
-        for (size_t i = 0; i < b->plans.size(); i++) {
-            const Plan& P = b->plans[i]->plan;
-            const void* f = kernel_for(pack, b->kind, b->dvar[i]);
-            const size_t smem = smem_bytes(pack, P.npad, P.dmax, P.m) + lut;
-            if (!f || smem > (size_t)smem_max)
-                return fail(LDPC_ERR_UNSUPPORTED, "batch: code %zu does not fit pack %d", i, pack);
-            CUDA_TRY(ldpc_internal_raise_smem(f, smem));
-            kf.push_back(f);
-            th.push_back(std::min(256, std::max(32, (b->widest[i] + 31) / 32 * 32)));
-            sm.push_back((int)smem);
+        (void)lut;
+        for (size_t i = 0; i < b->codes.size(); i++) {
+            int rc = batch_code_decoder(b, (int)i, pack, nullptr);
+            if (rc) return fail(rc, "batch: code %zu does not fit pack %d: %s", i, pack, ldpc_last_error_string());
         }
-        int rc = batch_lut(b, pack);
-        if (rc) return rc;
-        b->pc_kfn = kf;
-        b->pc_threads = th;
-        b->pc_smem = sm;
+        for (size_t i = 0; i < b->codes.size(); i++) b->pc_choice[i] = pack;
         b->per_code = true;
         b->pack = pack;
         b->kfn = nullptr;
@@ -1230,6 +1310,9 @@ extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes
         return fail(LDPC_ERR_CUDA, "ldpc_batch_create: %s", cudaGetErrorString(e));
     }
     for (int i = 0; i < n_codes; i++) {
+        b->codes.push_back(*codes[i]);
+        b->pc_dec.push_back(std::vector<ldpc_decoder*>(CAND_COUNT, nullptr));
+        b->pc_choice.push_back(CAND_SIMD4);
         const int dm = codes[i]->dmax;
         b->cls.push_back(dm <= 8 ? 0 : (dm <= 16 ? 1 : 2));
         b->dvar.push_back(degree_variant(codes[i]));
@@ -1266,7 +1349,13 @@ extern "C" int ldpc_batch_set_learned(ldpc_batch* b, int n_iters, const int8_t* 
     b->off.assign(offsets, offsets + 2 * n_iters);
     b->sc.assign(scales, scales + 2 * n_iters);
     b->lut_its = n_iters;
-    int rc = batch_configure(b, b->pack, b->threads, b->ctas_per_sm, b->per_code);
+    batch_drop_decoders(b);  // re-created with the new constants
+    int rc = LDPC_OK;
+    if (b->per_code) {
+        for (size_t i = 0; i < b->codes.size() && !rc; i++) rc = batch_code_decoder(b, (int)i, b->pc_choice[i], nullptr);
+    } else {
+        rc = batch_configure(b, b->pack, b->threads, b->ctas_per_sm, false);
+    }
     if (rc) {
         b->off.clear();
         b->sc.clear();
@@ -1281,6 +1370,7 @@ extern "C" int ldpc_batch_set_early_stop(ldpc_batch* b, int enabled, int slack)
     if (enabled && b->kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_batch_set_early_stop: slack must be >= 0");
+    if (b->early != (enabled != 0)) batch_drop_decoders(b);  // per-code decoders: re-created with the flag
     b->early = enabled != 0;
     b->slack = (unsigned)slack;
     b->key.clear();
@@ -1343,6 +1433,15 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
     void* codes = b->d_codes;
     unsigned long long* counter = b->d_counter;
     void* args[] = {(void*)&codes, (void*)&n, (void*)&counter, (void*)&total, (void*)&J};
+    if (b->per_code)
+        for (int i = 0; i < n; i++) {
+            ldpc_decoder* dc = nullptr;
+            int rc = batch_code_decoder(b, i, b->pc_choice[i], &dc);
+            if (rc) return rc;
+            key.push_back((uintptr_t)dc->kfn);
+        }
+    // the launches; per code: each code's own decoder (launch()), the codes forked onto the
+    // batch's side streams from `st` and joined back to it
     auto enqueue = [&]() -> cudaError_t {
         if (b->per_code) {
             cudaError_t e = cudaEventRecord(b->fork[0], st);
@@ -1351,18 +1450,12 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
                 cudaStream_t si = i == 0 ? st : b->side[i - 1];
                 if (i > 0) e = cudaStreamWaitEvent(si, b->fork[0], 0);
                 if (e != cudaSuccess) break;
-                Job Jc = J;
-                Jc.llr = d_llr[i];
-                Jc.out = d_out[i];
-                Jc.out_packed = out_format == LDPC_OUT_PACKED;
-                Jc.iters_out = d_iters_out ? d_iters_out[i] : nullptr;
-                Jc.synd_out = d_syndrome_ok ? d_syndrome_ok[i] : nullptr;
-                Jc.total_words = (long long)n_words[i];
-                Plan P = b->plans[i]->plan;
-                void* a[] = {(void*)&P, (void*)&Jc};
-                e = cudaLaunchKernel(b->pc_kfn[i], dim3((unsigned)n_words[i]), dim3(b->pc_threads[i]), a,
-                                     b->pc_smem[i], si);
-                if (e == cudaSuccess && i > 0) e = cudaEventRecord(b->fork[i], si);
+                ldpc_decoder* dc = b->pc_dec[i][b->pc_choice[i]];
+                if (launch(dc, d_llr[i], d_out[i], out_format == LDPC_OUT_PACKED, 0, (long long)n_words[i],
+                           (long long)n_words[i], iters, d_iters_out ? d_iters_out[i] : nullptr, nullptr, nullptr, si,
+                           nullptr, d_syndrome_ok ? d_syndrome_ok[i] : nullptr))
+                    return cudaErrorLaunchFailure;
+                if (i > 0) e = cudaEventRecord(b->fork[i], si);
                 if (e == cudaSuccess && i > 0) e = cudaStreamWaitEvent(st, b->fork[i], 0);
             }
             return e;
@@ -1397,34 +1490,107 @@ extern "C" int ldpc_batch_decode(ldpc_batch* b, const int8_t* const* d_llr, void
     return LDPC_OK;
 }
 
+// the per-code strategy with the per-code choices as they stand
+static void batch_use_per_code(ldpc_batch* b)
+{
+    b->per_code = true;
+    b->kfn = nullptr;
+    b->grid = b->threads = b->smem = b->ctas_per_sm = 0;
+    b->key.clear();
+}
+
+// Per-code choice: for each code, every candidate kernel (BatchCand) is timed alone on that
+// code's inputs and its frames whose decisions fail the syndrome are counted (the
+// d_syndrome_ok flags).  The fastest candidate wins among those that leave no more failing
+// frames than the reference's layered schedule (SIMD4) does, within 2 % and 2 frames: the
+// flooding schedule and the 2-frame QC kernel's per-pair early stop may converge differently.
+static int batch_tune_codes(ldpc_batch* b, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
+                            int iters, int32_t* const* d_iters_out, cudaStream_t st)
+{
+    size_t fmax = 0;
+    for (size_t i = 0; i < b->codes.size(); i++) fmax = std::max(fmax, 4 * n_words[i]);
+    if (fmax == 0) return LDPC_OK;
+    uint8_t* d_syn = nullptr;
+    CUDA_TRY(cudaMalloc(&d_syn, fmax));
+    std::vector<uint8_t> h_syn(fmax);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (size_t i = 0; i < b->codes.size(); i++) {
+        if (n_words[i] == 0) continue;
+        const long long w = (long long)n_words[i];
+        long long base_fail = -1;
+        double best = 1e30;
+        int best_c = b->pc_choice[i];
+        for (int c = 0; c < CAND_COUNT; c++) {
+            ldpc_decoder* dc = nullptr;
+            if (batch_code_decoder(b, (int)i, c, &dc)) continue;
+            int32_t* its = d_iters_out ? d_iters_out[i] : nullptr;
+            if (launch(dc, d_llr[i], d_out[i], 0, 0, w, w, iters, its, nullptr, nullptr, st, nullptr, d_syn)) continue;
+            if (cudaMemcpyAsync(h_syn.data(), d_syn, 4 * w, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                continue;
+            long long fail_c = 0;
+            for (long long f = 0; f < 4 * w; f++) fail_c += h_syn[f] == 0;
+            cudaEventRecord(e0, st);
+            bool ok = true;
+            for (int r = 0; r < 3 && ok; r++)
+                ok = !launch(dc, d_llr[i], d_out[i], 0, 0, w, w, iters, its, nullptr, nullptr, st, nullptr, nullptr);
+            cudaEventRecord(e1, st);
+            float ms = 0.f;
+            if (!ok || cudaEventSynchronize(e1) != cudaSuccess) continue;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (c == CAND_SIMD4) base_fail = fail_c;
+            const bool equal_fer = base_fail < 0 || fail_c <= base_fail + std::max(2LL, base_fail / 50);
+            if (equal_fer && ms / 3 < best) {
+                best = ms / 3;
+                best_c = c;
+            }
+        }
+        b->pc_choice[i] = best_c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_syn);
+    b->key.clear();
+    return LDPC_OK;
+}
+
 extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, void* const* d_out,
                                    const size_t* n_words, int iters, int32_t* const* d_iters_out, double* best_ms,
                                    void* stream)
 {
     if (!b) return fail(LDPC_ERR_ARG, "ldpc_batch_autotune: null batch");
     cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaSetDevice(b->device));
+    // the kernel of each code for the per-code strategy (schedule, packing, frames per CTA)
+    int rc = batch_tune_codes(b, d_llr, d_out, n_words, iters, d_iters_out, st);
+    if (rc) return rc;
+    const std::vector<int> choice = b->pc_choice;
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     const int packs[3] = {LDPC_PACK_SIMD4, LDPC_PACK_F16X2, LDPC_PACK_I8};
-    const int widths[4] = {64, 128, 256, 0};  // 0: the per-code strategy
+    const int widths[4] = {0, 64, 128, 256};  // 0: the per-code strategy (once, with the tuned choices)
     double best = 1e30;
     int bp = b->pack, bt = b->threads, bc = 0;
-    bool bpc = b->per_code;
+    bool bpc = false;
     const bool graph = b->use_graph;
     b->use_graph = false;  // time the launches themselves
     for (int p : packs) {
         for (int t : widths) {
             for (int half = 0; half < 2; half++) {
                 if (t == 0) {
-                    if (half || batch_configure(b, p, 0, 0, true)) continue;
+                    if (half || p != LDPC_PACK_SIMD4) continue;
+                    b->pc_choice = choice;
+                    batch_use_per_code(b);
                 } else {
                     if (batch_configure(b, p, t, 0)) continue;
                     const int ctas = half ? std::max(1, b->ctas_per_sm / 2) : b->ctas_per_sm;
                     if (half && ctas == b->ctas_per_sm) continue;
                     if (batch_configure(b, p, t, ctas)) continue;
                 }
-                int rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, nullptr, stream);
+                rc = ldpc_batch_decode(b, d_llr, d_out, n_words, iters, LDPC_OUT_BYTES, d_iters_out, nullptr, stream);
                 if (rc) continue;
                 float ms = 0.f;
                 cudaEventRecord(e0, st);
@@ -1446,10 +1612,46 @@ extern "C" int ldpc_batch_autotune(ldpc_batch* b, const int8_t* const* d_llr, vo
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->use_graph = graph;
-    int rc = batch_configure(b, bp, bt, bc, bpc);
-    if (rc) return rc;
+    b->pc_choice = choice;
+    if (bpc) {
+        batch_use_per_code(b);
+    } else {
+        rc = batch_configure(b, bp, bt, bc, false);
+        if (rc) return rc;
+    }
     if (best_ms) *best_ms = best;
     return best < 1e30 ? LDPC_OK : fail(LDPC_ERR_UNSUPPORTED, "ldpc_batch_autotune: no configuration ran");
+}
+
+extern "C" int ldpc_batch_set_code_kernel(ldpc_batch* b, int code, int candidate)
+{
+    if (!b || code < 0 || code >= (int)b->codes.size() || candidate < 0 || candidate >= CAND_COUNT)
+        return fail(LDPC_ERR_ARG, "ldpc_batch_set_code_kernel: bad argument");
+    CUDA_TRY(cudaSetDevice(b->device));
+    int rc = batch_code_decoder(b, code, candidate, nullptr);
+    if (rc) return rc;
+    if (!b->per_code) {
+        // the other codes keep the persistent kernel's packing as their level kernel
+        for (size_t i = 0; i < b->codes.size(); i++)
+            if ((int)i != code) b->pc_choice[i] = b->pack;
+    }
+    b->pc_choice[code] = candidate;
+    batch_use_per_code(b);
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_batch_code_info(const ldpc_batch* b, int code, int* info)
+{
+    if (!b || !info || code < 0 || code >= (int)b->codes.size())
+        return fail(LDPC_ERR_ARG, "ldpc_batch_code_info: bad argument");
+    const int c = b->pc_choice[code];
+    const ldpc_decoder* d = b->pc_dec[code][c];
+    info[0] = c;
+    info[1] = d ? d->path : -1;
+    info[2] = d ? d->threads : 0;
+    info[3] = d ? d->smem : 0;
+    info[4] = d ? d->ctas_per_sm : 0;
+    return LDPC_OK;
 }
 
 extern "C" int ldpc_batch_configure(ldpc_batch* b, int per_code, int pack, int threads, int ctas_per_sm)

@@ -77,9 +77,9 @@ class Decoder:
     lanes (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8;
     ``early_stop`` sets LDPC_FLAG_EARLY_STOP (syndrome early stop per word), or with
     ``early_stop="frame"`` LDPC_FLAG_EARLY_STOP_FRAMES (per frame, finished frames'
-    slots refilled; iteration counts per frame)."""
+    slots refilled; iteration counts per frame); ``flooding`` sets LDPC_FLAG_FLOODING."""
 
-    def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO", early_stop=False):
+    def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO", early_stop=False, flooding=False):
         if isinstance(code, str):
             code = load_table(code)
         self.code = code if isinstance(code, Code) else code.code
@@ -87,10 +87,12 @@ class Decoder:
         self.kind = kind.upper()
         self.nb_frames = int(nb_frames)
         h = ctypes.c_void_p()
+        flags = _lib.FLAG_EARLY_STOP_FRAMES if early_stop == "frame" else (_lib.FLAG_EARLY_STOP if early_stop else 0)
+        if flooding:
+            flags |= _lib.FLAG_FLOODING
         _lib.check(_lib.lib().ldpc_decoder_create(
             ctypes.byref(h), self.native.handle, _lib.KINDS[self.kind], self.nb_frames,
-            _lib.PACKS[pack.upper()], _lib.FLAG_EARLY_STOP_FRAMES if early_stop == "frame"
-            else (_lib.FLAG_EARLY_STOP if early_stop else 0)))
+            _lib.PACKS[pack.upper()], flags))
         self.handle = h
         self.early_stop = bool(early_stop)
         self.per_frame = early_stop == "frame"
@@ -244,6 +246,20 @@ class Batch:
 
     def set_early_stop(self, enabled=True, slack=_lib.EARLY_STOP_DEFAULT_SLACK):
         _lib.check(_lib.lib().ldpc_batch_set_early_stop(self.handle, int(bool(enabled)), int(slack)))
+
+    def set_code_kernel(self, candidates):
+        """Per-code kernels (ldpc_batch_set_code_kernel): one candidate number per code
+        (0 SIMD4, 1 F16X2, 2 I8 level kernels, 3 QC register kernel, 4 flooding)."""
+        for i, c in enumerate(candidates):
+            _lib.check(_lib.lib().ldpc_batch_set_code_kernel(self.handle, int(i), int(c)))
+
+    def code_info(self, i):
+        """The per-code strategy's kernel of code i (ldpc_batch_code_info)."""
+        a = (ctypes.c_int * 5)()
+        _lib.check(_lib.lib().ldpc_batch_code_info(self.handle, int(i), a))
+        names = {0: "SIMD4", 1: "F16X2", 2: "I8", 3: "QC", 4: "FLOODING"}
+        return {"candidate": names.get(a[0], a[0]), "path": a[1], "threads": a[2], "smem": a[3],
+                "ctas_per_sm": a[4]}
 
     def info(self):
         a = (ctypes.c_int * 9)()

@@ -147,6 +147,16 @@ void ldpc_code_destroy(ldpc_code* code);
  * no state dumps and no ldpc_simulate. */
 #define LDPC_FLAG_EARLY_STOP_FRAMES 4
 
+/* Flooding schedule (no reference counterpart; the reference is row-layered): every
+ * check row of an iteration reads the a-posteriori values of the previous iteration,
+ * and after all rows each variable's value is rebuilt as sat8(LLR + the sum of its
+ * edges' new messages), the sum taken exactly and saturated once.  Two barriers per
+ * iteration instead of one per level, at the price of more iterations to converge.
+ * Decoder path 6: the 4-frame LDPC_PACK_F16X2 level kernel (AUTO selects it), with or
+ * without LDPC_FLAG_EARLY_STOP; not with LDPC_FLAG_EARLY_STOP_FRAMES.  The CPU oracle
+ * states the same schedule (oracle_set_schedule). */
+#define LDPC_FLAG_FLOODING 8
+
 /* nb_frames counts 32-bit lanes like the reference's constructor argument:
  * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
  * Unlike the reference (decoder_oms/CGPU_Decoder_OMS_SIMD.cu:101-105), any
@@ -284,7 +294,8 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
  * CTA: LDPC_PACK_F16X2 for every kind but 2NMS, 3 = one frame per CTA with
  * packed row state: LDPC_PACK_FRAME, 4 = QC register-message with 2 frames per
  * CTA, see LDPC_PACK_F16X2, 5 = QC register-message with per-frame early stop,
- * see LDPC_FLAG_EARLY_STOP_FRAMES) */
+ * see LDPC_FLAG_EARLY_STOP_FRAMES, 6 = level kernel with the flooding schedule, see
+ * LDPC_FLAG_FLOODING) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
@@ -315,14 +326,33 @@ int ldpc_batch_decode(ldpc_batch* batch, const int8_t* const* d_llr, void* const
                       int iters, int out_format, int32_t* const* d_iters_out,
                       uint8_t* const* d_syndrome_ok, void* stream);
 
-/* Times, on these inputs (outputs are overwritten), the two strategies: the
- * persistent kernel for each packing (SIMD4, F16X2, I8), CTA width (64, 128,
- * 256) and residency (as many CTAs per SM as fit, or half), and one launch of
- * each code's own kernel per packing (shared memory sized per code, all launches
- * in the same graph with LDPC_BATCH_GRAPH); keeps the fastest and returns its
- * time per decode in *best_ms. */
+/* Times, on these inputs (outputs are overwritten), the two strategies and keeps the
+ * fastest, returning its time per decode in *best_ms:
+ *  - one launch per code (shared memory sized per code, the launches side by side and,
+ *    with LDPC_BATCH_GRAPH, in one graph), each code with its own kernel: first, per
+ *    code, every candidate is timed alone - the level kernel of each packing (SIMD4,
+ *    F16X2, I8: 4 or 2 frames per CTA), the QC register kernel (QC codes: 4 frames per
+ *    CTA on the regular base, else 2 with early stop per frame pair) and the flooding
+ *    schedule (LDPC_FLAG_FLOODING) - and the
+ *    fastest is kept among those whose frames failing the syndrome are no more than the
+ *    layered SIMD4 kernel's (within 2 % and 2 frames), so that a faster schedule is
+ *    never bought with a higher frame error rate;
+ *  - the persistent kernel for each packing, CTA width (64, 128, 256) and residency
+ *    (as many CTAs per SM as fit, or half).
+ * ldpc_batch_code_info reports each code's choice. */
 int ldpc_batch_autotune(ldpc_batch* batch, const int8_t* const* d_llr, void* const* d_out, const size_t* n_words,
                         int iters, int32_t* const* d_iters_out, double* best_ms, void* stream);
+
+/* The per-code strategy's kernel of code `code`: info[0] = candidate (0 SIMD4, 1 F16X2,
+ * 2 I8 level kernels, 3 the QC register kernel, 4 the flooding schedule), info[1] = its
+ * decoder path (ldpc_decoder_info), info[2] = threads per CTA, info[3] = shared bytes per
+ * CTA, info[4] = CTAs per SM; path -1 when that kernel has not been set up yet. */
+int ldpc_batch_code_info(const ldpc_batch* batch, int code, int* info);
+
+/* Gives code `code` the per-code kernel `candidate` (as ldpc_batch_code_info numbers them)
+ * and selects the per-code strategy; LDPC_ERR_UNSUPPORTED when that kernel cannot serve
+ * the code. */
+int ldpc_batch_set_code_kernel(ldpc_batch* batch, int code, int candidate);
 
 /* Sets the strategy by hand: per_code = 0: the persistent kernel with this pack,
  * CTA width (32..256) and resident CTAs per SM (0 = as many as fit); per_code = 1:

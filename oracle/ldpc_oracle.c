@@ -150,6 +150,19 @@ static int word_syndrome_zero(int n, int m, const int32_t* row_ptr, const int32_
     return 1;
 }
 
+/* Flooding schedule (LDPC_FLAG_FLOODING, no reference counterpart; set by
+ * oracle_set_schedule): every row of an iteration reads the APP of the previous
+ * iteration, computes its messages with the same check update as the layered
+ * schedule, and only after all rows APP[v] = sat8(LLR[v] + sum of the new messages
+ * of v's edges), the sum taken exactly and saturated once. */
+static int g_flood = 0;
+
+int oracle_set_schedule(int flooding)
+{
+    g_flood = flooding ? 1 : 0;
+    return 0;
+}
+
 static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols,
                        const uint8_t* row_class, int kind, int iters,
                        int8_t* app, int8_t* msg, int early, int nl)
@@ -160,10 +173,20 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
     for (int r = 0; r < m; r++)
         if (row_ptr[r + 1] - row_ptr[r] > dmax) dmax = row_ptr[r + 1] - row_ptr[r];
     int* tv = (int*)malloc(sizeof(int) * (dmax > 0 ? dmax : 1));
+    const int flood = g_flood;
+    int8_t* llr0 = NULL; /* flooding: the channel values of the nl lanes */
+    int* acc = NULL;     /* flooding: LLR + sum of the iteration's messages, per lane and variable */
+    if (flood) {
+        llr0 = (int8_t*)malloc((size_t)nl * n);
+        acc = (int*)malloc(sizeof(int) * (size_t)nl * n);
+        memcpy(llr0, app, (size_t)nl * n);
+    }
     int executed = 0;
     for (int it = 0; it < iters; it++) {
         int ov_sign = 0; /* OR over rows and lanes of the extrinsic sign parity */
         int odd_rows = 0; /* (row, lane) pairs whose extrinsic sign parity was odd */
+        if (flood)
+            for (size_t i = 0; i < (size_t)nl * n; i++) acc[i] = llr0[i];
         for (int r = 0; r < m; r++) {
             int b = row_ptr[r], d = row_ptr[r + 1] - b;
             for (int lane = 0; lane < nl; lane++) {
@@ -188,12 +211,17 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
                     int s = sgn ^ (t > 0);
                     int out = s ? (int)(int8_t)re : vneg8(re);
                     M[b + j] = (int8_t)out;
-                    A[cols[b + j]] = (int8_t)sat8(t + out);
+                    if (flood)
+                        acc[(size_t)lane * n + cols[b + j]] += out;
+                    else
+                        A[cols[b + j]] = (int8_t)sat8(t + out);
                 }
                 ov_sign |= sgn;
                 odd_rows += sgn;
             }
         }
+        if (flood)
+            for (size_t i = 0; i < (size_t)nl * n; i++) app[i] = (int8_t)sat8(acc[i]);
         executed = it + 1;
         if (et && it >= 1 && ov_sign == 0) break;
         /* syndrome early stop (LDPC_FLAG_EARLY_STOP, no reference counterpart;
@@ -203,6 +231,8 @@ static int decode_word(int n, int m, const int32_t* row_ptr, const int32_t* cols
         if (early && odd_rows <= early - 1 && word_syndrome_zero(n, m, row_ptr, cols, app, nl)) break;
     }
     free(tv);
+    free(llr0);
+    free(acc);
     return executed;
 }
 

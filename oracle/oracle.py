@@ -58,6 +58,8 @@ def lib():
         L.oracle_sigma.restype = ctypes.c_double
         L.oracle_set_learned.argtypes = [i, P, P]
         L.oracle_set_learned.restype = i
+        L.oracle_set_schedule.argtypes = [i]
+        L.oracle_set_schedule.restype = i
         L.oracle_philox.argtypes = [P, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
         L.oracle_awgn.argtypes = [P, P, ctypes.c_size_t, i, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, P,
                                   ctypes.c_size_t]
@@ -69,8 +71,13 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
+def set_schedule(flooding):
+    """Layered (False, the reference's) or flooding (True) schedule for decode()."""
+    lib().oracle_set_schedule(int(bool(flooding)))
+
+
 def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=None, early_stop=False,
-           early_slack=128, per_frame=False, pairs=False):
+           early_slack=128, per_frame=False, pairs=False, flooding=False):
     """Decodes ``llr`` (int8, nframes*n bytes, frame-major unless interleaved).
 
     Returns dict with ``hard`` [nframes, n] uint8, ``iters`` [nframes/4] and,
@@ -81,7 +88,8 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     stops on its own and ``iters`` has one entry per frame (LDPC_PACK_FRAME,
     LDPC_FLAG_EARLY_STOP_FRAMES);
     ``pairs``: frames 4g, 4g+1 and 4g+2, 4g+3 stop as pairs and ``iters`` has the
-    larger count of each word (the 2-frame QC kernel, decoder path 4).
+    larger count of each word (the 2-frame QC kernel, decoder path 4);
+    ``flooding``: the flooding schedule of LDPC_FLAG_FLOODING instead of the layered one.
     """
     k = KINDS[kind.upper()] if isinstance(kind, str) else int(kind)
     if interleaved is None:
@@ -93,10 +101,14 @@ def decode(code, kind, llr, iters, interleaved=None, want_state=False, nthreads=
     app = np.zeros(code.n * nframes, dtype=np.int8) if want_state else None
     msg = np.zeros(code.e * nframes, dtype=np.int8) if want_state else None
     nt = nthreads or os.cpu_count() or 1
-    rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
-                                k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
-                                _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0,
-                                1 if per_frame else (2 if pairs else 4))
+    set_schedule(flooding)
+    try:
+        rc = lib().oracle_decode_ex(code.n, code.m, _p(code.row_ptr), _p(code.cols), _p(code.row_class),
+                                    k, int(iters), nframes, int(bool(interleaved)), _p(llr), _p(hard),
+                                    _p(app), _p(msg), _p(it), nt, 1 + int(early_slack) if early_stop else 0,
+                                    1 if per_frame else (2 if pairs else 4))
+    finally:
+        set_schedule(False)
     if rc != 0:
         raise ValueError("oracle_decode rejected the arguments")
     out = {"hard": hard, "iters": it}

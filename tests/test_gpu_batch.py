@@ -40,13 +40,22 @@ def _inputs(cs, words, seed):
     return host, llrs, outs, its
 
 
-def _check(cs, words, host, outs, its, kind, iters, early):
+def _check(cs, words, host, outs, its, kind, iters, early, batch=None):
+    """Each code against the oracle; with `batch` in the per-code strategy, under the
+    schedule of the kernel chosen for that code (flooding, or the 2-frame QC kernel's
+    per-pair early stop)."""
     import torch
     torch.cuda.synchronize()
-    for c, w, llr, o, it in zip(cs, words, host, outs, its):
-        ref = oracle.decode(c, kind, llr, iters, interleaved=False, early_stop=early)
-        assert np.array_equal(o.cpu().numpy().reshape(4 * w, c.n), ref["hard"]), c.name
-        assert np.array_equal(it.cpu().numpy(), ref["iters"]), c.name
+    per_code = batch is not None and batch.info()["per_code"]
+    for i, (c, w, llr, o, it) in enumerate(zip(cs, words, host, outs, its)):
+        kw = {}
+        if per_code:
+            ci = batch.code_info(i)
+            kw["flooding"] = ci["candidate"] == "FLOODING"
+            kw["pairs"] = ci["path"] == 4 and early
+        ref = oracle.decode(c, kind, llr, iters, interleaved=False, early_stop=early, **kw)
+        assert np.array_equal(o.cpu().numpy().reshape(4 * w, c.n), ref["hard"]), (c.name, kw)
+        assert np.array_equal(it.cpu().numpy(), ref["iters"]), (c.name, kw)
 
 
 @pytest.mark.parametrize("early", [False, True])
@@ -106,7 +115,24 @@ def test_batch_autotune(cuda):
     for o in outs:
         o.zero_()
     b.decode(llrs, outs, words, 20, d_iters=its)
-    _check(cs, words, host, outs, its, "OMS", 20, True)
+    _check(cs, words, host, outs, its, "OMS", 20, True, batch=b)
+    b.close()
+
+
+@pytest.mark.parametrize("cand", ["FLOODING", "QC"])
+def test_batch_per_code_candidates(cuda, cand):
+    """Every code on the flooding schedule, or on the QC register kernel, through the
+    per-code strategy, against the oracle under that schedule."""
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
+    cs = codes()
+    words = [3, 2, 4, 2]
+    host, llrs, outs, its = _inputs(cs, words, 17)
+    b = Batch(cs, "OMS", early_stop=True)
+    b.configure(per_code=True, pack="SIMD4")
+    b.set_code_kernel([{"FLOODING": 4, "QC": 3}[cand]] * len(cs))
+    b.decode(llrs, outs, words, 20, d_iters=its)
+    assert all(b.code_info(i)["candidate"] == cand for i in range(len(cs)))
+    _check(cs, words, host, outs, its, "OMS", 20, True, batch=b)
     b.close()
 
 
