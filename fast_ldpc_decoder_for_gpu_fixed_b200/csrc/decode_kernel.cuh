@@ -155,13 +155,28 @@ __device__ __forceinline__ void read_group(const Plan& P, const Job& J, long lon
     } else if ((n & 3) == 0) {
         const uint32_t* f0 = reinterpret_cast<const uint32_t*>(J.llr + (4 * (g - J.word0)) * (long long)n);
         const int n4 = n >> 2;
-        for (int q = threadIdx.x; q < n4; q += blockDim.x) {
-            uint32_t a[4], w[4];
+        // the loads of B loop trips are issued before any of them is used, so that one
+        // global latency, not B, starts each word
+        constexpr int B = 4;
+        for (int q0 = threadIdx.x; q0 < n4; q0 += B * blockDim.x) {
+            uint32_t a[B][4];
 #pragma unroll
-            for (int k = 0; k < 4; k++) a[k] = __ldg(f0 + k * n4 + q);
-            transpose4x4(a, w);
+            for (int t = 0; t < B; t++) {
+                const int q = q0 + t * blockDim.x;
+                if (q < n4)
 #pragma unroll
-            for (int j = 0; j < 4; j++) put(4 * q + j, w[j]);
+                    for (int k = 0; k < 4; k++) a[t][k] = __ldg(f0 + k * n4 + q);
+            }
+#pragma unroll
+            for (int t = 0; t < B; t++) {
+                const int q = q0 + t * blockDim.x;
+                if (q < n4) {
+                    uint32_t w[4];
+                    transpose4x4(a[t], w);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) put(4 * q + j, w[j]);
+                }
+            }
         }
     } else {
         const int8_t* f0 = J.llr + (4 * (g - J.word0)) * (long long)n;

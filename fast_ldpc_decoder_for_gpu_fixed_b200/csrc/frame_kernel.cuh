@@ -7,8 +7,10 @@
 // messages (194 K for the rate-1/2 IRA code) go to the decoder's scratch in global
 // memory, one byte per edge, 8 bytes per check row for its edges 0-7 (and 8 more for
 // edges 8-15): the thread that updates a row reads and writes its row words
-// coalesced with the other rows of the level, two levels ahead of their use, so the
-// latency hides behind the levels in between.  Per frame and iteration that is 2E
+// coalesced with the other rows of the level, a level ahead of their use, so the
+// latency hides behind the level in between.  (Two levels ahead spilled the
+// prefetched registers under the two-CTAs-per-SM register budget, and a spill waits
+// for its load.)  Per frame and iteration that is 2E
 // bytes of message traffic, the HBM-bound case of this decoder.
 //
 // Early stop (ET) is per frame: the frame stops after an iteration in which at
@@ -136,7 +138,7 @@ __device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const 
 
 // The row a thread updates in one level: its record (columns, degree, class; see
 // Plan::rowrec), its index, and its c->v messages.  Records and messages do not depend
-// on the frame's APP, so they are loaded two levels ahead: the record table (1 MB for
+// on the frame's APP, so they are loaded a level ahead: the record table (1 MB for
 // M = 32400) lives in L2 and the messages in the decoder's scratch in HBM.
 struct FrameRow {
     uint4 c0, c1;
@@ -166,8 +168,8 @@ struct FrameMsgs {
 };
 
 // Loads issued where they stand: the compiler may not move a volatile asm across the
-// level barriers, so a load issued two levels ahead stays two levels ahead instead of
-// being sunk next to its use to save registers.
+// level barriers, so a load issued a level ahead stays a level ahead instead of being
+// sunk next to its use to save registers.
 __device__ __forceinline__ uint4 ld_nc_v4(const uint4* p)
 {
     uint4 v;
@@ -328,20 +330,19 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J, l
     __shared__ unsigned s_odd[2];
     const FrameMsgs M = {J.fmsg + (long long)blockIdx.x * P.m, J.fmsg + (J.fslots + blockIdx.x) * (long long)P.m};
     const int nl = P.nlevels;
-    // messages are fetched with the records two levels ahead; a row's messages are written
-    // back when its level is updated, so with fewer than 3 levels per iteration the fetch
-    // would come before that write: such codes load them when the row is updated
-    const bool pf = nl >= 3;
+    // messages are fetched with the records one level ahead; a row's messages are written
+    // back when its level is updated, so with a single level per iteration the fetch would
+    // come before that write: such codes load them when the row is updated
+    const bool pf = nl >= 2;
     for (long long lf = blockIdx.x; lf < frames; lf += gridDim.x) {
         const long long f = 4 * J.word0 + lf;
         if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
         read_frame(P, J, f, [&](int v, int x) { app[v] = (int8_t)x; });
         __syncthreads();
 
-        FrameRow next1, next2;  // the rows of levels l+1 and l+2 (cyclically)
-        fetch_row<DT>(P, M, 0, next1, pf);
-        fetch_row<DT>(P, M, nl > 1 ? 1 : 0, next2, pf);
-        int lf2 = nl > 2 ? 2 : 2 % nl;  // level fetched next
+        FrameRow next;  // the row of level l+1 (cyclically)
+        fetch_row<DT>(P, M, 0, next, pf);
+        int lnext = nl > 1 ? 1 : 0;  // level fetched next
         int executed = 0;
         bool passed = false;  // stopped by the syndrome early stop: every check holds
         for (int it = 0; it < J.iters; it++) {
@@ -349,10 +350,9 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J, l
             const bool first = it == 0, keep = it + 1 < J.iters;  // the last iteration's messages are not needed
             if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
             for (int l = 0; l < nl; l++) {
-                FrameRow cur = next1;
-                next1 = next2;
-                fetch_row<DT>(P, M, lf2, next2, pf);
-                lf2 = lf2 + 1 == nl ? 0 : lf2 + 1;
+                FrameRow cur = next;
+                fetch_row<DT>(P, M, lnext, next, pf);
+                lnext = lnext + 1 == nl ? 0 : lnext + 1;
                 if (cur.r < cur.end) {
                     if (!pf && !first) load_msgs<DT>(M, cur);
                     const bool noclip = J.quirk && first && cur.cls();
