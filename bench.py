@@ -261,6 +261,8 @@ def run_batch(args):
     b = Batch(codes, args.kind, early_stop=True, graph=True)
     tune_ms = b.autotune(llrs, outs, words, args.iters, d_iters=its, stream=st)
     info = b.info()
+    if info["per_code"]:
+        info["code_kernels"] = [b.code_info(i) for i in range(len(codes))]
 
     def step():
         b.decode(llrs, outs, words, args.iters, d_iters=its, stream=st)
@@ -549,6 +551,7 @@ def main():
                          "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, "
                                         "all SMs; profiles/int_peak.md); peak_nominal: 148 SMs x 128 lanes x 1.965 GHz"},
             "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
+                             "peak_source": peaks.get("source", "MEASURED_PEAKS.json"),
                              "unit": "GB/s", "frac": (hbm_bytes / (ms_step * 1e-3) / 1e9) / peaks["hbm_gbs"]
                              if peaks.get("hbm_gbs") else None, "alg_bytes_per_launch": hbm_bytes},
             "cpu_baseline": cpu,

@@ -251,7 +251,11 @@ class Batch:
         """Per-code kernels (ldpc_batch_set_code_kernel): one candidate number per code
         (0 SIMD4, 1 F16X2, 2 I8 level kernels, 3 QC register kernel, 4 flooding)."""
         for i, c in enumerate(candidates):
-            _lib.check(_lib.lib().ldpc_batch_set_code_kernel(self.handle, int(i), int(c)))
+            self.set_code_kernel_one(i, c)
+
+    def set_code_kernel_one(self, i, candidate):
+        """Code i's per-code kernel (ldpc_batch_set_code_kernel)."""
+        _lib.check(_lib.lib().ldpc_batch_set_code_kernel(self.handle, int(i), int(candidate)))
 
     def code_info(self, i):
         """The per-code strategy's kernel of code i (ldpc_batch_code_info)."""
