@@ -9,7 +9,8 @@ Default workload (the metric: learned-offset decoder vs plain OMS at equal FER):
   65536 frames per GPU, at most 10 layered iterations.
   value      : the deployed learned-offset decoder (LDPC_LEARNED with the constants in
                fast_ldpc_decoder_for_gpu_fixed_b200/trained/qc3x6_z256_T10.json,
-               syndrome early stop per 4-frame word), kernel only, LLRs resident in HBM
+               syndrome early stop per 4-frame word; --early-unit pairs|frame for the
+               other units), kernel only, LLRs resident in HBM
   plain_oms  : the plain 8-bit OMS kernel (offset 1, 10 fixed iterations) on the same
                batch and GPU; vs_plain_oms = value / plain_oms.value
   oms_early_stop : plain OMS with the same early stop; early_stop_gain = its value /
@@ -58,7 +59,10 @@ def parse():
     ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira", "batch"])
     ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
     ap.add_argument("--per-frame", action="store_true",
-                    help="early stop per frame with slot refill (LDPC_FLAG_EARLY_STOP_FRAMES) instead of per 4-frame word")
+                    help="early stop per frame with slot refill (LDPC_FLAG_EARLY_STOP_FRAMES); same as --early-unit frame")
+    ap.add_argument("--early-unit", default="word", choices=["word", "pairs", "frame"],
+                    help="frames that stop together under the early stop of the learned workload: the 4-frame word "
+                         "(LDPC_FLAG_EARLY_STOP, default), each frame pair (LDPC_FLAG_EARLY_STOP_PAIRS) or each frame")
     ap.add_argument("--fer-frames", type=int, default=1 << 20)
     ap.add_argument("--no-sweep", dest="sweep", action="store_false",
                     help="skip the learned-vs-plain ratio over Eb/N0 1.5..2.5 dB")
@@ -72,6 +76,8 @@ def parse():
     a = ap.parse_args()
     if a.table:
         a.workload = "oms"
+    if a.per_frame:
+        a.early_unit = "frame"
     if a.ebn0 is None:
         a.ebn0 = {"learned": 2.25, "oms": 2.0, "ira": 1.4, "batch": 3.0}[a.workload]
     if a.workload == "batch":
@@ -387,7 +393,7 @@ def main():
     early = args.workload in ("learned", "ira")
     constants = load_constants(args.constants)[:2] if learned else None
     kind = "LEARNED" if learned else args.kind
-    es = ("frame" if args.per_frame else True) if early else False
+    es = _early_mode(args) if early else False
     dec = Decoder(code, kind, nb_frames=words, pack=args.pack, early_stop=es)
     if constants is not None:
         dec.set_learned(*constants)
@@ -471,7 +477,7 @@ def main():
         launches += args.steps
         oms_es = {"value": world * info_bits * args.steps / (ems * 1e-3) / 1e9, "unit": "Gbit/s",
                   "ms_per_step": ems / args.steps, "mean_iterations": float(e_its.float().mean()),
-                  "early_stop": "per_frame" if per_frame else "per_word"}
+                  "early_stop": _early_name(args, per_frame)}
         edec.close()
 
     # equal-FER evidence on more frames (untimed)
@@ -495,8 +501,17 @@ def main():
     # roofline of the decode kernel (one launch per step), from the iterations it executed
     int_peak = _int_peak()
     one_lane = info["path"] == 3  # one frame per thread lane: one int32 op per frame-edge-update
+    pair_iters = None
     if per_frame:
         edge_updates = float(d_its.sum().item()) * code.e
+    elif es == "pairs":
+        # the iterations each pair ran: the same frames decoded with each pair doubled into a
+        # word of its own (the pairs are independent, so its count is that pair's), untimed
+        pair_iters = _pair_counts(code, kind, constants, d_llr, words, args, stream)
+        word_max = torch.maximum(pair_iters[:words], pair_iters[words:])
+        if not torch.equal(word_max, d_its):
+            raise RuntimeError("per-pair iteration counts disagree with the word counts")
+        edge_updates = float(pair_iters.sum().item()) * 2 * code.e
     else:
         edge_updates = float(d_its.sum().item()) * 4 * code.e if early else float(args.frames) * code.e * args.iters
     alg_ops = (1.0 if one_lane else 2.0) * edge_updates
@@ -527,8 +542,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic (seeded codewords, AWGN, reference quantiser)",
             "config": {"workload": workload, "kind": kind, "pack": info["pack"], "frames_per_gpu": args.frames,
-                       "max_iterations": args.iters, "early_stop": ("per_frame" if per_frame else "per_word") if early
-                       else False, "mean_iterations": mean_iters,
+                       "max_iterations": args.iters, "early_stop": _early_name(args, per_frame) if early else False, "mean_iterations": mean_iters,
                        "ebn0_db": args.ebn0, "batch_fer": fer, "batch_ber": ber,
                        "l2": ("inputs %d MB: L2 flushed (256 MB write) between steps, outside the timed spans" % (
                            llr.nbytes // 2**20)) if flush else
@@ -547,6 +561,7 @@ def main():
                          "frac": achieved / int_peak, "traffic": _traffic(info["path"], args),
                          "peak_nominal": NOMINAL_INT_TOPS, "frac_nominal": achieved / NOMINAL_INT_TOPS,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
+                         "mean_pair_iterations": float(pair_iters.float().mean()) if pair_iters is not None else None,
                          "ops_per_edge_update": 1.0 if one_lane else 2.0,
                          "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, "
                                         "all SMs; profiles/int_peak.md); peak_nominal: 148 SMs x 128 lanes x 1.965 GHz"},
@@ -568,6 +583,40 @@ def main():
     return 0
 
 
+def _pair_counts(code, kind, constants, d_llr, words, args, stream):
+    """Iterations run by each frame pair under LDPC_FLAG_EARLY_STOP_PAIRS: entry g (g < words)
+    is pair 0 of word g, entry words + g its pair 1."""
+    import torch
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import Decoder, _lib
+    l4 = d_llr.view(words, 4, code.n)
+    dup = torch.cat([l4[:, [0, 1, 0, 1]], l4[:, [2, 3, 2, 3]]], 0).reshape(-1).contiguous()
+    out = torch.empty(dup.numel(), dtype=torch.uint8, device="cuda")
+    its = torch.zeros(2 * words, dtype=torch.int32, device="cuda")
+    dec = Decoder(code, kind, nb_frames=2 * words, pack=args.pack, early_stop="pairs")
+    if constants is not None:
+        dec.set_learned(*constants)
+    if args.slack is not None:
+        dec.set_early_stop(True, args.slack)
+    dec.decode_device(dup, out, 2 * words, args.iters, _lib.OUT_BYTES, its, stream)
+    torch.cuda.synchronize()
+    dec.close()
+    return its
+
+
+def _early_mode(args):
+    """Decoder early_stop argument of the learned workload (the IRA workload's frame path
+    stops per frame whatever it is given)."""
+    if args.workload != "learned":
+        return True
+    return {"word": True, "pairs": "pairs", "frame": "frame"}[args.early_unit]
+
+
+def _early_name(args, per_frame):
+    if per_frame:
+        return "per_frame"
+    return "per_pair" if _early_mode(args) == "pairs" else "per_word"
+
+
 def _sweep(code, constants, args, stream):
     """Learned decoder with early stop vs plain OMS (10 fixed iterations) at each Eb/N0 of the
     config-2 range: kernel Gbit/s of both on 65 536 channel frames, and their FER on 2^18 frames."""
@@ -578,8 +627,8 @@ def _sweep(code, constants, args, stream):
     cw = torch.from_numpy(random_codewords(code, 64, 77)).cuda()
     llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
     out = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")
-    es = "frame" if args.per_frame else True
-    its = torch.zeros(4 * words if args.per_frame else words, dtype=torch.int32, device="cuda")
+    es = _early_mode(args)
+    its = torch.zeros(4 * words if es == "frame" else words, dtype=torch.int32, device="cuda")
     ldec = Decoder(code, "LEARNED", nb_frames=words, early_stop=es)
     ldec.set_learned(*constants)
     pdec = Decoder(code, "OMS", nb_frames=words)

@@ -18,6 +18,7 @@ OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
 FLAG_EARLY_STOP_FRAMES = 4
 FLAG_FLOODING = 8
+FLAG_EARLY_STOP_PAIRS = 16
 BATCH_GRAPH = 2
 EARLY_STOP_DEFAULT_SLACK = 128
 TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2
@@ -41,6 +42,7 @@ SIGNATURES = {
     "ldpc_decoder_info": (_I, [_P, _P]),
     "ldpc_decoder_set_learned": (_I, [_P, _I, _P, _P]),
     "ldpc_decoder_set_early_stop": (_I, [_P, _I, _I]),
+    "ldpc_decoder_status": (_I, [_P, _P]),
     "ldpc_decoder_destroy": (_I, [_P]),
     "ldpc_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I, _I, _I]),
     "ldpc_batch_decode": (_I, [_P, _P, _P, _P, _I, _I, _P, _P, _P]),

@@ -39,9 +39,6 @@ struct Plan {
     const uint8_t* rowcls;  // [m] 1 = reference's second degree group
     const int2* levels;     // [nlevels] (first r', row count)
     const int32_t* edge_orig;  // [dmax][m] edge index in table order (state dumps)
-    // [m][2] 32-byte row records (dmax <= 14): u16 columns 0..13, slot 14 unused,
-    // slot 15 = degree | class << 8; null when dmax > 14
-    const uint4* rowrec;
     // the flooding schedule: variable v's edges as message indices j * m + r' (schedule
     // order), vedge[vptr[v] .. vptr[v + 1])
     const int32_t* vptr;
@@ -76,9 +73,6 @@ struct Job {
     // KIND_LEARNED: magnitude tables [lut_its][2 row groups][128] (see packs.cuh)
     const uint16_t* lut;
     int lut_its;
-    // one-frame-per-CTA decoder: message scratch of fslots CTA slots (frame_kernel.cuh)
-    uint2* fmsg;
-    long long fslots;
 };
 
 // KIND_LEARNED: loads the tables of iteration `it` into shared memory (256 entries);
@@ -369,16 +363,23 @@ template <> struct Access<PackI8> {
 // decisions of its frames then satisfy every check.  The count goes through a
 // double-buffered shared counter, so one barrier serves both the sum and the
 // reset for the next iteration.  Uniform across the CTA.
-__device__ __forceinline__ bool odd_rows_within_slack(const Job& J, unsigned odd, int it, unsigned* s_odd)
+// The CTA's sum of `odd` in iteration it (s_odd: two words, zeroed before the first
+// iteration; each iteration clears the other's word).  Every thread of the CTA calls it.
+__device__ __forceinline__ unsigned odd_rows_total(unsigned odd, int it, unsigned* s_odd)
 {
-    // one shared atomic per warp, not per thread (every thread of the CTA is here)
+    // one shared atomic per warp, not per thread
     const unsigned lanes = __activemask();
     const unsigned w = __reduce_add_sync(lanes, odd);
     if (w && (int)(threadIdx.x & 31) == __ffs(lanes) - 1) atomicAdd(&s_odd[it & 1], w);
     __syncthreads();
     const unsigned total = s_odd[it & 1];
     if (threadIdx.x == 0) s_odd[(it + 1) & 1] = 0;
-    return total <= J.early_slack;
+    return total;
+}
+
+__device__ __forceinline__ bool odd_rows_within_slack(const Job& J, unsigned odd, int it, unsigned* s_odd)
+{
+    return odd_rows_total(odd, it, s_odd) <= J.early_slack;
 }
 
 // true in some thread when a check has odd hard-decision parity (x > 0 is bit 1)

@@ -4,14 +4,18 @@
 // The 4-frame state of a long code does not fit in one CTA's shared memory
 // (N = 64800 needs 259 KB of APP alone for 4 frames).  One frame's APP as int8 is
 // N bytes (64.8 KB), so two CTAs, two frames, fit on an SM.  The frame's E
-// messages (194 K for the rate-1/2 IRA code) go to the decoder's scratch in global
-// memory, one byte per edge, 8 bytes per check row for its edges 0-7 (and 8 more for
-// edges 8-15): the thread that updates a row reads and writes its row words
-// coalesced with the other rows of the level, a level ahead of their use, so the
-// latency hides behind the level in between.  (Two levels ahead spilled the
-// prefetched registers under the two-CTAs-per-SM register budget, and a spill waits
-// for its load.)  Per frame and iteration that is 2E
-// bytes of message traffic, the HBM-bound case of this decoder.
+// messages (194 K for the rate-1/2 IRA code) live in the decoder's scratch in global
+// memory, one byte per edge.
+//
+// Stages: the host cuts every schedule level into chunks of at most blockDim.x rows
+// (FrameStage); each thread updates at most one row of a stage.  A stage's record
+// (row words, then the rows' columns) and its messages are contiguous, 16-byte aligned
+// blocks in global memory, which the TMA engine copies (cp.async.bulk, completion on
+// an mbarrier) into a ring of FRAME_RING shared-memory slots two stages ahead of their
+// use; after a stage its updated messages go back with a bulk store from the slot.
+// So no thread waits on a global load inside the iteration loop, no register holds a
+// prefetched row, and message traffic is exactly one byte per edge (plus one per odd
+// row degree) each way per iteration.
 //
 // Early stop (ET) is per frame: the frame stops after an iteration in which at
 // most J.early_slack of its rows had odd extrinsic parity and its hard decisions
@@ -136,93 +140,80 @@ __device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const 
     return bad;
 }
 
-// The row a thread updates in one level: its record (columns, degree, class; see
-// Plan::rowrec), its index, and its c->v messages.  Records and messages do not depend
-// on the frame's APP, so they are loaded a level ahead: the record table (1 MB for
-// M = 32400) lives in L2 and the messages in the decoder's scratch in HBM.
-struct FrameRow {
-    uint4 c0, c1;
-    uint2 m0, m1;  // messages of edges 0-7 and 8-15, one byte each (see frame_row)
-    int r, end;    // row, end of its level
-    __device__ __forceinline__ int deg() const { return (c1.w >> 16) & 0xff; }
-    __device__ __forceinline__ int cls() const { return c1.w >> 24; }
-    __device__ __forceinline__ int col(int j) const  // j a compile-time constant after unrolling
-    {
-        const uint4& q = j < 8 ? c0 : c1;
-        const int k = (j & 7) >> 1;
-        const uint32_t w = k == 0 ? q.x : (k == 1 ? q.y : (k == 2 ? q.z : q.w));
-        return (j & 1) ? (int)(w >> 16) : (int)(w & 0xffff);
-    }
-    // the 32-bit word of the messages that holds edges 2p and 2p+1 (bytes 2(p&1), +1)
-    __device__ __forceinline__ uint32_t& mword(int p)
-    {
-        return p < 4 ? ((p >> 1) ? m0.y : m0.x) : ((p >> 1) & 1 ? m1.y : m1.x);
-    }
+// One stage of the schedule: at most blockDim.x rows of one level (schedule order r0..).
+// Record: rows u32 row words (edge offset of the row within the stage, even | degree << 16
+// | class << 24), padded to 16 bytes, then u16 columns, each row's padded to an even count.
+// Messages: one byte per edge slot of the record (128 - msg), the same offsets.
+struct FrameStage {
+    int rec_off;    // byte offset of the record in FrameStages::rec (16-aligned)
+    int rec_bytes;  // multiple of 16
+    int msg_off;    // byte offset of the messages in a CTA's scratch slot (16-aligned)
+    int msg_bytes;  // multiple of 16
+    int rows;
+    int cols_off;   // byte offset of the columns within the record
+    int pad0, pad1;
 };
 
-// The decoder's message scratch: one slot per resident CTA, M rows of 8 bytes for edges
-// 0-7 and, for row degrees above 8, a second array of M rows for edges 8-15.
-struct FrameMsgs {
-    uint2* lo;
-    uint2* hi;
+struct FrameStages {
+    const FrameStage* st;     // [nst], one iteration's stages in order
+    const unsigned char* rec;
+    unsigned char* msg;       // fslots scratch slots of slot_bytes, one per resident CTA
+    long long slot_bytes;
+    int nst;
+    int rec_max, msg_max;     // the ring slot layout: record area, then message area
+    int* status;              // set to 1 when a wait on the copy engine gave up
 };
 
-// Loads issued where they stand: the compiler may not move a volatile asm across the
-// level barriers, so a load issued a level ahead stays a level ahead instead of being
-// sunk next to its use to save registers.
-__device__ __forceinline__ uint4 ld_nc_v4(const uint4* p)
+constexpr int FRAME_RING = 4;
+// a wait on a bulk copy gives up after this many clock cycles (about a second)
+constexpr long long FRAME_WAIT_CYCLES = 2000000000ll;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
-    uint4 v;
-    asm volatile("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p)
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// thread-scope try_wait loop with a cycle limit; false when it gave up
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > FRAME_WAIT_CYCLES) return false;
+    }
+}
+
+// the bulk copies of stage `st` (its messages too when msgs) into ring slot `slot`,
+// completing on bar; issued by one thread
+__device__ __forceinline__ void stage_load(const FrameStages& S, const FrameStage& st, unsigned char* slot,
+                                           const unsigned char* gmsg, bool msgs, unsigned long long* bar)
+{
+    const uint32_t b = smem_u32(bar);
+    const uint32_t bytes = st.rec_bytes + (msgs ? st.msg_bytes : 0);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(slot)),
+                 "l"(S.rec + st.rec_off), "r"(st.rec_bytes), "r"(b)
                  : "memory");
-    return v;
-}
-
-__device__ __forceinline__ uint2 ld_v2(const uint2* p)
-{
-    uint2 v;
-    asm volatile("ld.global.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void load_row(const Plan& P, int r, FrameRow& x)
-{
-    x.c0 = ld_nc_v4(P.rowrec + 2 * r);
-    x.c1 = ld_nc_v4(P.rowrec + 2 * r + 1);
-}
-
-template <int DT>
-__device__ __forceinline__ void load_msgs(const FrameMsgs& M, FrameRow& x)
-{
-    x.m0 = ld_v2(M.lo + x.r);
-    if (DT > 8) x.m1 = ld_v2(M.hi + x.r);
-}
-
-template <int DT>
-__device__ __forceinline__ void store_msgs(const FrameMsgs& M, const FrameRow& x)
-{
-    // ordered with the volatile loads of the same words (a row's words are written and
-    // read back by the same thread)
-    asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(M.lo + x.r), "r"(x.m0.x), "r"(x.m0.y) : "memory");
-    if (DT > 8)
-        asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(M.hi + x.r), "r"(x.m1.x), "r"(x.m1.y) : "memory");
-}
-
-// the row of level l this thread updates first (records and, with msgs, messages)
-template <int DT>
-__device__ __forceinline__ void fetch_row(const Plan& P, const FrameMsgs& M, int l, FrameRow& x, bool msgs)
-{
-    const int2 lv = __ldg(P.levels + l);
-    x.r = lv.x + threadIdx.x;
-    x.end = lv.x + lv.y;
-    if (x.r < x.end) {
-        load_row(P, x.r, x);
-        if (msgs) load_msgs<DT>(M, x);
-    } else {
-        x.c1.w = 0;  // degree 0: no row for this thread
-    }
+    if (msgs)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(slot + S.rec_max)),
+                     "l"(gmsg + st.msg_off), "r"(st.msg_bytes), "r"(b)
+                     : "memory");
 }
 
 // f16x2 of 1152 and -1152: a message byte y = 128 + u (u the negated message, |u| <= 127)
@@ -231,8 +222,9 @@ __device__ __forceinline__ void fetch_row(const Plan& P, const FrameMsgs& M, int
 constexpr uint32_t FRAME_C1152 = 0x64806480u, FRAME_CNEG1152 = 0xe480e480u;
 
 // One check row of one frame (the reference's per-byte update, CUDA_OMS_SIMD.cu:40-134):
-// APP bytes in shared memory, this row's messages in row.m0 / row.m1 (in / out), one byte
-// per edge holding 128 - msg.  D: the row's degree (fully unrolled).
+// APP bytes in shared memory, the row's columns (cp: u32 pairs) and messages (mp: u16
+// pairs, in / out, one byte per edge holding 128 - msg) in the stage's ring slot.
+// D: the row's degree (fully unrolled).
 //
 // Two edges per 32-bit word: edges 2p and 2p+1 are the fp16 halves of pair p, in the
 // biased negated form of the F16X2 packing (b = 127 - x in [0, 255], integer-valued,
@@ -241,24 +233,27 @@ constexpr uint32_t FRAME_C1152 = 0x64806480u, FRAME_CNEG1152 = 0xe480e480u;
 // odd degree's last pair carries a dummy edge x = -127 with no message: |u| = 127
 // equals the initial min1 and min2 and its sign is positive, so it changes nothing.
 template <int KIND, int D>
-__device__ __forceinline__ void frame_row(int8_t* app, FrameRow& row, bool first, bool noclip, int& odd,
-                                          const uint16_t* lut)
+__device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint16_t* mp, bool first, bool noclip,
+                                          int& odd, const uint16_t* lut)
 {
     using namespace h2;
     constexpr int NP = (D + 1) / 2;
     uint32_t bt[NP];  // the extrinsics t = 127 - bt are recomputed where needed (registers)
+    uint32_t cw[NP];  // column pairs
     uint32_t mn1 = C127, mn2 = C127;
 #pragma unroll
+    for (int p = 0; p < NP; p++) cw[p] = cp[p];
+#pragma unroll
     for (int p = 0; p < NP; p++) {
-        const int j0 = 2 * p, j1 = 2 * p + 1;
+        const bool two = 2 * p + 1 < D;
         // bytes x of the two edges; 127 - x as an unsigned byte is x ^ 0x7f (Access<PackF16x2>::pair)
-        uint32_t w = (uint32_t)(uint8_t)app[row.col(j0)];
-        w |= (j1 < D ? (uint32_t)(uint8_t)app[row.col(j1)] : 0x81u) << 16;
+        uint32_t w = (uint32_t)(uint8_t)app[cw[p] & 0xffffu];
+        w |= (two ? (uint32_t)(uint8_t)app[cw[p] >> 16] : 0x81u) << 16;
         const uint32_t b = add((w ^ 0x007f007fu) | 0x64006400u, CNEG1024);
         uint32_t u = 0;  // negated old messages (h2 convention: t = clamp(b - u))
         if (!first) {
-            u = add(__byte_perm(row.mword(p), 0x64646464u, (p & 1) ? 0x4342 : 0x4140), FRAME_CNEG1152);
-            if (j1 >= D) u &= 0xffffu;
+            u = add(__byte_perm((uint32_t)mp[p], 0x64646464u, 0x4140), FRAME_CNEG1152);
+            if (!two) u &= 0xffffu;
         }
         bt[p] = hmin(fma_relu(u, NEG1, b), C255);
         const uint32_t ut = add(bt[p], CNEG127);
@@ -285,31 +280,29 @@ __device__ __forceinline__ void frame_row(int8_t* app, FrameRow& row, bool first
     const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
 #pragma unroll
     for (int p = 0; p < NP; p++) {
-        const int j0 = 2 * p, j1 = 2 * p + 1;
         const uint32_t ut = add(bt[p], CNEG127);
         const uint32_t fl = add_sat(habs(ut), na1);  // 0.0 on minimum edges, 1.0 elsewhere
         const uint32_t mo = fma(fl, dcs, c1s) ^ (ut & SIGN);
         const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[p]), C255), C1024) ^ 0x007f007fu;  // x bytes
-        app[row.col(j0)] = (int8_t)bn;
-        if (j1 < D) app[row.col(j1)] = (int8_t)(bn >> 16);
-        uint32_t& mw = row.mword(p);
-        mw = __byte_perm(mw, add(mo, FRAME_C1152), (p & 1) ? 0x6410 : 0x3264);
+        app[cw[p] & 0xffffu] = (int8_t)bn;
+        if (2 * p + 1 < D) app[cw[p] >> 16] = (int8_t)(bn >> 16);
+        mp[p] = (uint16_t)__byte_perm(add(mo, FRAME_C1152), 0, 0x0020);
     }
     odd += (m1 >> 15) & 1u;
 }
 
 // Dispatches a row to the unrolled update for its degree.  Rows of a level are
-// sorted by degree, so the warps of a level mostly take one case.
+// sorted by degree, so the warps of a stage mostly take one case.
 template <int KIND, int DT, bool EXACT>
-__device__ __forceinline__ void frame_row_any(int8_t* app, FrameRow& row, bool first, bool noclip, int& odd,
-                                              const uint16_t* lut)
+__device__ __forceinline__ void frame_row_any(int deg, int8_t* app, const uint32_t* cp, uint16_t* mp, bool first,
+                                              bool noclip, int& odd, const uint16_t* lut)
 {
-    if (EXACT) return frame_row<KIND, DT>(app, row, first, noclip, odd, lut);
+    if (EXACT) return frame_row<KIND, DT>(app, cp, mp, first, noclip, odd, lut);
 #define LDPC_FRAME_CASE(D)                                                                        \
     case D:                                                                                       \
-        if (D <= DT) frame_row<KIND, (D <= DT ? D : DT)>(app, row, first, noclip, odd, lut);      \
+        if (D <= DT) frame_row<KIND, (D <= DT ? D : DT)>(app, cp, mp, first, noclip, odd, lut);   \
         return;
-    switch (row.deg()) {
+    switch (deg) {
         LDPC_FRAME_CASE(1) LDPC_FRAME_CASE(2) LDPC_FRAME_CASE(3) LDPC_FRAME_CASE(4) LDPC_FRAME_CASE(5)
         LDPC_FRAME_CASE(6) LDPC_FRAME_CASE(7) LDPC_FRAME_CASE(8) LDPC_FRAME_CASE(9) LDPC_FRAME_CASE(10)
         LDPC_FRAME_CASE(11) LDPC_FRAME_CASE(12) LDPC_FRAME_CASE(13) LDPC_FRAME_CASE(14)
@@ -318,60 +311,112 @@ __device__ __forceinline__ void frame_row_any(int8_t* app, FrameRow& row, bool f
 }
 
 // Persistent CTAs: CTA c decodes frames c, c + G, c + 2G, ... of the launch (G = gridDim.x),
-// one at a time, with slot c of the message scratch (J.fmsg: J.fslots slots of P.m rows,
-// then as many again for edges 8-15 when DT > 8).  Shared memory: the frame's APP
-// (npad bytes) and, for KIND_LEARNED, the iteration's tables.
+// one at a time, with slot c of the message scratch.  Shared memory: the frame's APP
+// (npad bytes), for KIND_LEARNED the iteration's tables (512 bytes), then the ring of
+// FRAME_RING stage slots (rec_max + msg_max bytes each).
+//
+// Copy protocol (the last thread of the CTA is the producer):
+//   * stage g of the frame lives in ring slot (G0 + g) % FRAME_RING, whose mbarrier
+//     completes its phase ((G0 + g) / FRAME_RING) & 1 when the stage's bytes landed;
+//   * with at least FRAME_RING stages per iteration the producer issues stage g + 2 at
+//     the start of stage g, after cp.async.bulk.wait_group 1: every message store but
+//     stage g-1's has then completed, in particular stage g-2's (the slot being
+//     refilled) and the store of the same stage one iteration earlier (the messages
+//     being loaded); with fewer stages it issues stage g itself after wait_group 0;
+//   * every stage stores its messages back (one bulk group per stage, the last
+//     iteration included), and a frame ends with wait_group 0 and the wait for any
+//     stage it had already issued, so the next frame starts with an idle ring.
 template <int KIND, int DT, bool EXACT, bool ET>
-__global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J, long long frames)
+__global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J,
+                                                                        const FrameStages S, long long frames)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                     // [npad]
-    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad);       // KIND_LEARNED
+    int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                       // [npad]
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad);         // KIND_LEARNED
+    unsigned char* ring = smem_raw + P.npad + (KIND == KIND_LEARNED ? 512 : 0);
+    const int slot_sz = S.rec_max + S.msg_max;
+    __shared__ __align__(8) unsigned long long bars[FRAME_RING];
     __shared__ unsigned s_odd[2];
-    const FrameMsgs M = {J.fmsg + (long long)blockIdx.x * P.m, J.fmsg + (J.fslots + blockIdx.x) * (long long)P.m};
-    const int nl = P.nlevels;
-    // messages are fetched with the records one level ahead; a row's messages are written
-    // back when its level is updated, so with a single level per iteration the fetch would
-    // come before that write: such codes load them when the row is updated
-    const bool pf = nl >= 2;
+    __shared__ int s_abort;
+    const bool producer = threadIdx.x == blockDim.x - 1;
+    const unsigned char* gmsg_c = S.msg + (long long)blockIdx.x * S.slot_bytes;
+    unsigned char* gmsg = S.msg + (long long)blockIdx.x * S.slot_bytes;
+    const int nst = S.nst;
+    const int pd = nst >= FRAME_RING ? 2 : 0;  // stages issued ahead of their use
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < FRAME_RING; i++) mbar_init(&bars[i]);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned long long G0 = 0;  // stages this CTA issued before the current frame
     for (long long lf = blockIdx.x; lf < frames; lf += gridDim.x) {
         const long long f = 4 * J.word0 + lf;
+        const long long total = (long long)J.iters * nst;  // stages of the frame at most
         if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+        if (producer && pd)
+            for (int g = 0; g < pd && g < total; g++)
+                stage_load(S, S.st[g], ring + ((G0 + g) % FRAME_RING) * slot_sz, gmsg_c, false,
+                           &bars[(G0 + g) % FRAME_RING]);
+        long long issued = pd ? (total < pd ? total : pd) : 0;  // stages of this frame issued so far
         read_frame(P, J, f, [&](int v, int x) { app[v] = (int8_t)x; });
         __syncthreads();
 
-        FrameRow next;  // the row of level l+1 (cyclically)
-        fetch_row<DT>(P, M, 0, next, pf);
-        int lnext = nl > 1 ? 1 : 0;  // level fetched next
         int executed = 0;
         bool passed = false;  // stopped by the syndrome early stop: every check holds
+        long long g = 0;      // stage of the frame
         for (int it = 0; it < J.iters; it++) {
             int odd = 0;
-            const bool first = it == 0, keep = it + 1 < J.iters;  // the last iteration's messages are not needed
+            const bool first = it == 0;
             if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
-            for (int l = 0; l < nl; l++) {
-                FrameRow cur = next;
-                fetch_row<DT>(P, M, lnext, next, pf);
-                lnext = lnext + 1 == nl ? 0 : lnext + 1;
-                if (cur.r < cur.end) {
-                    if (!pf && !first) load_msgs<DT>(M, cur);
-                    const bool noclip = J.quirk && first && cur.cls();
-                    frame_row_any<KIND, DT, EXACT>(app, cur, first, noclip, odd, slut + 128 * cur.cls());
-                    if (keep) store_msgs<DT>(M, cur);
+            for (int l = 0; l < nst; l++, g++) {
+                const unsigned long long gg = G0 + g;
+                unsigned char* slot = ring + (gg % FRAME_RING) * slot_sz;
+                // every thread keeps the same count of issued stages (G0 must agree); the
+                // producer alone issues
+                if (pd) {
+                    if (g + pd < total) {
+                        const long long gn = g + pd;
+                        if (producer) {
+                            asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");
+                            stage_load(S, S.st[gn % nst], ring + ((G0 + gn) % FRAME_RING) * slot_sz, gmsg_c,
+                                       gn >= nst, &bars[(G0 + gn) % FRAME_RING]);
+                        }
+                        issued = gn + 1;
+                    }
+                } else {
+                    if (producer) {
+                        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                        stage_load(S, S.st[l], slot, gmsg_c, !first, &bars[gg % FRAME_RING]);
+                    }
+                    issued = g + 1;
                 }
-                // levels wider than the CTA: the remaining rows load their records directly
-                for (int r = cur.r + blockDim.x; r < cur.end; r += blockDim.x) {
-                    FrameRow x;
-                    x.r = r;
-                    x.end = cur.end;
-                    load_row(P, r, x);
-                    if (!first) load_msgs<DT>(M, x);
-                    const bool noclip = J.quirk && first && x.cls();
-                    frame_row_any<KIND, DT, EXACT>(app, x, first, noclip, odd, slut + 128 * x.cls());
-                    if (keep) store_msgs<DT>(M, x);
+                const FrameStage st = S.st[l];
+                if (!mbar_wait(&bars[gg % FRAME_RING], (uint32_t)((gg / FRAME_RING) & 1))) s_abort = 1;
+                const int t = threadIdx.x;
+                if (t < st.rows) {
+                    const uint32_t rw = reinterpret_cast<const uint32_t*>(slot)[t];
+                    const int off = (int)(rw & 0xffffu);  // even
+                    const uint32_t* cp = reinterpret_cast<const uint32_t*>(slot + st.cols_off) + (off >> 1);
+                    uint16_t* mp = reinterpret_cast<uint16_t*>(slot + S.rec_max) + (off >> 1);
+                    const int cls = (int)(rw >> 24);
+                    const bool noclip = J.quirk && first && cls;
+                    frame_row_any<KIND, DT, EXACT>((int)((rw >> 16) & 0xffu), app, cp, mp, first, noclip, odd,
+                                                   slut + 128 * cls);
                 }
+                // the slot's messages, written by this CTA's threads, are read next by the
+                // copy engine's store
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncthreads();
+                if (s_abort) break;
+                if (producer) {
+                    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gmsg + st.msg_off),
+                                 "r"(smem_u32(slot + S.rec_max)), "r"(st.msg_bytes)
+                                 : "memory");
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
             }
+            if (s_abort) break;
             executed = it + 1;
             if (ET) {
                 if (odd_rows_within_slack(J, (unsigned)odd, it, s_odd) &&
@@ -381,13 +426,25 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J, l
                 }
             }
         }
+        // the stages issued ahead that the frame did not use, and the message stores
+        for (long long q = g; q < issued; q++) {
+            const unsigned long long gg = G0 + q;
+            if (!mbar_wait(&bars[gg % FRAME_RING], (uint32_t)((gg / FRAME_RING) & 1))) s_abort = 1;
+        }
+        if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        G0 += issued;
+        __syncthreads();
+        if (s_abort) {
+            if (threadIdx.x == 0) atomicExch(S.status, 1);
+            return;
+        }
 
         write_frame(P, J, f, [&](int v) { return (int)app[v]; });
         if (J.iters_out && threadIdx.x == 0) J.iters_out[lf] = executed;
         if (J.synd_out) {
-            int odd = 0;
-            if (!passed) odd = __syncthreads_or(frame_rows_unsatisfied(app, P));
-            if (threadIdx.x == 0) J.synd_out[lf] = odd ? 0 : 1;
+            int bad = 0;
+            if (!passed) bad = __syncthreads_or(frame_rows_unsatisfied(app, P));
+            if (threadIdx.x == 0) J.synd_out[lf] = bad ? 0 : 1;
         }
         __syncthreads();  // the APP is refilled by the next frame
     }

@@ -1,7 +1,8 @@
 // Instantiations of the QC register-message decoder for the code shapes in use,
 // each with and without the syndrome early stop compiled in:
 //   4 frames per CTA (WPT = 2): the regular (3,6) rate-1/2 8x16 base (row degree 6,
-//     8 layers, Z a power of two), every kind and the offset-only learned kind;
+//     8 layers, Z a power of two), every kind and the offset-only learned kind, the
+//     early stop per word or per frame pair (et = 1, 2);
 //   2 frames per CTA (WPT = 1): 24-column irregular bases (802.11n-like) at rates
 //     1/2, 2/3, 3/4, 5/6, i.e. 12, 8, 6, 4 layers of row degree up to 10, 14, 18, 24,
 //     any Z.  Not for 2NMS, whose early termination is per 4-frame word;
@@ -13,8 +14,9 @@ namespace ldpc {
 
 #define LDPC_QC(KIND, D, EX, L, P2, W)                                                                  \
     if (kind == KIND && dt == D && exact == EX && layers == L && pow2 == P2 && wpt == W)                \
-        return et ? (const void*)decode_qc_kernel<KIND, D, EX, L, P2, true, W>                          \
-                  : (const void*)decode_qc_kernel<KIND, D, EX, L, P2, false, W>;
+        return et == 2 && W == 2 ? (const void*)decode_qc_kernel<KIND, D, EX, L, P2, (W == 2 ? 2 : 1), W> \
+               : et              ? (const void*)decode_qc_kernel<KIND, D, EX, L, P2, 1, W>                  \
+                                 : (const void*)decode_qc_kernel<KIND, D, EX, L, P2, 0, W>;
 #define LDPC_QC_KINDS(D, EX, L, P2)                                                                    \
     LDPC_QC(KIND_MS, D, EX, L, P2, 2) LDPC_QC(KIND_OMS, D, EX, L, P2, 2)                                \
     LDPC_QC(KIND_NMS, D, EX, L, P2, 2) LDPC_QC(KIND_2NMS, D, EX, L, P2, 2) LDPC_QC(KIND_LEARNED, D, EX, L, P2, 2) \
@@ -23,7 +25,7 @@ namespace ldpc {
     LDPC_QC(KIND_MS, D, false, L, false, 1) LDPC_QC(KIND_OMS, D, false, L, false, 1) \
     LDPC_QC(KIND_NMS, D, false, L, false, 1) LDPC_QC(KIND_LEARNED, D, false, L, false, 1)
 
-const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et, int wpt)
+const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, int et, int wpt)
 {
     LDPC_QC_KINDS(6, true, 8, true)  // regular (3,6) rate-1/2 QC, 8x16 base (Z = 2^k)
     LDPC_QC_PAIR(10, 12) LDPC_QC_PAIR(14, 8) LDPC_QC_PAIR(18, 6) LDPC_QC_PAIR(24, 4)

@@ -89,7 +89,6 @@ struct ldpc_decoder {
     int n = 0, m = 0, e = 0;
     Plan plan{};
     uint16_t* d_cols = nullptr;
-    void* d_rowrec = nullptr;
     uint8_t* d_rowdeg = nullptr;
     uint8_t* d_rowcls = nullptr;
     int2* d_levels = nullptr;
@@ -111,7 +110,13 @@ struct ldpc_decoder {
     // per-frame early stop and lane refill (persistent CTAs)
     int path = 0;
     int sms = 0;  // paths 3 and 5: multiprocessors (grid size)
-    uint2* d_fmsg = nullptr;  // path 3: message scratch, fslots CTA slots (frame_kernel.cuh)
+    // path 3 (frame_kernel.cuh): the stages of one iteration, their records, the message
+    // scratch (fslots CTA slots) and the status word the kernel sets when a copy wait gave up
+    FrameStages fst{};
+    FrameStage* d_fst = nullptr;
+    unsigned char* d_frec = nullptr;
+    unsigned char* d_fmsg = nullptr;
+    int* d_status = nullptr;
     long long fslots = 0;
     int grid_mult = 1;  // CTAs per 4-frame word
     QCParams qcp{};
@@ -319,7 +324,7 @@ namespace ldpc {
 const void* kernel_table_simd4(int kind, int variant);
 const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
-const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, bool et, int wpt);
+const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, int et, int wpt);
 const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
@@ -334,7 +339,9 @@ static size_t qc_smem(const ldpc_code* c, int wpt) { return (size_t)c->n * 4 * w
 // when an instantiation matches the code's shape, else 2 frames per CTA (*wpt = 1)
 // with the smallest instantiated row degree that holds it.  Fills q for that layout.
 // refill: the per-frame early-stop kernel with lane refill (4 frames per CTA) instead.
-static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et = false, int* wpt_out = nullptr,
+// et: 0 = no early stop, 1 = per CTA (word or, with 2 frames per CTA, frame pair), 2 = per
+// frame pair in the 4-frame kernel (LDPC_FLAG_EARLY_STOP_PAIRS)
+static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, int et = 0, int* wpt_out = nullptr,
                                  bool refill = false, bool ofs = false)
 {
     if (!c->qc || c->mb > QC_MAX_LAYERS || c->z > 256 || (long long)c->n * 8 > (1 << 20)) return nullptr;
@@ -354,14 +361,14 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool
     const bool pow2 = (c->z & (c->z - 1)) == 0;
     // KIND_* values equal LDPC_* values; ofs: the learned kind with every scale 1.0
     const int k = (kind == LDPC_XMS) ? LDPC_OMS : (ofs && kind == LDPC_LEARNED ? KIND_LEARNED_OFS : kind);
-    const bool e = et && kind != LDPC_2NMS;
+    const int e = kind != LDPC_2NMS ? et : 0;
     int wpt = 2;
     const void* f =
         refill ? kernel_table_qc_refill(k, dt, exact, c->mb, pow2) : kernel_table_qc(k, dt, exact, c->mb, pow2, e, 2);
     if (!f && !refill) {
         wpt = 1;
         for (int D : {10, 14, 18, 24})
-            if (D >= dt && (f = kernel_table_qc(k, D, false, c->mb, false, e, 1))) break;
+            if (D >= dt && (f = kernel_table_qc(k, D, false, c->mb, false, e ? 1 : 0, 1))) break;
     }
     if (!f) return nullptr;
     const int vb = 4 * wpt;  // APP bytes per variable
@@ -427,7 +434,6 @@ static void decoder_free(ldpc_decoder* d)
 {
     if (!d) return;
     cudaFree(d->d_cols);
-    cudaFree(d->d_rowrec);
     cudaFree(d->d_rowdeg);
     cudaFree(d->d_rowcls);
     cudaFree(d->d_levels);
@@ -438,6 +444,9 @@ static void decoder_free(ldpc_decoder* d)
     cudaFree(d->d_out);
     cudaFree(d->d_aux);
     cudaFree(d->d_fmsg);
+    cudaFree(d->d_fst);
+    cudaFree(d->d_frec);
+    cudaFree(d->d_status);
     cudaFree(d->d_lut);
     if (d->s_comp) cudaStreamDestroy(d->s_comp);
     if (d->s_h2d) cudaStreamDestroy(d->s_h2d);
@@ -459,15 +468,6 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
             cols[(size_t)j * m + rp] = (uint16_t)c->cols[b + j];
             eorig[(size_t)j * m + rp] = b + j;
         }
-    }
-    if (dmax <= 14) {  // row records of the one-frame-per-CTA kernel
-        std::vector<uint16_t> rec((size_t)m * 16, 0);
-        for (int rp = 0; rp < m; rp++) {
-            for (int j = 0; j < deg[rp]; j++) rec[(size_t)rp * 16 + j] = cols[(size_t)j * m + rp];
-            rec[(size_t)rp * 16 + 15] = (uint16_t)(deg[rp] | (cls[rp] << 8));
-        }
-        CUDA_TRY(cudaMalloc(&d->d_rowrec, rec.size() * sizeof(uint16_t)));
-        CUDA_TRY(cudaMemcpy(d->d_rowrec, rec.data(), rec.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
     }
     CUDA_TRY(cudaMalloc(&d->d_cols, cols.size() * sizeof(uint16_t)));
     CUDA_TRY(cudaMalloc(&d->d_edge_orig, eorig.size() * sizeof(int32_t)));
@@ -504,9 +504,67 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
     P.rowcls = d->d_rowcls;
     P.levels = d->d_levels;
     P.edge_orig = d->d_edge_orig;
-    P.rowrec = reinterpret_cast<const uint4*>(d->d_rowrec);
     P.vptr = d->d_vptr;
     P.vedge = d->d_vedge;
+    return LDPC_OK;
+}
+
+// Path 3: cuts each level of the schedule into stages of at most d->threads rows and lays
+// out their records (row words, then columns with each row padded to an even count) and
+// message offsets, 16-byte aligned for the bulk copies (FrameStage in frame_kernel.cuh).
+static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c)
+{
+    const int T = d->threads;
+    auto pad16 = [](long long x) { return (x + 15) / 16 * 16; };
+    std::vector<FrameStage> st;
+    std::vector<unsigned char> rec;
+    long long moff = 0;
+    int rec_max = 0, msg_max = 0;
+    for (const int2& lv : c->levels) {
+        for (int r0 = lv.x; r0 < lv.x + lv.y; r0 += T) {
+            const int rows = std::min(T, lv.x + lv.y - r0);
+            std::vector<uint32_t> words(rows);
+            std::vector<uint16_t> cols;
+            int off = 0;
+            for (int i = 0; i < rows; i++) {
+                const int r = c->order[r0 + i], b = c->row_ptr[r], dg = c->row_ptr[r + 1] - b;
+                words[i] = (uint32_t)off | (uint32_t)dg << 16 | (uint32_t)c->row_class[r] << 24;
+                for (int j = 0; j < dg; j++) cols.push_back((uint16_t)c->cols[b + j]);
+                if (dg & 1) cols.push_back(0);  // the dummy edge of an odd degree
+                off += dg + (dg & 1);
+            }
+            if (off > 65535) return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: %d edges in one stage", off);
+            FrameStage s{};
+            s.rows = rows;
+            s.cols_off = (int)pad16(4ll * rows);
+            s.rec_bytes = (int)(s.cols_off + pad16(2ll * off));
+            s.msg_bytes = (int)pad16(off);
+            s.rec_off = (int)rec.size();
+            s.msg_off = (int)moff;
+            rec.resize(rec.size() + s.rec_bytes, 0);
+            memcpy(rec.data() + s.rec_off, words.data(), 4 * (size_t)rows);
+            memcpy(rec.data() + s.rec_off + s.cols_off, cols.data(), 2 * (size_t)off);
+            moff += s.msg_bytes;
+            rec_max = std::max(rec_max, s.rec_bytes);
+            msg_max = std::max(msg_max, s.msg_bytes);
+            st.push_back(s);
+        }
+    }
+    if (rec.size() > (size_t)INT32_MAX || moff > INT32_MAX)
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: stage records too large");
+    CUDA_TRY(cudaMalloc(&d->d_fst, st.size() * sizeof(FrameStage)));
+    CUDA_TRY(cudaMalloc(&d->d_frec, rec.size()));
+    CUDA_TRY(cudaMalloc(&d->d_status, sizeof(int)));
+    CUDA_TRY(cudaMemcpy(d->d_fst, st.data(), st.size() * sizeof(FrameStage), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d->d_frec, rec.data(), rec.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(d->d_status, 0, sizeof(int)));
+    d->fst.st = d->d_fst;
+    d->fst.rec = d->d_frec;
+    d->fst.slot_bytes = moff;
+    d->fst.nst = (int)st.size();
+    d->fst.rec_max = rec_max;
+    d->fst.msg_max = msg_max;
+    d->fst.status = d->d_status;
     return LDPC_OK;
 }
 
@@ -516,14 +574,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     if (!out || !c) return fail(LDPC_ERR_ARG, "ldpc_decoder_create: null pointer");
     if (kind < LDPC_MS || kind > LDPC_LEARNED) return fail(LDPC_ERR_ARG, "unknown decoder kind %d", kind);
     if (nb_frames < 1) return fail(LDPC_ERR_SHAPE, "nb_frames must be >= 1");
-    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES | LDPC_FLAG_FLOODING))
+    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES | LDPC_FLAG_FLOODING | LDPC_FLAG_EARLY_STOP_PAIRS))
         return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
     const bool per_frame = flags & LDPC_FLAG_EARLY_STOP_FRAMES;
+    const bool pairs = flags & LDPC_FLAG_EARLY_STOP_PAIRS;
     const bool flood = flags & LDPC_FLAG_FLOODING;
-    if (flood && (per_frame || (pack != LDPC_PACK_AUTO && pack != LDPC_PACK_F16X2)))
+    if (pairs && per_frame)
+        return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP_PAIRS and LDPC_FLAG_EARLY_STOP_FRAMES exclude each other");
+    if (flood && (per_frame || pairs || (pack != LDPC_PACK_AUTO && pack != LDPC_PACK_F16X2)))
         return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_FLOODING: the flooding schedule runs on the 4-frame "
                                           "LDPC_PACK_F16X2 level kernel, per-word early stop only");
-    const bool early = (flags & LDPC_FLAG_EARLY_STOP) || per_frame;
+    const bool early = (flags & LDPC_FLAG_EARLY_STOP) || per_frame || pairs;
+    const int etm = pairs ? 2 : 1;  // the QC kernels' early-stop mode when early
     if (early && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     const int pack_req = pack;
@@ -588,7 +650,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     }
     int qc_wpt = 2;
     const void* qk = !frame && !flood && (pack_req == LDPC_PACK_AUTO || pack_req == LDPC_PACK_F16X2)
-                         ? qc_kernel_for(c, kind, d->qcp, early, &qc_wpt)
+                         ? qc_kernel_for(c, kind, d->qcp, early ? etm : 0, &qc_wpt)
                          : nullptr;
     if (qc_wpt == 1 && pack_req != LDPC_PACK_F16X2) qk = nullptr;
     if (frame) {
@@ -598,8 +660,18 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->path = 3;
         d->pack = LDPC_PACK_FRAME;
         d->grid_mult = 4;
-        d->smem = (int)frame_smem;
         d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32));
+        rc = frame_stages_setup(d, c);
+        if (rc) {
+            decoder_free(d);
+            return rc;
+        }
+        d->smem = (int)(frame_smem + (size_t)FRAME_RING * (d->fst.rec_max + d->fst.msg_max));
+        if (d->smem > smem_max) {
+            decoder_free(d);
+            return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: the frame and its stage ring need %d B of shared "
+                                              "memory (> %d)", d->smem, smem_max);
+        }
     } else if (per_frame && qk && qc_wpt == 2 && qc_smem(c, 2) + QC_STAGE * (size_t)c->n <= (size_t)smem_max &&
                (d->kfn = qc_kernel_for(c, kind, d->qcp, true, nullptr, true))) {
         d->path = 5;
@@ -609,10 +681,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     } else if (qk && qc_smem(c, qc_wpt) + lut_smem <= (size_t)smem_max) {
         QCParams alt;
         d->kfn = qk;
-        d->kfn_alt = qc_kernel_for(c, kind, alt, !early);  // for ldpc_decoder_set_early_stop (same layout)
+        d->kfn_alt = qc_kernel_for(c, kind, alt, early ? 0 : etm);  // for ldpc_decoder_set_early_stop (same layout)
         if (kind == LDPC_LEARNED && qc_wpt == 2)
             for (int o = 0; o < 2; o++)
-                for (int e = 0; e < 2; e++) d->kfn_lrn[o][e] = qc_kernel_for(c, kind, alt, e != 0, nullptr, false, o != 0);
+                for (int e = 0; e < 2; e++)
+                    d->kfn_lrn[o][e] = qc_kernel_for(c, kind, alt, e != 0 ? etm : 0, nullptr, false, o != 0);
         d->path = qc_wpt == 2 ? 1 : 4;
         d->grid_mult = qc_wpt == 2 ? 1 : 2;
         d->pack = LDPC_PACK_F16X2;
@@ -634,6 +707,10 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->kfn = kernel_for(pack, kind, degree_variant(c));
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
+    }
+    if (pairs && d->path != 1 && d->path != 4) {
+        decoder_free(d);
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_PAIRS: needs a QC register kernel (decoder path 1 or 4)");
     }
     if (per_frame && d->path != 3 && d->path != 5) {
         decoder_free(d);
@@ -666,11 +743,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         return fail(LDPC_ERR_UNSUPPORTED, "kernel cannot be resident (smem %d B, %d threads)", d->smem, d->threads);
     }
     if (d->path == 3) {
-        // one message slot per resident CTA: 8 bytes per check row for edges 0-7, and as many
-        // again for edges 8-15 when a row has more than 8
+        // one message slot per resident CTA: a byte per edge slot of the stage records
         d->fslots = (long long)d->ctas_per_sm * d->sms;
-        const size_t bytes = (size_t)d->fslots * d->m * sizeof(uint2) * (c->dmax > 8 ? 2 : 1);
+        const size_t bytes = (size_t)d->fslots * (size_t)d->fst.slot_bytes;
         cudaError_t ea = cudaMalloc(&d->d_fmsg, bytes);
+        d->fst.msg = d->d_fmsg;
         if (ea != cudaSuccess) {
             decoder_free(d);
             return fail(ea == cudaErrorMemoryAllocation ? LDPC_ERR_NOMEM : LDPC_ERR_CUDA,
@@ -833,10 +910,8 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     if (d->path == 3) {
         // persistent CTAs, one message-scratch slot each
         long long frames = 4 * words;
-        J.fmsg = d->d_fmsg;
-        J.fslots = d->fslots;
         const long long grid = std::min(frames, d->fslots);
-        void* a[] = {(void*)&d->plan, (void*)&J, (void*)&frames};
+        void* a[] = {(void*)&d->plan, (void*)&J, (void*)&d->fst, (void*)&frames};
         CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
         return LDPC_OK;
     }
@@ -966,6 +1041,21 @@ static int decode_host_impl(ldpc_decoder* d, const int8_t* llr, void* out, int i
     for (auto ev : ev_in) cudaEventDestroy(ev);
     for (auto ev : ev_dec) cudaEventDestroy(ev);
     if (e != cudaSuccess) return fail(LDPC_ERR_CUDA, "decode_host: %s", cudaGetErrorString(e));
+    int status = 0;
+    rc = ldpc_decoder_status(d, &status);
+    if (rc) return rc;
+    if (status) return fail(LDPC_ERR_CUDA, "decode_host: a wait on the copy engine gave up (results invalid)");
+    return LDPC_OK;
+}
+
+extern "C" int ldpc_decoder_status(ldpc_decoder* d, int* status)
+{
+    if (!d || !status) return fail(LDPC_ERR_ARG, "ldpc_decoder_status: null pointer");
+    *status = 0;
+    if (!d->d_status) return LDPC_OK;
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaMemcpy(status, d->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (*status) CUDA_TRY(cudaMemset(d->d_status, 0, sizeof(int)));
     return LDPC_OK;
 }
 

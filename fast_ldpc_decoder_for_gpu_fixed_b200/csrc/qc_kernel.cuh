@@ -116,11 +116,16 @@ __device__ __noinline__ unsigned qc_rows_unsat_mask(const QCParams& Q, const cha
     return ((bad0 >> 15) & 1u) | ((bad0 >> 30) & 2u) | ((bad1 >> 13) & 4u) | ((bad1 >> 28) & 8u);
 }
 
-// ET: the syndrome early stop compiled in (J.early is then always set); without
-// it the extrinsic-parity count is dead code for every kind but 2NMS
-template <int KIND, int DT, bool EXACT, int L, bool POW2, bool ET, int WPT>
+// ET: the syndrome early stop compiled in (J.early is then always set): 1 = the CTA's
+// frames stop together, 2 (WPT = 2 only) = each frame pair (frames 0, 1 and 2, 3 of the
+// word) stops on its own: a stopped pair's rows are no longer updated and its APP stays
+// as it was, and the word reports the larger of its pairs' counts.  Without it the
+// extrinsic-parity count is dead code for every kind but 2NMS.
+template <int KIND, int DT, bool EXACT, int L, bool POW2, int ET, int WPT>
 __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const __grid_constant__ QCParams Q, const Job J)
 {
+    static_assert(ET != 2 || WPT == 2, "per-pair early stop: 4 frames per CTA");
+    constexpr bool PAIRS = ET == 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* app = reinterpret_cast<uint2*>(smem_raw);     // WPT = 2: [n] (pair-word 0, pair-word 1)
     uint32_t* app1 = reinterpret_cast<uint32_t*>(smem_raw);  // WPT = 1: [n] pair-word of frames 2h, 2h+1
@@ -164,8 +169,9 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
 
     int executed = 0;
     bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
+    unsigned live = 3;    // PAIRS: bit p set while pair p is decoding (the same in every thread)
     for (int it = 0; it < J.iters; it++) {
-        uint32_t ov = 0;
+        uint32_t ov = 0, ov1 = 0;  // PAIRS: ov1 is pair 1's odd-row accumulator
         const int lt = LRN ? min(it, J.lut_its - 1) : 0;  // constants of this iteration
 #pragma unroll
         for (int l = 0; l < L; l++) {
@@ -197,8 +203,10 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                 lk = kb.x;
                 lb = kb.y;
             }
-            h2::row<KIND, DT, EXACT, CM>(b0, msg[0][l], d, noclip, ov, lk, lb);
-            if (WPT == 2) h2::row<KIND, DT, EXACT, CM>(b1, msg[WPT - 1][l], d, noclip, ov, lk, lb);
+            // a stopped pair's words are stored back unchanged
+            if (!PAIRS || (live & 1u)) h2::row<KIND, DT, EXACT, CM>(b0, msg[0][l], d, noclip, ov, lk, lb);
+            if (WPT == 2 && (!PAIRS || (live & 2u)))
+                h2::row<KIND, DT, EXACT, CM>(b1, msg[WPT - 1][l], d, noclip, PAIRS ? ov1 : ov, lk, lb);
 #pragma unroll
             for (int j = 0; j < DT; j++) {
                 if (EXACT || j < d) {
@@ -219,7 +227,28 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
         // every layer.  For a biased APP b (x = 127 - b, an fp16 in [0, 255]),
         // b - 126.5 is negative iff the hard decision is 1 (qc_one_signs); a row is
         // satisfied when its count of 1s is even.
-        if (KIND != KIND_2NMS && ET) {
+        if (KIND != KIND_2NMS && PAIRS) {
+            // both pairs' counts in one word (each at most 2 * L * 256 < 2^16)
+            const unsigned tot = odd_rows_total(h2::odd_count(ov, L) | (h2::odd_count(ov1, L) << 16), it, s_odd);
+            unsigned gate = live & (((tot & 0xffffu) <= J.early_slack ? 1u : 0u) | ((tot >> 16) <= J.early_slack ? 2u : 0u));
+            if (gate) {
+                // staged as below; bit p of a thread's mask: pair p has an odd row among its rows k
+                constexpr int LS = L > 2 ? 2 : L;
+                unsigned m = qc_rows_unsat_mask<DT, EXACT, 0, LS, POW2, 2>(Q, appb, k);
+                if ((gate & 1u) && __syncthreads_or(m & 3u)) gate &= ~1u;
+                if ((gate & 2u) && __syncthreads_or(m & 12u)) gate &= ~2u;
+                if (LS < L && gate) {
+                    m = qc_rows_unsat_mask<DT, EXACT, LS, L, POW2, 2>(Q, appb, k);
+                    if ((gate & 1u) && __syncthreads_or(m & 3u)) gate &= ~1u;
+                    if ((gate & 2u) && __syncthreads_or(m & 12u)) gate &= ~2u;
+                }
+                live &= ~gate;  // the pairs whose frames are codewords stop here
+                if (!live) {
+                    passed = true;
+                    break;
+                }
+            }
+        } else if (KIND != KIND_2NMS && ET) {
             if (odd_rows_within_slack(J, h2::odd_count(ov, L * WPT), it, s_odd)) {
                 // staged: the first layers alone reject most words that are not codewords yet
                 constexpr int LS = L > 2 ? 2 : L;

@@ -77,7 +77,9 @@ class Decoder:
     lanes (4*nb_frames codewords per call), ``pack`` in AUTO/SIMD4/F16X2/I8;
     ``early_stop`` sets LDPC_FLAG_EARLY_STOP (syndrome early stop per word), or with
     ``early_stop="frame"`` LDPC_FLAG_EARLY_STOP_FRAMES (per frame, finished frames'
-    slots refilled; iteration counts per frame); ``flooding`` sets LDPC_FLAG_FLOODING."""
+    slots refilled; iteration counts per frame), ``early_stop="pairs"``
+    LDPC_FLAG_EARLY_STOP_PAIRS (each frame pair of a word on its own); ``flooding`` sets
+    LDPC_FLAG_FLOODING."""
 
     def __init__(self, code, kind="OMS", nb_frames=1024, pack="AUTO", early_stop=False, flooding=False):
         if isinstance(code, str):
@@ -87,7 +89,12 @@ class Decoder:
         self.kind = kind.upper()
         self.nb_frames = int(nb_frames)
         h = ctypes.c_void_p()
-        flags = _lib.FLAG_EARLY_STOP_FRAMES if early_stop == "frame" else (_lib.FLAG_EARLY_STOP if early_stop else 0)
+        if early_stop == "frame":
+            flags = _lib.FLAG_EARLY_STOP_FRAMES
+        elif early_stop == "pairs":
+            flags = _lib.FLAG_EARLY_STOP_PAIRS
+        else:
+            flags = _lib.FLAG_EARLY_STOP if early_stop else 0
         if flooding:
             flags |= _lib.FLAG_FLOODING
         _lib.check(_lib.lib().ldpc_decoder_create(
@@ -96,6 +103,7 @@ class Decoder:
         self.handle = h
         self.early_stop = bool(early_stop)
         self.per_frame = early_stop == "frame"
+        self.pairs = early_stop == "pairs"
         self.early_slack = _lib.EARLY_STOP_DEFAULT_SLACK
 
     def info(self):
@@ -109,6 +117,13 @@ class Decoder:
         _lib.check(_lib.lib().ldpc_decoder_set_early_stop(self.handle, int(bool(enabled)), int(slack)))
         self.early_stop = bool(enabled)
         self.early_slack = int(slack)
+
+    def status(self):
+        """1 when a kernel of this decoder gave up waiting on a bulk copy since the last
+        call (ldpc_decoder_status), else 0."""
+        st = ctypes.c_int(0)
+        _lib.check(_lib.lib().ldpc_decoder_status(self.handle, ctypes.byref(st)))
+        return st.value
 
     def set_learned(self, offsets, scales):
         """LDPC_LEARNED constants: [n_iters][2] int8 offsets and uint8 Q1.7 scales."""
@@ -238,6 +253,13 @@ class Batch:
         """The strategy by hand (ldpc_batch_configure)."""
         _lib.check(_lib.lib().ldpc_batch_configure(self.handle, int(bool(per_code)), _lib.PACKS[pack.upper()],
                                                    int(threads), int(ctas_per_sm)))
+
+    def status(self):
+        """1 when a kernel of this decoder gave up waiting on a bulk copy since the last
+        call (ldpc_decoder_status), else 0."""
+        st = ctypes.c_int(0)
+        _lib.check(_lib.lib().ldpc_decoder_status(self.handle, ctypes.byref(st)))
+        return st.value
 
     def set_learned(self, offsets, scales):
         off = np.ascontiguousarray(offsets, dtype=np.int8).reshape(-1, 2)

@@ -71,9 +71,10 @@ extern "C" {
 #define LDPC_PACK_F16X2 1
 #define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
 /* 1 frame per CTA: the frame's APP as int8 in shared memory (N bytes, two CTAs per
- * SM at N = 64800) and its c->v messages, one byte per edge, in a message scratch
- * the decoder allocates in device memory (8 bytes per check row and resident CTA,
- * 16 when a row has more than 8 edges: 153 MB for N = 64800 rate 1/2 on 148 SMs).
+ * SM at N = 64800) and its c->v messages, one byte per edge (plus one per odd row
+ * degree), in a message scratch the decoder allocates in device memory, one slot per
+ * resident CTA (about 64 MB for N = 64800 rate 1/2 on 148 SMs); row records and
+ * messages reach shared memory by bulk copies a stage ahead of their use.
  * For long codes whose 4-frame state exceeds shared memory.  Row degree <= 14.
  * LDPC_PACK_AUTO falls back to it when nothing else fits.  Not for LDPC_2NMS
  * (whose early termination is per 4-frame word).  With LDPC_FLAG_EARLY_STOP each
@@ -157,12 +158,22 @@ void ldpc_code_destroy(ldpc_code* code);
  * states the same schedule (oracle_set_schedule). */
 #define LDPC_FLAG_FLOODING 8
 
+/* Per-pair early stop (implies LDPC_FLAG_EARLY_STOP): the rule above applied to each
+ * frame pair of a word (frames 4g, 4g+1 and 4g+2, 4g+3: their own odd rows against
+ * `slack`, their own syndrome).  A stopped pair keeps its decisions while the other pair
+ * of the word goes on; d_iters_out receives per word the larger of its pairs' counts.
+ * Decoder path 1 (the 4-frame QC register kernel) and path 4 (whose early stop is per
+ * pair anyway); other decoders fail with LDPC_ERR_UNSUPPORTED.  Not with
+ * LDPC_FLAG_EARLY_STOP_FRAMES or LDPC_FLAG_FLOODING. */
+#define LDPC_FLAG_EARLY_STOP_PAIRS 16
+
 /* nb_frames counts 32-bit lanes like the reference's constructor argument:
  * a decoder serves up to 4*nb_frames codewords per call (src/main.cpp:309).
  * Unlike the reference (decoder_oms/CGPU_Decoder_OMS_SIMD.cu:101-105), any
  * nb_frames >= 1 is accepted.  The decoder owns its device buffers; the code
  * may be destroyed after this call.  pack = LDPC_PACK_*; flags = 0 or
- * LDPC_FLAG_EARLY_STOP, LDPC_FLAG_EARLY_STOP_FRAMES. */
+ * LDPC_FLAG_EARLY_STOP, LDPC_FLAG_EARLY_STOP_FRAMES, LDPC_FLAG_EARLY_STOP_PAIRS,
+ * LDPC_FLAG_FLOODING. */
 int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* code, int kind, size_t nb_frames,
                         int pack, int flags);
 
@@ -299,6 +310,14 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
+
+/* Kernel status of a decoder (no reference counterpart): *status = 1 when a kernel of
+ * this decoder gave up waiting on a bulk copy since the last call (its frames' results
+ * are then invalid), else 0; reading clears it.  Only the one-frame-per-CTA path
+ * (LDPC_PACK_FRAME) waits on copies.  Call it after the decodes it should cover have
+ * completed (for example after synchronizing their stream); ldpc_decode_host and
+ * ldpc_decode_host_ex check it themselves and fail with LDPC_ERR_CUDA. */
+int ldpc_decoder_status(ldpc_decoder* dec, int* status);
 
 /* ---- batches of codes (no reference counterpart) ------------------------ */
 

@@ -155,3 +155,55 @@ def test_reference_long_table(cuda):
     dec.close()
     hard, _ = _decode(code, "OMS", llr, 3, words)
     assert np.array_equal(hard, ref["hard"])
+
+
+def _small_code(name, rows, n, seed):
+    """A code whose rows are the given column lists (layer order)."""
+    from fast_ldpc_decoder_for_gpu_fixed_b200.codes import Code
+    ptr = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    return Code(name, n, ptr, np.concatenate(rows).astype(np.int32))
+
+
+@pytest.mark.parametrize("shape", ["one_level", "three_levels", "split_level"])
+def test_frame_few_stages(cuda, shape):
+    """Schedules of fewer than four stages (each stage issued when it starts, no copy
+    ahead) and a level wider than the CTA (cut into stages of at most 512 rows)."""
+    rng = np.random.default_rng(5)
+    if shape == "one_level":      # 12 disjoint rows of degree 5..7: one level, one stage
+        n, rows, start = 96, [], 0
+        for d in rng.integers(5, 8, size=12):
+            rows.append(np.arange(start, start + d))
+            start += d
+    elif shape == "three_levels":  # a chain: row i shares a variable with row i-1
+        n = 64
+        rows = [np.array([0, 1, 2, 3, 4, 5]), np.array([5, 6, 7, 8, 9, 10, 11]), np.array([11, 12, 13, 14, 15])]
+    else:                          # 1000 disjoint rows of degree 3 and 4: one level of 1000 rows
+        degs = rng.integers(3, 5, size=1000)
+        n = int(degs.sum()) + 8
+        rows, start = [], 0
+        for d in degs:
+            rows.append(rng.permutation(np.arange(start, start + d)))
+            start += d
+    code = _small_code(shape, rows, n, 5)
+    words = 8
+    llr = make_llr("uniform", 4 * words * code.n, 23)
+    for kind in ("OMS", "NMS"):
+        ref = oracle.decode(code, kind, llr, 6)
+        hard, its = _decode(code, kind, llr, 6, words)
+        assert np.array_equal(hard, ref["hard"])
+        assert (its == 6).all()
+
+
+def test_frame_many_frames_per_cta(cuda):
+    """More frames than resident CTAs (each persistent CTA decodes several frames in a
+    row, the copies it issued ahead for a frame that stopped early are drained first),
+    mixed noise so that frames stop at many different iterations."""
+    code = load_table("576x288")
+    words = 240  # 960 frames, about three per CTA
+    llr = np.concatenate([make_llr("awgn", 4 * 80 * code.n, 29 + i, sigma=llr_gen.sigma_for(e, 0.5))
+                          for i, e in enumerate((1.0, 2.5, 4.0))])
+    ref = oracle.decode(code, "OMS", llr, 20, early_stop=True, per_frame=True)
+    hard, its = _decode(code, "OMS", llr, 20, words, early=True)
+    assert np.array_equal(its, ref["iters"])
+    assert np.array_equal(hard, ref["hard"])
+    assert len(set(its.tolist())) > 5
