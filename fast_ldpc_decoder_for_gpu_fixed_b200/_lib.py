@@ -13,7 +13,7 @@ LDPC_OK = 0
 ERRORS = {-1: "LDPC_ERR_ARG", -2: "LDPC_ERR_CUDA", -3: "LDPC_ERR_UNSUPPORTED", -4: "LDPC_ERR_NOMEM",
           -5: "LDPC_ERR_SHAPE"}
 KINDS = {"MS": 0, "FMS": 0, "OMS": 1, "NMS": 2, "2NMS": 3, "XMS": 4, "LEARNED": 5}
-PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2, "FRAME": 3}
+PACKS = {"AUTO": -1, "SIMD4": 0, "F16X2": 1, "I8": 2, "FRAME": 3, "F16X2_SPLIT": 4}
 OUT_BYTES, OUT_PACKED = 0, 1
 FLAG_EARLY_STOP = 1
 FLAG_EARLY_STOP_FRAMES = 4

@@ -25,7 +25,7 @@
 
 namespace ldpc {
 
-constexpr int FRAME_MAX_THREADS = 512;
+constexpr int FRAME_MAX_THREADS = 512;  // rows of a stage at most; the CTA adds one producer warp
 constexpr int FRAME_MAX_DEGREE = 14;
 
 // Reads frame f (batch index) and calls put(v, x) with its int8 LLR of variable v.
@@ -82,7 +82,7 @@ __device__ __forceinline__ void write_frame(const Plan& P, const Job& J, long lo
     const int n = P.n;
     const long long lf = f - 4 * J.word0;
     if (J.counts) {
-        __shared__ int part[FRAME_MAX_THREADS / 32];
+        __shared__ int part[FRAME_MAX_THREADS / 32 + 1];
         int e = 0;
         const uint8_t* cw = J.cw ? J.cw + ((unsigned long long)f % (unsigned long long)J.n_cw) * n : nullptr;
         for (int v = threadIdx.x; v < J.n_vars; v += blockDim.x) e += (x(v) > 0) != (cw ? cw[v] != 0 : false);
@@ -140,19 +140,24 @@ __device__ __forceinline__ bool frame_rows_unsatisfied(const int8_t* app, const 
     return bad;
 }
 
-// One stage of the schedule: at most blockDim.x rows of one level (schedule order r0..).
-// Record: rows u32 row words (edge offset of the row within the stage, even | degree << 16
-// | class << 24), padded to 16 bytes, then u16 columns, each row's padded to an even count.
-// Messages: one byte per edge slot of the record (128 - msg), the same offsets.
+// One stage of the schedule: at most blockDim.x rows of one level (consecutive rows of the
+// level, whose rows are sorted by decreasing degree).  Record (copied to shared memory):
+//   a 32-byte header: word 0 = rows, word 1 = the record's bytes (where the stage's messages
+//     follow it in the ring slot); bytes 16..31 = pair-slot offsets poff[0..7] (u16, in
+//     pairs): pair slot p holds pair p (edges 2p, 2p+1) of every row of degree > 2p, the
+//     stage's row t at poff[p] + t;
+//   the row words, u32 per row (degree | class << 8), padded to 16 bytes;
+//   the column pairs, u32 per pair slot entry (column of edge 2p | column of edge 2p+1 << 16).
+// Messages: one u16 per pair slot entry (the two edges' bytes 128 - msg), same indexing.
+// Rows t of a warp read consecutive words of each pair slot: no bank conflicts.
 struct FrameStage {
     int rec_off;    // byte offset of the record in FrameStages::rec (16-aligned)
     int rec_bytes;  // multiple of 16
     int msg_off;    // byte offset of the messages in a CTA's scratch slot (16-aligned)
     int msg_bytes;  // multiple of 16
-    int rows;
-    int cols_off;   // byte offset of the columns within the record
-    int pad0, pad1;
 };
+
+constexpr int FRAME_STAGE_HEADER = 32;
 
 struct FrameStages {
     const FrameStage* st;     // [nst], one iteration's stages in order
@@ -160,7 +165,7 @@ struct FrameStages {
     unsigned char* msg;       // fslots scratch slots of slot_bytes, one per resident CTA
     long long slot_bytes;
     int nst;
-    int rec_max, msg_max;     // the ring slot layout: record area, then message area
+    int slot_sz;              // bytes of a ring slot: the largest record plus its messages
     int* status;              // set to 1 when a wait on the copy engine gave up
 };
 
@@ -211,7 +216,7 @@ __device__ __forceinline__ void stage_load(const FrameStages& S, const FrameStag
                  : "memory");
     if (msgs)
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_u32(slot + S.rec_max)),
+                         smem_u32(slot + st.rec_bytes)),
                      "l"(gmsg + st.msg_off), "r"(st.msg_bytes), "r"(b)
                      : "memory");
 }
@@ -233,16 +238,21 @@ constexpr uint32_t FRAME_C1152 = 0x64806480u, FRAME_CNEG1152 = 0xe480e480u;
 // odd degree's last pair carries a dummy edge x = -127 with no message: |u| = 127
 // equals the initial min1 and min2 and its sign is positive, so it changes nothing.
 template <int KIND, int D>
-__device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint16_t* mp, bool first, bool noclip,
-                                          int& odd, const uint16_t* lut)
+__device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint16_t* mp, const uint4& po, bool first,
+                                          bool noclip, int& odd, const uint16_t* lut)
 {
     using namespace h2;
     constexpr int NP = (D + 1) / 2;
     uint32_t bt[NP];  // the extrinsics t = 127 - bt are recomputed where needed (registers)
     uint32_t cw[NP];  // column pairs
+    int pi[NP];       // this row's entry of each pair slot
     uint32_t mn1 = C127, mn2 = C127;
 #pragma unroll
-    for (int p = 0; p < NP; p++) cw[p] = cp[p];
+    for (int p = 0; p < NP; p++) {
+        const uint32_t w = p < 2 ? po.x : (p < 4 ? po.y : (p < 6 ? po.z : po.w));
+        pi[p] = (int)((p & 1) ? (w >> 16) : (w & 0xffffu));
+        cw[p] = cp[pi[p]];
+    }
 #pragma unroll
     for (int p = 0; p < NP; p++) {
         const bool two = 2 * p + 1 < D;
@@ -252,7 +262,7 @@ __device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint1
         const uint32_t b = add((w ^ 0x007f007fu) | 0x64006400u, CNEG1024);
         uint32_t u = 0;  // negated old messages (h2 convention: t = clamp(b - u))
         if (!first) {
-            u = add(__byte_perm((uint32_t)mp[p], 0x64646464u, 0x4140), FRAME_CNEG1152);
+            u = add(__byte_perm((uint32_t)mp[pi[p]], 0x64646464u, 0x4140), FRAME_CNEG1152);
             if (!two) u &= 0xffffu;
         }
         bt[p] = hmin(fma_relu(u, NEG1, b), C255);
@@ -286,7 +296,7 @@ __device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint1
         const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[p]), C255), C1024) ^ 0x007f007fu;  // x bytes
         app[cw[p] & 0xffffu] = (int8_t)bn;
         if (2 * p + 1 < D) app[cw[p] >> 16] = (int8_t)(bn >> 16);
-        mp[p] = (uint16_t)__byte_perm(add(mo, FRAME_C1152), 0, 0x0020);
+        mp[pi[p]] = (uint16_t)__byte_perm(add(mo, FRAME_C1152), 0, 0x0020);
     }
     odd += (m1 >> 15) & 1u;
 }
@@ -294,13 +304,13 @@ __device__ __forceinline__ void frame_row(int8_t* app, const uint32_t* cp, uint1
 // Dispatches a row to the unrolled update for its degree.  Rows of a level are
 // sorted by degree, so the warps of a stage mostly take one case.
 template <int KIND, int DT, bool EXACT>
-__device__ __forceinline__ void frame_row_any(int deg, int8_t* app, const uint32_t* cp, uint16_t* mp, bool first,
-                                              bool noclip, int& odd, const uint16_t* lut)
+__device__ __forceinline__ void frame_row_any(int deg, int8_t* app, const uint32_t* cp, uint16_t* mp, const uint4& po,
+                                              bool first, bool noclip, int& odd, const uint16_t* lut)
 {
-    if (EXACT) return frame_row<KIND, DT>(app, cp, mp, first, noclip, odd, lut);
-#define LDPC_FRAME_CASE(D)                                                                        \
-    case D:                                                                                       \
-        if (D <= DT) frame_row<KIND, (D <= DT ? D : DT)>(app, cp, mp, first, noclip, odd, lut);   \
+    if (EXACT) return frame_row<KIND, DT>(app, cp, mp, po, first, noclip, odd, lut);
+#define LDPC_FRAME_CASE(D)                                                                            \
+    case D:                                                                                           \
+        if (D <= DT) frame_row<KIND, (D <= DT ? D : DT)>(app, cp, mp, po, first, noclip, odd, lut);   \
         return;
     switch (deg) {
         LDPC_FRAME_CASE(1) LDPC_FRAME_CASE(2) LDPC_FRAME_CASE(3) LDPC_FRAME_CASE(4) LDPC_FRAME_CASE(5)
@@ -313,9 +323,10 @@ __device__ __forceinline__ void frame_row_any(int deg, int8_t* app, const uint32
 // Persistent CTAs: CTA c decodes frames c, c + G, c + 2G, ... of the launch (G = gridDim.x),
 // one at a time, with slot c of the message scratch.  Shared memory: the frame's APP
 // (npad bytes), for KIND_LEARNED the iteration's tables (512 bytes), then the ring of
-// FRAME_RING stage slots (rec_max + msg_max bytes each).
+// FRAME_RING stage slots (S.slot_sz bytes each).
 //
-// Copy protocol (the last thread of the CTA is the producer):
+// Copy protocol (the last thread of the CTA, in a warp of its own after the rows' warps, is
+// the producer):
 //   * stage g of the frame lives in ring slot (G0 + g) % FRAME_RING, whose mbarrier
 //     completes its phase ((G0 + g) / FRAME_RING) & 1 when the stage's bytes landed;
 //   * with at least FRAME_RING stages per iteration the producer issues stage g + 2 at
@@ -334,7 +345,7 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J,
     int8_t* app = reinterpret_cast<int8_t*>(smem_raw);                       // [npad]
     uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + P.npad);         // KIND_LEARNED
     unsigned char* ring = smem_raw + P.npad + (KIND == KIND_LEARNED ? 512 : 0);
-    const int slot_sz = S.rec_max + S.msg_max;
+    const int slot_sz = S.slot_sz;
     __shared__ __align__(8) unsigned long long bars[FRAME_RING];
     __shared__ unsigned s_odd[2];
     __shared__ int s_abort;
@@ -391,17 +402,19 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J,
                     }
                     issued = g + 1;
                 }
-                const FrameStage st = S.st[l];
                 if (!mbar_wait(&bars[gg % FRAME_RING], (uint32_t)((gg / FRAME_RING) & 1))) s_abort = 1;
                 const int t = threadIdx.x;
-                if (t < st.rows) {
-                    const uint32_t rw = reinterpret_cast<const uint32_t*>(slot)[t];
-                    const int off = (int)(rw & 0xffffu);  // even
-                    const uint32_t* cp = reinterpret_cast<const uint32_t*>(slot + st.cols_off) + (off >> 1);
-                    uint16_t* mp = reinterpret_cast<uint16_t*>(slot + S.rec_max) + (off >> 1);
-                    const int cls = (int)(rw >> 24);
+                const int2 hd = *reinterpret_cast<const int2*>(slot);  // rows, record bytes
+                const int rows = hd.x;
+                if (t < rows) {
+                    const uint4 po = reinterpret_cast<const uint4*>(slot)[1];  // pair-slot offsets
+                    const uint32_t rw = reinterpret_cast<const uint32_t*>(slot + FRAME_STAGE_HEADER)[t];
+                    const int cols_off = FRAME_STAGE_HEADER + (4 * rows + 15) / 16 * 16;
+                    const uint32_t* cp = reinterpret_cast<const uint32_t*>(slot + cols_off) + t;
+                    uint16_t* mp = reinterpret_cast<uint16_t*>(slot + hd.y) + t;
+                    const int cls = (int)(rw >> 8);
                     const bool noclip = J.quirk && first && cls;
-                    frame_row_any<KIND, DT, EXACT>((int)((rw >> 16) & 0xffu), app, cp, mp, first, noclip, odd,
+                    frame_row_any<KIND, DT, EXACT>((int)(rw & 0xffu), app, cp, mp, po, first, noclip, odd,
                                                    slut + 128 * cls);
                 }
                 // the slot's messages, written by this CTA's threads, are read next by the
@@ -410,8 +423,9 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J,
                 __syncthreads();
                 if (s_abort) break;
                 if (producer) {
+                    const FrameStage st = S.st[l];
                     asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gmsg + st.msg_off),
-                                 "r"(smem_u32(slot + S.rec_max)), "r"(st.msg_bytes)
+                                 "r"(smem_u32(slot + st.rec_bytes)), "r"(st.msg_bytes)
                                  : "memory");
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }

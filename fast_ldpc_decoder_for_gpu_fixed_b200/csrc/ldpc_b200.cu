@@ -326,6 +326,7 @@ const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, int et, int wpt);
 const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
+const void* kernel_table_qc_split(int kind, int dt, int layers, int split, bool et);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
 const void* kernel_table_flood(int kind, int variant);
@@ -391,6 +392,27 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, int 
     }
     if (wpt_out) *wpt_out = wpt;
     return f;
+}
+
+// Path 7: the 2-frame QC kernel with each check row over `split` lanes (4 when Z * 4 <= 256,
+// else 2 when Z * 2 <= 256) for a code that has a 2-frame QC kernel; q as for that kernel.
+static const void* qc_split_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et, int* split_out)
+{
+    int wpt = 2;
+    if (kind == LDPC_2NMS || !qc_kernel_for(c, kind, q, et ? 1 : 0, &wpt) || wpt != 1) return nullptr;
+    const int split = c->z * 4 <= 256 ? 4 : (c->z * 2 <= 256 ? 2 : 0);
+    if (!split) return nullptr;
+    int dt = 0;
+    for (int i = 0; i < c->mb; i++) dt = std::max(dt, q.deg[i]);
+    const int k = kind == LDPC_XMS ? LDPC_OMS : kind;
+    for (int D : {10, 14, 18, 24}) {
+        if (D < dt) continue;
+        if (const void* f = kernel_table_qc_split(k, D, c->mb, split, et)) {
+            *split_out = split;
+            return f;
+        }
+    }
+    return nullptr;
 }
 
 // variant: 0/1 = every row has degree 6/7 (fully unrolled), 2/3/4 = rows of
@@ -509,46 +531,88 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
     return LDPC_OK;
 }
 
-// Path 3: cuts each level of the schedule into stages of at most d->threads rows and lays
-// out their records (row words, then columns with each row padded to an even count) and
-// message offsets, 16-byte aligned for the bulk copies (FrameStage in frame_kernel.cuh).
-static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c)
+// Path 3: cuts each level of the schedule into stages (consecutive rows of the level, at most
+// d->threads - 32 of them and at most one ring slot of bytes, the slot sized so that two CTAs fit
+// on an SM where the frame allows it) and lays out their records and message offsets,
+// 16-byte aligned for the bulk copies (FrameStage in frame_kernel.cuh).  base_smem: the
+// kernel's shared memory before the ring (the APP and the learned tables).
+static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_smem)
 {
-    const int T = d->threads;
+    const int T = d->threads - 32;  // the last warp is the producer's
     auto pad16 = [](long long x) { return (x + 15) / 16 * 16; };
+    int smem_sm = 0, reserved = 0, smem_blk = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, d->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+    // a stage slot holds the header, the row words, the column pairs and the messages of
+    // its rows: at least one row of the largest degree
+    const int np_max = (c->dmax + 1) / 2;
+    const long long slot_min = FRAME_STAGE_HEADER + 16 + pad16(4ll * np_max) + pad16(2ll * np_max);
+    const long long static_smem = 512;  // the kernel's static shared memory, rounded up
+    long long slot_cap = 0;
+    for (int ctas = 2; ctas >= 1 && slot_cap < slot_min; ctas--) {
+        const long long avail = (long long)(ctas == 1 ? smem_blk : smem_sm / ctas - reserved) - static_smem -
+                                (long long)base_smem;
+        slot_cap = avail / FRAME_RING / 16 * 16;
+    }
+    if (slot_cap < slot_min)
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: no room for the stage ring next to the frame");
     std::vector<FrameStage> st;
     std::vector<unsigned char> rec;
     long long moff = 0;
-    int rec_max = 0, msg_max = 0;
-    for (const int2& lv : c->levels) {
-        for (int r0 = lv.x; r0 < lv.x + lv.y; r0 += T) {
-            const int rows = std::min(T, lv.x + lv.y - r0);
-            std::vector<uint32_t> words(rows);
-            std::vector<uint16_t> cols;
-            int off = 0;
-            for (int i = 0; i < rows; i++) {
-                const int r = c->order[r0 + i], b = c->row_ptr[r], dg = c->row_ptr[r + 1] - b;
-                words[i] = (uint32_t)off | (uint32_t)dg << 16 | (uint32_t)c->row_class[r] << 24;
-                for (int j = 0; j < dg; j++) cols.push_back((uint16_t)c->cols[b + j]);
-                if (dg & 1) cols.push_back(0);  // the dummy edge of an odd degree
-                off += dg + (dg & 1);
-            }
-            if (off > 65535) return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: %d edges in one stage", off);
-            FrameStage s{};
-            s.rows = rows;
-            s.cols_off = (int)pad16(4ll * rows);
-            s.rec_bytes = (int)(s.cols_off + pad16(2ll * off));
-            s.msg_bytes = (int)pad16(off);
-            s.rec_off = (int)rec.size();
-            s.msg_off = (int)moff;
-            rec.resize(rec.size() + s.rec_bytes, 0);
-            memcpy(rec.data() + s.rec_off, words.data(), 4 * (size_t)rows);
-            memcpy(rec.data() + s.rec_off + s.cols_off, cols.data(), 2 * (size_t)off);
-            moff += s.msg_bytes;
-            rec_max = std::max(rec_max, s.rec_bytes);
-            msg_max = std::max(msg_max, s.msg_bytes);
-            st.push_back(s);
+    int slot_max = 0;
+    auto slot_bytes = [&](int rows, int pairs) {
+        return FRAME_STAGE_HEADER + pad16(4ll * rows) + pad16(4ll * pairs) + pad16(2ll * pairs);
+    };
+    auto emit = [&](int r0, int rows) {
+        // pair slots: rows sorted by decreasing degree, so slot p is a prefix of the rows
+        int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0}, poff[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < rows; i++) {
+            const int r = c->order[r0 + i], dg = c->row_ptr[r + 1] - c->row_ptr[r];
+            for (int p = 0; p < (dg + 1) / 2; p++) cnt[p]++;
         }
+        int pairs = 0;
+        for (int p = 0; p < 8; p++) {
+            poff[p] = pairs;
+            pairs += cnt[p];
+        }
+        FrameStage s{};
+        const long long cols_off = FRAME_STAGE_HEADER + pad16(4ll * rows);
+        s.rec_bytes = (int)(cols_off + pad16(4ll * pairs));
+        s.msg_bytes = (int)pad16(2ll * pairs);
+        s.rec_off = (int)rec.size();
+        s.msg_off = (int)moff;
+        rec.resize(rec.size() + s.rec_bytes, 0);
+        unsigned char* b = rec.data() + s.rec_off;
+        reinterpret_cast<int32_t*>(b)[0] = rows;
+        reinterpret_cast<int32_t*>(b)[1] = s.rec_bytes;
+        for (int p = 0; p < 8; p++) reinterpret_cast<uint16_t*>(b + 16)[p] = (uint16_t)poff[p];
+        for (int i = 0; i < rows; i++) {
+            const int r = c->order[r0 + i], e0 = c->row_ptr[r], dg = c->row_ptr[r + 1] - e0;
+            reinterpret_cast<uint32_t*>(b + FRAME_STAGE_HEADER)[i] = (uint32_t)dg | (uint32_t)c->row_class[r] << 8;
+            for (int p = 0; p < (dg + 1) / 2; p++) {
+                const uint32_t lo = (uint32_t)c->cols[e0 + 2 * p];
+                const uint32_t hi = 2 * p + 1 < dg ? (uint32_t)c->cols[e0 + 2 * p + 1] : 0u;  // odd degree: dummy
+                reinterpret_cast<uint32_t*>(b + cols_off)[poff[p] + i] = lo | hi << 16;
+            }
+        }
+        moff += s.msg_bytes;
+        slot_max = std::max(slot_max, s.rec_bytes + s.msg_bytes);
+        st.push_back(s);
+    };
+    for (const int2& lv : c->levels) {
+        int r0 = lv.x, rows = 0, pairs = 0;
+        for (int i = lv.x; i < lv.x + lv.y; i++) {
+            const int r = c->order[i], np = (c->row_ptr[r + 1] - c->row_ptr[r] + 1) / 2;
+            if (rows > 0 && (rows == T || slot_bytes(rows + 1, pairs + np) > slot_cap)) {
+                emit(r0, rows);
+                r0 = i;
+                rows = pairs = 0;
+            }
+            rows++;
+            pairs += np;
+        }
+        if (rows) emit(r0, rows);
     }
     if (rec.size() > (size_t)INT32_MAX || moff > INT32_MAX)
         return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: stage records too large");
@@ -562,8 +626,7 @@ static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c)
     d->fst.rec = d->d_frec;
     d->fst.slot_bytes = moff;
     d->fst.nst = (int)st.size();
-    d->fst.rec_max = rec_max;
-    d->fst.msg_max = msg_max;
+    d->fst.slot_sz = slot_max;
     d->fst.status = d->d_status;
     return LDPC_OK;
 }
@@ -588,6 +651,12 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     const int etm = pairs ? 2 : 1;  // the QC kernels' early-stop mode when early
     if (early && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
+    // LDPC_PACK_F16X2_SPLIT: the F16X2 arithmetic on the 2-frame QC kernel with split rows
+    const bool split_req = pack == LDPC_PACK_F16X2_SPLIT;
+    if (split_req) {
+        if (flood) return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_FLOODING: not on LDPC_PACK_F16X2_SPLIT");
+        pack = LDPC_PACK_F16X2;
+    }
     const int pack_req = pack;
     // AUTO: the QC register kernel where one fits (below); otherwise fp16x2 with 2 frames per
     // CTA for the fixed-iteration MS / OMS / NMS / xMS decoders (the fastest level kernel where
@@ -653,20 +722,38 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
                          ? qc_kernel_for(c, kind, d->qcp, early ? etm : 0, &qc_wpt)
                          : nullptr;
     if (qc_wpt == 1 && pack_req != LDPC_PACK_F16X2) qk = nullptr;
-    if (frame) {
+    int split = 0;
+    const void* qsk = split_req && !frame ? qc_split_kernel_for(c, kind, d->qcp, early, &split) : nullptr;
+    if (split_req && (!qsk || per_frame)) {
+        decoder_free(d);
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_F16X2_SPLIT: needs a QC code with a 2-frame QC kernel "
+                                          "(24-column bases), Z <= 128, no per-frame early stop");
+    }
+    if (qsk) {
+        QCParams alt;
+        int s2 = 0;
+        d->kfn = qsk;
+        d->kfn_alt = qc_split_kernel_for(c, kind, alt, !early, &s2);
+        d->path = 7;
+        d->grid_mult = 2;
+        d->pack = LDPC_PACK_F16X2;
+        d->smem = (int)(qc_smem(c, 1) + lut_smem);
+        d->threads = c->z * split;
+    } else if (frame) {
         const int k = kind == LDPC_XMS ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
         d->kfn = kernel_table_frame(k, degree_variant(c), early);
         d->kfn_alt = kernel_table_frame(k, degree_variant(c), !early);
         d->path = 3;
         d->pack = LDPC_PACK_FRAME;
         d->grid_mult = 4;
-        d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32));
-        rc = frame_stages_setup(d, c);
+        // the rows of a stage, then one warp whose last thread issues the bulk copies
+        d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32)) + 32;
+        rc = frame_stages_setup(d, c, frame_smem);
         if (rc) {
             decoder_free(d);
             return rc;
         }
-        d->smem = (int)(frame_smem + (size_t)FRAME_RING * (d->fst.rec_max + d->fst.msg_max));
+        d->smem = (int)(frame_smem + (size_t)FRAME_RING * d->fst.slot_sz);
         if (d->smem > smem_max) {
             decoder_free(d);
             return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: the frame and its stage ring need %d B of shared "
@@ -708,7 +795,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     }
-    if (pairs && d->path != 1 && d->path != 4) {
+    if (pairs && d->path != 1 && d->path != 4 && d->path != 7) {
         decoder_free(d);
         return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_PAIRS: needs a QC register kernel (decoder path 1 or 4)");
     }
@@ -773,7 +860,8 @@ extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int sla
     if (enabled && d->path == 2)
         return fail(LDPC_ERR_ARG, "early stop needs a decoder created with LDPC_FLAG_EARLY_STOP for this packing");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: slack must be >= 0");
-    if ((d->path == 1 || d->path == 3 || d->path == 4) && (enabled != 0) != d->early) std::swap(d->kfn, d->kfn_alt);
+    if ((d->path == 1 || d->path == 3 || d->path == 4 || d->path == 7) && (enabled != 0) != d->early)
+        std::swap(d->kfn, d->kfn_alt);
     d->early = enabled != 0;
     d->early_slack = (unsigned)slack;
     return LDPC_OK;
@@ -896,7 +984,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     J.synd_out = synd_out;
     J.app_out = app_out;
     J.msg_out = msg_out;
-    if (d->path == 4 && iters_out)  // each 2-frame CTA raises its word's count with atomicMax
+    if ((d->path == 4 || d->path == 7) && iters_out)  // each 2-frame CTA raises its word's count with atomicMax
         CUDA_TRY(cudaMemsetAsync(iters_out, 0, sizeof(int32_t) * (size_t)words, st));
     if (d->path == 5) {
         // persistent CTAs, at most the resident ones, each decoding a strided share of the frames
@@ -915,7 +1003,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
         CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
         return LDPC_OK;
     }
-    void* args[] = {(d->path == 1 || d->path == 4) ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
+    void* args[] = {(d->path == 1 || d->path == 4 || d->path == 7) ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
     CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
 }
@@ -946,7 +1034,7 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
-    if (d->path >= 3 && d->path != 6 && (d_app || d_msg))
+    if (d->path >= 3 && d->path != 6 && (d_app || d_msg))  // paths 3, 4, 5, 7
         return fail(LDPC_ERR_UNSUPPORTED, "this decoder (path %d) has no state dumps", d->path);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
@@ -1221,7 +1309,7 @@ struct ldpc_batch {
 // packings, the QC register kernel (QC codes only: 4 frames per CTA on the regular base,
 // path 1, else 2 frames per CTA with early stop per frame pair, path 4) and the flooding
 // schedule (path 6)
-enum BatchCand { CAND_SIMD4 = 0, CAND_F16X2 = 1, CAND_I8 = 2, CAND_QC = 3, CAND_FLOOD = 4, CAND_COUNT = 5 };
+enum BatchCand { CAND_SIMD4 = 0, CAND_F16X2 = 1, CAND_I8 = 2, CAND_QC = 3, CAND_FLOOD = 4, CAND_QC_SPLIT = 5, CAND_COUNT = 6 };
 
 static void batch_free(ldpc_batch* b)
 {
@@ -1283,8 +1371,12 @@ static int batch_code_decoder(ldpc_batch* b, int i, int cand, ldpc_decoder** out
     ldpc_decoder*& d = b->pc_dec[i][cand];
     if (!d) {
         ldpc_code c = b->codes[i];
-        int pack = cand == CAND_SIMD4 ? LDPC_PACK_SIMD4 : (cand == CAND_I8 ? LDPC_PACK_I8 : LDPC_PACK_F16X2);
-        if (cand != CAND_QC) c.qc = false;  // the level kernels, also for a QC code
+        int pack = cand == CAND_SIMD4 ? LDPC_PACK_SIMD4
+                   : cand == CAND_I8  ? LDPC_PACK_I8
+                   : cand == CAND_QC_SPLIT ? LDPC_PACK_F16X2_SPLIT
+                                           : LDPC_PACK_F16X2;
+        const bool qc_cand = cand == CAND_QC || cand == CAND_QC_SPLIT;
+        if (!qc_cand) c.qc = false;  // the level kernels, also for a QC code
         else if (!c.qc) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d is not quasi-cyclic", i);
         const int flags = (b->early ? LDPC_FLAG_EARLY_STOP : 0) | (cand == CAND_FLOOD ? LDPC_FLAG_FLOODING : 0);
         // nb_frames only bounds the words of a call; the batch passes its own counts

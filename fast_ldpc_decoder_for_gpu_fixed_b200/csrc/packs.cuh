@@ -335,6 +335,55 @@ __device__ __forceinline__ void row(uint32_t (&b)[DT], uint32_t (&m)[DT], int d,
         ov += __popc(mn1 & SIGN);  // odd (row, frame) pairs
 }
 
+// row() for a check row split over SPLIT lanes of a warp (lanes k*SPLIT .. k*SPLIT+SPLIT-1):
+// this lane holds nv (<= DL) of the row's edges.  Each lane takes the running min1 / min2 /
+// sign parity of its own edges, then the lanes merge them with log2(SPLIT) butterfly
+// shuffles: min1 = min of both (xorsign: the parities combine), min2 = min(both min2s, max of
+// the two min1s).  A lane without edges contributes (127, 127, +), the reference's initial
+// minima, so it changes nothing.  The reference's min1 / min2 / parity do not depend on the
+// order of the edges, so every lane ends with the row's values and computes its own edges'
+// messages.  wmask: the warp's lanes (all of them take part in every call); lead: the lane
+// that counts the row (CMODE 2).
+template <int KIND, int DL, int SPLIT, int CMODE>
+__device__ __forceinline__ void row_split(uint32_t (&b)[DL], uint32_t (&m)[DL], int nv, bool noclip, uint32_t& ov,
+                                          uint32_t lk, uint32_t lb, unsigned wmask, bool lead)
+{
+    uint32_t ut[DL];
+    uint32_t mn1 = C127, mn2 = C127;
+#pragma unroll
+    for (int i = 0; i < DL; i++) {
+        if (i < nv) {
+            const uint32_t bt = hmin(fma_relu(m[i], NEG1, b[i]), C255);  // clamp(b - m, 0, 255)
+            b[i] = bt;
+            ut[i] = add(bt, CNEG127);
+            const uint32_t mx = max_xs(ut[i], mn1);
+            mn1 = min_xs(mn1, ut[i]);
+            mn2 = min_xs(mn2, mx);
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < SPLIT; o <<= 1) {
+        const uint32_t p1 = __shfl_xor_sync(wmask, mn1, o), p2 = __shfl_xor_sync(wmask, mn2, o);
+        mn2 = min_xs(min_xs(mn2, p2), max_xs(mn1, p1));
+        mn1 = min_xs(mn1, p1);
+    }
+    const uint32_t a1 = habs(mn1), a2 = habs(mn2);
+    uint32_t c1, c2;
+    mags<KIND>(a1, a2, noclip, c1, c2, lk, lb);
+    const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
+    const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
+#pragma unroll
+    for (int i = 0; i < DL; i++) {
+        if (i < nv) {
+            const uint32_t r = fma(add_sat(habs(ut[i]), na1), dcs, c1s);
+            const uint32_t mo = r ^ (ut[i] & SIGN);
+            m[i] = mo;
+            b[i] = hmin(fma_relu(mo, ONE, b[i]), C255);
+        }
+    }
+    if (CMODE == 2 && lead) ov = add(ov, (mn1 & SIGN) | ONE);
+}
+
 // The number of odd rows from a CMODE 2 accumulator of row() after `rows` rows per lane:
 // each row added +1 (even) or -1 (odd) per lane, so 2 * rows - sum is twice that number.
 __device__ __forceinline__ unsigned odd_count(uint32_t acc, int rows)

@@ -309,6 +309,104 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     }
 }
 
+// ---- 2 frames per CTA with each check row split over SPLIT lanes (decoder path 7) ----
+//
+// The layout of the WPT = 1 kernel (CTA 2(g - word0) + h holds frames 2h, 2h + 1 of word g,
+// one fp16x2 pair-word per variable), but row k of a layer belongs to the SPLIT lanes
+// k*SPLIT .. k*SPLIT + SPLIT - 1 of the CTA: lane s takes the row's edges s, s + SPLIT, ...
+// (DL = ceil(DT / SPLIT) of them, their messages in its registers), and the lanes merge their
+// partial min1 / min2 / sign parity with warp shuffles (h2::row_split).  High-degree rows
+// (the rate-3/4 and 5/6 bases reach 18 and 24) then cost DL serial steps instead of DT, a
+// CTA has SPLIT times the threads, and each thread holds 1/SPLIT of the messages.  Every
+// kind but 2NMS; the early stop is per frame pair, as on path 4.
+template <int KIND, int DT, int L, int SPLIT, bool ET>
+__global__ void __launch_bounds__(256) decode_qc_split_kernel(const __grid_constant__ QCParams Q, const Job J)
+{
+    constexpr int DL = (DT + SPLIT - 1) / SPLIT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* app1 = reinterpret_cast<uint32_t*>(smem_raw);  // [n] pair-word of frames 2h, 2h+1
+    char* appb = reinterpret_cast<char*>(smem_raw);
+    const long long g = J.word0 + (blockIdx.x >> 1);
+    const int h = blockIdx.x & 1;
+    const int k = threadIdx.x / SPLIT, s = threadIdx.x % SPLIT;
+    const bool lead = s == 0;
+    // the lanes of this warp (a CTA of Z * SPLIT threads may end in a partial warp; a row's
+    // lanes are never split between warps because SPLIT divides 32)
+    const unsigned wmask = __activemask();
+    __shared__ unsigned s_odd[2];
+    constexpr bool LRN = KIND == KIND_LEARNED;
+    __shared__ uint2 s_kb[LRN ? QC_LUT_ITS : 1][2];
+    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+    if (LRN && threadIdx.x < 2 * J.lut_its) {
+        const int t = threadIdx.x;
+        s_kb[t >> 1][t & 1] = *reinterpret_cast<const uint2*>(J.lut + (t >> 1) * 256 + (t & 1) * 128);
+    }
+    constexpr int CM = ET ? 2 : 0;
+
+    Plan P;
+    P.n = Q.n;
+    read_group(P, J, g, [&](int v, uint32_t w) { app1[v] = Access<PackF16x2>::pair(w, 2 * h); });
+    __syncthreads();
+
+    uint32_t msg[L][DL];
+#pragma unroll
+    for (int l = 0; l < L; l++)
+#pragma unroll
+        for (int i = 0; i < DL; i++) msg[l][i] = 0;
+
+    int executed = 0;
+    bool passed = false;
+    for (int it = 0; it < J.iters; it++) {
+        uint32_t ov = 0;
+        const int lt = LRN ? min(it, J.lut_its - 1) : 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = Q.deg[l];
+            const int nv = d > s ? (d - s + SPLIT - 1) / SPLIT : 0;  // this lane's edges of the row
+            const bool noclip = J.quirk && it == 0 && Q.cls[l];
+            int kk = 4 * k;
+            asm volatile("" : "+r"(kk));
+            int off[DL];
+            uint32_t b[DL];
+#pragma unroll
+            for (int i = 0; i < DL; i++) {
+                if (i < nv) {
+                    off[i] = qc_var_off<false>(Q, l * QC_MAX_DEG + s + SPLIT * i, kk);
+                    b[i] = *reinterpret_cast<const uint32_t*>(appb + off[i]);
+                }
+            }
+            uint32_t lk = 0, lb = 0;
+            if (LRN) {
+                const uint2 kb = s_kb[lt][Q.cls[l]];
+                lk = kb.x;
+                lb = kb.y;
+            }
+            h2::row_split<KIND, DL, SPLIT, CM>(b, msg[l], nv, noclip, ov, lk, lb, wmask, lead);
+#pragma unroll
+            for (int i = 0; i < DL; i++)
+                if (i < nv) *reinterpret_cast<uint32_t*>(appb + off[i]) = b[i];
+            if (!(ET && l == L - 1)) __syncthreads();
+        }
+        executed = it + 1;
+        if (ET) {
+            // the lead lane of each row counts and checks it (the other lanes add nothing)
+            if (odd_rows_within_slack(J, lead ? h2::odd_count(ov, L) : 0u, it, s_odd) &&
+                !__syncthreads_or(lead && qc_rows_unsatisfied<DT, false, 0, L, false, 1>(Q, appb, k))) {
+                passed = true;
+                break;
+            }
+        }
+    }
+    // frames 2h, 2h+1 only; the word's iteration count is the larger of its two pairs
+    // (the host zeroes d_iters_out before the launch)
+    write_group(P, J, g, [&](int v) { return AccessHalf::get(app1, v, h); }, 3 << (2 * h));
+    if (J.iters_out && threadIdx.x == 0) atomicMax(J.iters_out + (g - J.word0), executed);
+    if (J.synd_out) {
+        const unsigned bad = passed || !lead ? 0u : qc_rows_unsat_mask<DT, false, 0, L, false, 1>(Q, appb, k);
+        write_syndrome_flags(J, 4 * (g - J.word0) + 2 * h, bad, 3, true);
+    }
+}
+
 // ---- per-frame early stop with lane refill (decoder path 5) ----
 //
 // The 4 frames of a CTA (the fp16 halves of its two pair-words, "lanes" 0..3) are

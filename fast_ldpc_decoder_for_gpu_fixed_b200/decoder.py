@@ -283,7 +283,7 @@ class Batch:
         """The per-code strategy's kernel of code i (ldpc_batch_code_info)."""
         a = (ctypes.c_int * 5)()
         _lib.check(_lib.lib().ldpc_batch_code_info(self.handle, int(i), a))
-        names = {0: "SIMD4", 1: "F16X2", 2: "I8", 3: "QC", 4: "FLOODING"}
+        names = {0: "SIMD4", 1: "F16X2", 2: "I8", 3: "QC", 4: "FLOODING", 5: "QC_SPLIT"}
         return {"candidate": names.get(a[0], a[0]), "path": a[1], "threads": a[2], "smem": a[3],
                 "ctas_per_sm": a[4]}
 

@@ -82,6 +82,12 @@ extern "C" {
  * frame (4*n_words entries), and state dumps (ldpc_decode_device_state) are
  * unsupported. */
 #define LDPC_PACK_FRAME 3
+/* The 2-frame QC register kernel of path 4 (24-column bases, Z <= 128) with each check row
+ * split over 4 lanes (Z <= 64) or 2 lanes: every lane takes every 4th (2nd) edge of the row
+ * and the lanes merge their min1 / min2 / sign parity with warp shuffles, so a row of
+ * degree 24 costs 6 serial steps and a CTA has Z * 4 (Z * 2) threads.  Info path 7.  Same
+ * decisions, iteration counts (per pair, as path 4) and restrictions as path 4. */
+#define LDPC_PACK_F16X2_SPLIT 4
 
 /* output formats of ldpc_decode_device */
 #define LDPC_OUT_BYTES 0  /* frame-major 0/1 bytes [frames][n] (the reference's)  */
@@ -306,7 +312,8 @@ int ldpc_decoder_set_early_stop(ldpc_decoder* dec, int enabled, int slack);
  * packed row state: LDPC_PACK_FRAME, 4 = QC register-message with 2 frames per
  * CTA, see LDPC_PACK_F16X2, 5 = QC register-message with per-frame early stop,
  * see LDPC_FLAG_EARLY_STOP_FRAMES, 6 = level kernel with the flooding schedule, see
- * LDPC_FLAG_FLOODING) */
+ * LDPC_FLAG_FLOODING, 7 = QC register-message with 2 frames per CTA and split rows, see
+ * LDPC_PACK_F16X2_SPLIT) */
 int ldpc_decoder_info(const ldpc_decoder* dec, int* info);
 
 int ldpc_decoder_destroy(ldpc_decoder* dec);
@@ -351,8 +358,9 @@ int ldpc_batch_decode(ldpc_batch* batch, const int8_t* const* d_llr, void* const
  *    with LDPC_BATCH_GRAPH, in one graph), each code with its own kernel: first, per
  *    code, every candidate is timed alone - the level kernel of each packing (SIMD4,
  *    F16X2, I8: 4 or 2 frames per CTA), the QC register kernel (QC codes: 4 frames per
- *    CTA on the regular base, else 2 with early stop per frame pair) and the flooding
- *    schedule (LDPC_FLAG_FLOODING) - and the
+ *    CTA on the regular base, else 2 with early stop per frame pair), the same 2-frame
+ *    kernel with split rows (LDPC_PACK_F16X2_SPLIT) and the flooding schedule
+ *    (LDPC_FLAG_FLOODING) - and the
  *    fastest is kept among those whose frames failing the syndrome are no more than the
  *    layered SIMD4 kernel's (within 2 % and 2 frames), so that a faster schedule is
  *    never bought with a higher frame error rate;
@@ -363,7 +371,8 @@ int ldpc_batch_autotune(ldpc_batch* batch, const int8_t* const* d_llr, void* con
                         int iters, int32_t* const* d_iters_out, double* best_ms, void* stream);
 
 /* The per-code strategy's kernel of code `code`: info[0] = candidate (0 SIMD4, 1 F16X2,
- * 2 I8 level kernels, 3 the QC register kernel, 4 the flooding schedule), info[1] = its
+ * 2 I8 level kernels, 3 the QC register kernel, 4 the flooding schedule, 5 the QC register
+ * kernel with split rows, LDPC_PACK_F16X2_SPLIT), info[1] = its
  * decoder path (ldpc_decoder_info), info[2] = threads per CTA, info[3] = shared bytes per
  * CTA, info[4] = CTAs per SM; path -1 when that kernel has not been set up yet. */
 int ldpc_batch_code_info(const ldpc_batch* batch, int code, int* info);

@@ -52,7 +52,7 @@ def _check(cs, words, host, outs, its, kind, iters, early, batch=None):
         if per_code:
             ci = batch.code_info(i)
             kw["flooding"] = ci["candidate"] == "FLOODING"
-            kw["pairs"] = ci["path"] == 4 and early
+            kw["pairs"] = ci["path"] in (4, 7) and early
         ref = oracle.decode(c, kind, llr, iters, interleaved=False, early_stop=early, **kw)
         assert np.array_equal(o.cpu().numpy().reshape(4 * w, c.n), ref["hard"]), (c.name, kw)
         assert np.array_equal(it.cpu().numpy(), ref["iters"]), (c.name, kw)
@@ -119,7 +119,7 @@ def test_batch_autotune(cuda):
     b.close()
 
 
-@pytest.mark.parametrize("cand", ["FLOODING", "QC"])
+@pytest.mark.parametrize("cand", ["FLOODING", "QC", "QC_SPLIT"])
 def test_batch_per_code_candidates(cuda, cand):
     """Every code on the flooding schedule, or on the QC register kernel, through the
     per-code strategy, against the oracle under that schedule."""
@@ -132,10 +132,10 @@ def test_batch_per_code_candidates(cuda, cand):
     took = 0
     for i in range(len(cs)):
         try:
-            b.set_code_kernel_one(i, {"FLOODING": 4, "QC": 3}[cand])
+            b.set_code_kernel_one(i, {"FLOODING": 4, "QC": 3, "QC_SPLIT": 5}[cand])
             took += 1
         except LdpcError as e:   # a QC shape without an instantiated register kernel
-            assert cand == "QC" and e.code == -3
+            assert cand.startswith("QC") and e.code == -3
     assert took >= (len(cs) if cand == "FLOODING" else 2)
     b.decode(llrs, outs, words, 20, d_iters=its)
     assert sum(b.code_info(i)["candidate"] == cand for i in range(len(cs))) == took

@@ -176,3 +176,54 @@ def test_pair_qc_kernel_other_paths(cuda):
     sim_llr, _ = oracle.awgn(4 * words, code.n, 0.8, 9, 2)
     assert np.array_equal(d_hard.cpu().numpy().reshape(4 * words, code.n), oracle.decode(code, "OMS", sim_llr, 15)["hard"])
     dec.close()
+
+
+# ---- path 7: the 2-frame QC kernel with each row split over 2 or 4 lanes ----
+
+@pytest.mark.parametrize("rate,z", [((1, 2), 81), ((2, 3), 54), ((3, 4), 27), ((5, 6), 27), ((5, 6), 64),
+                                    ((1, 2), 128)])
+@pytest.mark.parametrize("kind", ["MS", "OMS", "NMS"])
+def test_split_qc_kernel_fixed_iterations(cuda, rate, z, kind):
+    """Rows of degree up to 24 split over 4 lanes (Z <= 64) or 2 (Z <= 128): the warp-shuffle
+    merge of min1 / min2 / parity equals the serial row update bit for bit."""
+    from oracle import oracle
+    code = irregular(rate, z)
+    words = 10
+    llr = make_llr("uniform" if kind == "MS" else "awgn", 4 * words * code.n, 61,
+                   sigma=llr_gen.sigma_for(2.5, rate[0] / rate[1]))
+    path, hard, its = _pair_decode(code, kind, llr, 12, words, pack="F16X2_SPLIT")
+    assert path == 7
+    ref = oracle.decode(code, kind, llr, 12)
+    assert np.array_equal(hard, ref["hard"])
+    assert (its == 12).all()
+
+
+@pytest.mark.parametrize("rate,z", [((1, 2), 81), ((5, 6), 27)])
+def test_split_qc_kernel_early_stop_and_learned(cuda, rate, z):
+    from oracle import oracle
+    code = irregular(rate, z)
+    words = 24
+    r = rate[0] / rate[1]
+    llr = np.concatenate([make_llr("awgn", 4 * 8 * code.n, 67 + i, sigma=llr_gen.sigma_for(e, r))
+                          for i, e in enumerate((1.5, 3.0, 5.0))])
+    path, hard, its = _pair_decode(code, "OMS", llr, 20, words, early=True, pack="F16X2_SPLIT")
+    assert path == 7
+    ref = oracle.decode(code, "OMS", llr, 20, early_stop=True, pairs=True)
+    assert np.array_equal(its, ref["iters"])
+    assert np.array_equal(hard, ref["hard"])
+    assert len(set(its.tolist())) > 2
+    off = np.array([[1, 1], [0, 0], [1, 2]], dtype=np.int8)
+    sc = np.array([[120, 128], [112, 104], [128, 96]], dtype=np.uint8)
+    oracle.set_learned(off, sc)
+    path, hard, _ = _pair_decode(code, "LEARNED", llr, 10, words, early=True, constants=(off, sc),
+                                 pack="F16X2_SPLIT")
+    assert path == 7
+    assert np.array_equal(hard, oracle.decode(code, "LEARNED", llr, 10, early_stop=True, pairs=True)["hard"])
+
+
+def test_split_qc_kernel_refusals(cuda):
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import LdpcError
+    with pytest.raises(LdpcError):   # the regular 8x16 base has no 2-frame kernel
+        Decoder(qc_code(), "OMS", nb_frames=4, pack="F16X2_SPLIT")
+    with pytest.raises(LdpcError):   # 2NMS terminates per 4-frame word
+        Decoder(irregular((1, 2), 81), "2NMS", nb_frames=4, pack="F16X2_SPLIT")
