@@ -27,6 +27,7 @@ def _decode(code, kind, llr, iters, words, early=False, slack=None, constants=No
     d_it = torch.zeros(4 * words, dtype=torch.int32, device="cuda")
     dec.decode_device(d_llr, d_hard, words, iters, d_iters=d_it)
     torch.cuda.synchronize()
+    assert dec.status() == 0   # no wait on the copy engine gave up
     dec.close()
     return d_hard.cpu().numpy().reshape(4 * words, code.n), d_it.cpu().numpy()
 

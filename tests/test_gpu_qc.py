@@ -181,7 +181,7 @@ def test_pair_qc_kernel_other_paths(cuda):
 # ---- path 7: the 2-frame QC kernel with each row split over 2 or 4 lanes ----
 
 @pytest.mark.parametrize("rate,z", [((1, 2), 81), ((2, 3), 54), ((3, 4), 27), ((5, 6), 27), ((5, 6), 64),
-                                    ((1, 2), 128)])
+                                    ((3, 4), 128)])
 @pytest.mark.parametrize("kind", ["MS", "OMS", "NMS"])
 def test_split_qc_kernel_fixed_iterations(cuda, rate, z, kind):
     """Rows of degree up to 24 split over 4 lanes (Z <= 64) or 2 (Z <= 128): the warp-shuffle
