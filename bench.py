@@ -7,8 +7,10 @@ Default workload (the metric: learned-offset decoder vs plain OMS at equal FER):
   at Eb/N0 = 2.25 dB, int8 LLRs quantised like the reference channel
   (q = trunc(clamp(8y, -31, 31)), awgn_channel/CChanel_AWGN_SIMD.cu:21-24),
   65536 frames per GPU, at most 10 layered iterations.
-  value      : the deployed learned-offset decoder (LDPC_LEARNED with the constants in
-               fast_ldpc_decoder_for_gpu_fixed_b200/trained/qc3x6_z256_T10.json,
+  value      : the deployed learned-offset decoder (LDPC_LEARNED with the per-iteration
+               offsets in fast_ldpc_decoder_for_gpu_fixed_b200/trained/qc3x6_z256_T10_offsets.json,
+               trained with every scale held at 1.0; --constants for another set, such as the
+               offsets-and-scales set qc3x6_z256_T10.json,
                syndrome early stop per 4-frame word; --early-unit pairs|frame for the
                other units), kernel only, LLRs resident in HBM
   plain_oms  : the plain 8-bit OMS kernel (offset 1, 10 fixed iterations) on the same
@@ -42,7 +44,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "qc(3,6) N=4096 K=2048 Z=256, 65536 frames, Eb/N0 %.2f dB: learned-offset int8 decoder with early stop " \
            "(max %d layered iterations) vs plain OMS offset 1, %d fixed iterations"
-TRAINED = os.path.join(ROOT, "fast_ldpc_decoder_for_gpu_fixed_b200", "trained", "qc3x6_z256_T10.json")
+TRAINED = os.path.join(ROOT, "fast_ldpc_decoder_for_gpu_fixed_b200", "trained", "qc3x6_z256_T10_offsets.json")
 
 
 def parse():

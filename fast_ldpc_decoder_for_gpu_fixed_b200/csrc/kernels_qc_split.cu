@@ -1,5 +1,5 @@
 // Instantiations of the 2-frame QC register-message decoder whose check rows are split over
-// 2 or 4 lanes (decode_qc_split_kernel, decoder path 7), for the 24-column irregular bases
+// 4 lanes (decode_qc_split_kernel, decoder path 7; Z <= 128), for the 24-column irregular bases
 // at rates 1/2, 2/3, 3/4, 5/6 (12, 8, 6, 4 layers of row degree up to 10, 14, 18, 24), any
 // Z, every kind but 2NMS, with and without the syndrome early stop.
 #include "qc_kernel.cuh"
@@ -15,7 +15,6 @@ namespace ldpc {
 
 const void* kernel_table_qc_split(int kind, int dt, int layers, int split, bool et)
 {
-    LDPC_QCS_KINDS(10, 12, 2) LDPC_QCS_KINDS(14, 8, 2) LDPC_QCS_KINDS(18, 6, 2) LDPC_QCS_KINDS(24, 4, 2)
     LDPC_QCS_KINDS(10, 12, 4) LDPC_QCS_KINDS(14, 8, 4) LDPC_QCS_KINDS(18, 6, 4) LDPC_QCS_KINDS(24, 4, 4)
     return nullptr;
 }

@@ -102,9 +102,11 @@ struct ldpc_decoder {
     int threads = 0, smem = 0, ctas_per_sm = 0, regs = 0;
     const void* kfn = nullptr;
     const void* kfn_alt = nullptr;  // the same kernel with the other early-stop setting (paths 1, 3 and 4)
-    // path 1, LDPC_LEARNED: the general and the offset-only (every scale 1.0) kernels with
-    // and without the early stop; ldpc_decoder_set_learned picks from them
-    const void* kfn_lrn[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [offset-only][early stop]
+    // path 1, LDPC_LEARNED: the general, the offset-only (every scale 1.0) and the OMS kernel
+    // (every scale 1.0 and every offset 1: OMS's arithmetic, without its first-iteration
+    // quirk, which the learned kind does not have) with and without the early stop;
+    // ldpc_decoder_set_learned picks from them
+    const void* kfn_lrn[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};  // [constants][early stop]
     // 0 = level-scheduled kernel, 1 = QC register-message kernel, 2 = level-scheduled, 2 frames per CTA,
     // 3 = one frame per CTA, 4 = QC register-message, 2 frames per CTA, 5 = QC register-message with
     // per-frame early stop and lane refill (persistent CTAs)
@@ -394,13 +396,13 @@ static const void* qc_kernel_for(const ldpc_code* c, int kind, QCParams& q, int 
     return f;
 }
 
-// Path 7: the 2-frame QC kernel with each check row over `split` lanes (4 when Z * 4 <= 256,
-// else 2 when Z * 2 <= 256) for a code that has a 2-frame QC kernel; q as for that kernel.
+// Path 7: the 2-frame QC kernel with each check row over 4 lanes (Z <= 128, so that a CTA has
+// at most 512 threads) for a code that has a 2-frame QC kernel; q as for that kernel.
 static const void* qc_split_kernel_for(const ldpc_code* c, int kind, QCParams& q, bool et, int* split_out)
 {
     int wpt = 2;
     if (kind == LDPC_2NMS || !qc_kernel_for(c, kind, q, et ? 1 : 0, &wpt) || wpt != 1) return nullptr;
-    const int split = c->z * 4 <= 256 ? 4 : (c->z * 2 <= 256 ? 2 : 0);
+    const int split = c->z * 4 <= 512 ? 4 : 0;
     if (!split) return nullptr;
     int dt = 0;
     for (int i = 0; i < c->mb; i++) dt = std::max(dt, q.deg[i]);
@@ -770,9 +772,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->kfn = qk;
         d->kfn_alt = qc_kernel_for(c, kind, alt, early ? 0 : etm);  // for ldpc_decoder_set_early_stop (same layout)
         if (kind == LDPC_LEARNED && qc_wpt == 2)
-            for (int o = 0; o < 2; o++)
-                for (int e = 0; e < 2; e++)
+            for (int e = 0; e < 2; e++) {
+                for (int o = 0; o < 2; o++)
                     d->kfn_lrn[o][e] = qc_kernel_for(c, kind, alt, e != 0 ? etm : 0, nullptr, false, o != 0);
+                d->kfn_lrn[2][e] = qc_kernel_for(c, LDPC_OMS, alt, e != 0 ? etm : 0);
+            }
         d->path = qc_wpt == 2 ? 1 : 4;
         d->grid_mult = qc_wpt == 2 ? 1 : 2;
         d->pack = LDPC_PACK_F16X2;
@@ -813,7 +817,7 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
     }
     cudaError_t e1 = ldpc_internal_raise_smem(d->kfn, d->smem);
     if (e1 == cudaSuccess && d->kfn_alt) e1 = ldpc_internal_raise_smem(d->kfn_alt, d->smem);
-    for (int o = 0; o < 2; o++)
+    for (int o = 0; o < 3; o++)
         for (int e = 0; e < 2; e++)
             if (e1 == cudaSuccess && d->kfn_lrn[o][e]) e1 = ldpc_internal_raise_smem(d->kfn_lrn[o][e], d->smem);
     cudaFuncAttributes fa;
@@ -927,11 +931,17 @@ extern "C" int ldpc_decoder_set_learned(ldpc_decoder* d, int n_iters, const int8
     d->lut_its = n_iters;
     if (d->kfn_lrn[0][0]) {
         // the QC register kernel: constants with every scale 1.0 (offsets only) take the kernel
-        // whose magnitude is min - offset, the arithmetic of OMS, without the floor step
-        bool ofs = true;
-        for (int i = 0; i < 2 * n_iters; i++) ofs = ofs && scales[i] == 128;
-        d->kfn = d->kfn_lrn[ofs][d->early];
-        d->kfn_alt = d->kfn_lrn[ofs][!d->early];
+        // whose magnitude is min - offset, without the floor step; with every offset 1 as well
+        // that is OMS's magnitude clamp(min - 1, 0, 31) in every iteration, and the OMS kernel
+        // (launched without the OMS first-iteration quirk, J.quirk = 0) computes it
+        bool ofs = true, oms = true;
+        for (int i = 0; i < 2 * n_iters; i++) {
+            ofs = ofs && scales[i] == 128;
+            oms = oms && scales[i] == 128 && offsets[i] == 1;
+        }
+        const int sel = oms ? 2 : (ofs ? 1 : 0);
+        d->kfn = d->kfn_lrn[sel][d->early];
+        d->kfn_alt = d->kfn_lrn[sel][!d->early];
     }
     return LDPC_OK;
 }

@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
 // CTA has SPLIT times the threads, and each thread holds 1/SPLIT of the messages.  Every
 // kind but 2NMS; the early stop is per frame pair, as on path 4.
 template <int KIND, int DT, int L, int SPLIT, bool ET>
-__global__ void __launch_bounds__(256) decode_qc_split_kernel(const __grid_constant__ QCParams Q, const Job J)
+__global__ void __launch_bounds__(512) decode_qc_split_kernel(const __grid_constant__ QCParams Q, const Job J)
 {
     constexpr int DL = (DT + SPLIT - 1) / SPLIT;
     extern __shared__ __align__(16) unsigned char smem_raw[];

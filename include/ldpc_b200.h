@@ -83,10 +83,10 @@ extern "C" {
  * unsupported. */
 #define LDPC_PACK_FRAME 3
 /* The 2-frame QC register kernel of path 4 (24-column bases, Z <= 128) with each check row
- * split over 4 lanes (Z <= 64) or 2 lanes: every lane takes every 4th (2nd) edge of the row
- * and the lanes merge their min1 / min2 / sign parity with warp shuffles, so a row of
- * degree 24 costs 6 serial steps and a CTA has Z * 4 (Z * 2) threads.  Info path 7.  Same
- * decisions, iteration counts (per pair, as path 4) and restrictions as path 4. */
+ * split over 4 lanes: every lane takes every 4th edge of the row and the lanes merge their
+ * min1 / min2 / sign parity with warp shuffles, so a row of degree 24 costs 6 serial steps
+ * and a CTA has Z * 4 threads.  Info path 7.  Same decisions, iteration counts (per pair, as
+ * path 4) and restrictions as path 4. */
 #define LDPC_PACK_F16X2_SPLIT 4
 
 /* output formats of ldpc_decode_device */

@@ -67,6 +67,34 @@ def test_learned_equals_oms_without_quirk(cuda):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("early", [False, True])
+def test_learned_oms_constants_on_the_qc_kernel(cuda, early):
+    """Constants equal to OMS's (scale 1.0, offset 1 in every iteration and group) run the OMS
+    QC kernel with the first-iteration quirk off (a QC code has one row group, so the quirk
+    never applies there anyway): decisions and iteration counts equal the oracle's LEARNED
+    decode with those constants."""
+    import torch
+    code = qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
+    words = 12
+    off, sc = np.ones((10, 2), dtype=np.int8), np.full((10, 2), 128, dtype=np.uint8)
+    oracle.set_learned(off, sc)
+    llr = make_llr("awgn", 4 * words * code.n, 8, sigma=llr_gen.sigma_for(2.25, 0.5))
+    dec = Decoder(code, "LEARNED", nb_frames=words, early_stop=early)
+    dec.set_learned(off, sc)
+    assert dec.info()["path"] == 1
+    d_llr = torch.from_numpy(llr).cuda()
+    d_out = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    d_it = torch.zeros(words, dtype=torch.int32, device="cuda")
+    dec.decode_device(d_llr, d_out, words, 10, d_iters=d_it)
+    torch.cuda.synchronize()
+    dec.close()
+    ref = oracle.decode(code, "LEARNED", llr, 10, interleaved=False, early_stop=early)
+    assert np.array_equal(d_out.cpu().numpy().reshape(4 * words, code.n), ref["hard"])
+    assert np.array_equal(d_it.cpu().numpy(), ref["iters"])
+    if early:
+        assert len(set(ref["iters"].tolist())) > 1
+
+
 def test_learned_requires_constants(cuda):
     import torch
     code = load_table("576x288")

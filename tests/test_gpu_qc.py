@@ -184,7 +184,7 @@ def test_pair_qc_kernel_other_paths(cuda):
                                     ((3, 4), 128)])
 @pytest.mark.parametrize("kind", ["MS", "OMS", "NMS"])
 def test_split_qc_kernel_fixed_iterations(cuda, rate, z, kind):
-    """Rows of degree up to 24 split over 4 lanes (Z <= 64) or 2 (Z <= 128): the warp-shuffle
+    """Rows of degree up to 24 split over 4 lanes (Z up to 128, 512 threads): the warp-shuffle
     merge of min1 / min2 / parity equals the serial row update bit for bit."""
     from oracle import oracle
     code = irregular(rate, z)
@@ -227,3 +227,5 @@ def test_split_qc_kernel_refusals(cuda):
         Decoder(qc_code(), "OMS", nb_frames=4, pack="F16X2_SPLIT")
     with pytest.raises(LdpcError):   # 2NMS terminates per 4-frame word
         Decoder(irregular((1, 2), 81), "2NMS", nb_frames=4, pack="F16X2_SPLIT")
+    with pytest.raises(LdpcError):   # Z = 192: more than 512 threads
+        Decoder(irregular((3, 4), 192), "OMS", nb_frames=4, pack="F16X2_SPLIT")
