@@ -28,12 +28,13 @@ struct BatchCode {
 
 // VMAX: the largest degree class of the batch; each word runs the unrolled update
 // of its own code's class
-template <class PK, int KIND, int VMAX>
+// PF: the per-frame early stop (PackSIMD4; iters_out then holds one count per frame)
+template <class PK, int KIND, int VMAX, bool PF = false>
 __global__ void __launch_bounds__(256) decode_batch_kernel(const BatchCode* __restrict__ codes, int n_codes,
                                                            unsigned long long* counter, long long total, const Job base)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ unsigned s_odd[2];
+    __shared__ unsigned s_odd[4];
     __shared__ long long s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ull);
@@ -55,11 +56,11 @@ __global__ void __launch_bounds__(256) decode_batch_kernel(const BatchCode* __re
         const Plan P = bc.plan;
         const long long g = item - bc.first_item;
         if (VMAX == 0 || bc.variant == 0)
-            decode_word_levels<PK, KIND, 8, false>(P, J, g, smem_raw, s_odd);
+            decode_word_levels<PK, KIND, 8, false, PF>(P, J, g, smem_raw, s_odd);
         else if (VMAX == 1 || bc.variant == 1)
-            decode_word_levels<PK, KIND, (VMAX >= 1 ? 16 : 8), false>(P, J, g, smem_raw, s_odd);
+            decode_word_levels<PK, KIND, (VMAX >= 1 ? 16 : 8), false, PF>(P, J, g, smem_raw, s_odd);
         else
-            decode_word_levels<PK, KIND, (VMAX >= 2 ? 32 : 8), false>(P, J, g, smem_raw, s_odd);
+            decode_word_levels<PK, KIND, (VMAX >= 2 ? 32 : 8), false, PF>(P, J, g, smem_raw, s_odd);
         __syncthreads();  // shared memory and s_item are reused by the next item
     }
 }
@@ -78,6 +79,20 @@ const void* kernel_table_batch(int pack, int kind, int variant)
     const int row = kind == KIND_LEARNED ? 4 : kind;
     if (pack < 0 || pack > 2 || row < 0 || row > 4 || variant < 0 || variant > 2) return nullptr;
     return table[pack][row][variant];
+}
+
+#define LDPC_BATCH_ROW_PF(KIND)                                                                                \
+    {(const void*)decode_batch_kernel<PackSIMD4, KIND, 0, true>, (const void*)decode_batch_kernel<PackSIMD4, KIND, 1, true>, \
+     (const void*)decode_batch_kernel<PackSIMD4, KIND, 2, true>},
+
+// the per-frame early stop, PackSIMD4: [kind: MS, OMS, NMS, LEARNED][largest degree class]
+const void* kernel_table_batch_pf(int kind, int variant)
+{
+    static const void* table[4][3] = {LDPC_BATCH_ROW_PF(KIND_MS) LDPC_BATCH_ROW_PF(KIND_OMS) LDPC_BATCH_ROW_PF(KIND_NMS)
+                                          LDPC_BATCH_ROW_PF(KIND_LEARNED)};
+    const int row = kind == KIND_LEARNED ? 3 : kind;
+    if (kind == KIND_2NMS || row < 0 || row > 3 || variant < 0 || variant > 2) return nullptr;
+    return table[row][variant];
 }
 
 size_t batch_code_bytes() { return sizeof(BatchCode); }

@@ -462,20 +462,74 @@ __device__ __forceinline__ void row_update(typename PK::S* app, typename PK::S* 
     }
 }
 
+// row_update() for PackSIMD4 with the odd rows counted per frame (PackSIMD4::update_lanes)
+template <int KIND, int DT, bool EXACT>
+__device__ __forceinline__ void row_update_lanes(uint32_t* app, uint32_t* msg, const Plan& P, int r, int d,
+                                                 bool noclip, uint32_t& oc01, uint32_t& oc23, const uint16_t* lut)
+{
+    int v[DT];
+    uint32_t x[DT], mm[DT];
+#pragma unroll
+    for (int j = 0; j < DT; j++) {
+        if (EXACT || j < d) {
+            v[j] = __ldg(P.cols + j * P.m + r);
+            x[j] = app[v[j]];
+            mm[j] = msg[j * P.m + r];
+        }
+    }
+    PackSIMD4::template update_lanes<KIND, DT, EXACT>(x, mm, d, noclip, oc01, oc23, lut);
+#pragma unroll
+    for (int j = 0; j < DT; j++) {
+        if (EXACT || j < d) {
+            msg[j * P.m + r] = mm[j];
+            app[v[j]] = x[j];
+        }
+    }
+}
+
+// The CTA's per-frame odd-row totals of iteration it: a holds frames 0 and 1 in its 16-bit
+// halves, b frames 2 and 3 (each total at most m < 2^16).  s4: four words, zeroed before the
+// first iteration; each iteration uses one pair and clears the other.  Every thread calls it.
+__device__ __forceinline__ uint2 odd_rows_total_lanes(uint32_t a, uint32_t b, int it, unsigned* s4)
+{
+    const unsigned lanes = __activemask();
+    const unsigned wa = __reduce_add_sync(lanes, a), wb = __reduce_add_sync(lanes, b);
+    unsigned* cur = s4 + 2 * (it & 1);
+    if ((int)(threadIdx.x & 31) == __ffs(lanes) - 1) {
+        if (wa) atomicAdd(cur, wa);
+        if (wb) atomicAdd(cur + 1, wb);
+    }
+    __syncthreads();
+    const uint2 t = make_uint2(cur[0], cur[1]);
+    if (threadIdx.x == 0) {
+        unsigned* nxt = s4 + 2 * ((it + 1) & 1);
+        nxt[0] = 0;
+        nxt[1] = 0;
+    }
+    return t;
+}
+
 // Decodes word g (4 frames) with the level schedule, all state in the CTA's shared
 // memory (smem_raw: APP, messages, then the LEARNED table).  Every thread of the
 // CTA calls it; it has no barrier after its last shared-memory access, so a
 // caller that reuses the memory synchronises first.
-template <class PK, int KIND, int DT, bool EXACT>
+// PF (PackSIMD4 only, LDPC_FLAG_EARLY_STOP_FRAMES): each frame (byte lane) stops on its own:
+// after an iteration in which at most J.early_slack of its rows had odd extrinsic parity
+// and its hard decisions satisfy every check, its decisions are written and its count is
+// recorded (d_iters_out: one count per frame); the lanes are independent, so what it writes
+// is what decoding that frame alone gives.  The CTA goes on while a frame is live.
+// s_odd: two words, four with PF.
+template <class PK, int KIND, int DT, bool EXACT, bool PF = false>
 __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, long long g, unsigned char* smem_raw,
                                                    unsigned* s_odd)
 {
+    static_assert(!PF || (PK::ID == 0 && KIND != KIND_2NMS), "per-frame early stop: PackSIMD4, not 2NMS");
     using S = typename PK::S;
     using R = typename PK::R;
     S* app = reinterpret_cast<S*>(smem_raw);
     S* msg = app + PK::WPC * P.npad;
     uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + PK::WPC * sizeof(S) * ((size_t)P.npad + (size_t)P.dmax * P.m));
-    if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+    if (threadIdx.x < (PF ? 4 : 2)) s_odd[threadIdx.x] = 0;
 
     read_group(P, J, g, [&](int v, uint32_t w) { Access<PK>::put(app, P.npad, v, w); });
     {
@@ -487,8 +541,12 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
 
     int executed = 0;
     bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
+    unsigned live = 0xFu;        // PF: frames still decoding (the same in every thread)
+    int its[4] = {0, 0, 0, 0};   // PF: iterations of the frames that stopped
+    const auto get = [&](int v) { return Access<PK>::get(app, P.npad, v); };
     for (int it = 0; it < J.iters; it++) {
         R ov = 0;
+        uint32_t oc01 = 0, oc23 = 0;  // PF: odd rows per frame (16-bit halves)
         const bool first = (it == 0);
         if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
         for (int l = 0; l < P.nlevels; l++) {
@@ -497,11 +555,40 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
                 const int d = EXACT ? DT : __ldg(P.rowdeg + r);
                 const int cls = __ldg(P.rowcls + r);
                 const bool noclip = J.quirk && first && cls;
-                row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov, slut + 128 * cls);
+                if (PF)
+                    row_update_lanes<KIND, DT, EXACT>(reinterpret_cast<uint32_t*>(app), reinterpret_cast<uint32_t*>(msg),
+                                                      P, r, d, noclip, oc01, oc23, slut + 128 * cls);
+                else
+                    row_update<PK, KIND, DT, EXACT>(app, msg, P, r, d, noclip, ov, slut + 128 * cls);
             }
             __syncthreads();
         }
         executed = it + 1;
+        if (PF) {
+            const uint2 t = odd_rows_total_lanes(oc01, oc23, it, s_odd);
+            const unsigned cnt[4] = {t.x & 0xffffu, t.x >> 16, t.y & 0xffffu, t.y >> 16};
+            unsigned gate = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (((live >> k) & 1u) && cnt[k] <= J.early_slack) gate |= 1u << k;
+            if (gate) {
+                const uint32_t bad = rows_odd_mask(P, get);  // 0xff in byte k: frame k has an odd check
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (((gate >> k) & 1u) && __syncthreads_or((bad >> (8 * k)) & 0xffu)) gate &= ~(1u << k);
+                if (gate) {
+                    // these frames stop here: their decisions now, their count
+                    write_group(P, J, g, get, (int)gate);
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if ((gate >> k) & 1u) its[k] = it + 1;
+                    live &= ~gate;
+                    if (!live) break;
+                    __syncthreads();  // write_group read the APP that the next iteration updates
+                }
+            }
+            continue;
+        }
         if (KIND == KIND_2NMS && it >= 1) {
             if (!__syncthreads_or(ov != 0)) break;
         }
@@ -513,10 +600,23 @@ __device__ __forceinline__ void decode_word_levels(const Plan& P, const Job& J, 
         }
     }
 
-    write_group(P, J, g, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+    if (PF) {
+        // the frames still live ran every iteration
+        if (live) write_group(P, J, g, get, (int)live);
+        if (J.iters_out && threadIdx.x == 0)
+            for (int k = 0; k < 4; k++) J.iters_out[4 * (g - J.word0) + k] = ((live >> k) & 1u) ? executed : its[k];
+        if (J.synd_out) {
+            if (threadIdx.x == 0)
+                for (int k = 0; k < 4; k++)
+                    if (!((live >> k) & 1u)) J.synd_out[4 * (g - J.word0) + k] = 1;
+            if (live) write_syndrome_flags(J, 4 * (g - J.word0), rows_odd_mask(P, get), (int)live);
+        }
+        return;
+    }
+    write_group(P, J, g, get);
     if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = executed;
     if (J.synd_out) {
-        const uint32_t bad = passed ? 0u : rows_odd_mask(P, [&](int v) { return Access<PK>::get(app, P.npad, v); });
+        const uint32_t bad = passed ? 0u : rows_odd_mask(P, get);
         write_syndrome_flags(J, 4 * (g - J.word0), bad, 0xF);
     }
     if (J.app_out) {
@@ -651,12 +751,12 @@ __global__ void __launch_bounds__(256) decode_flood_kernel(const Plan P, const J
     }
 }
 
-template <class PK, int KIND, int DT, bool EXACT>
+template <class PK, int KIND, int DT, bool EXACT, bool PF = false>
 __global__ void __launch_bounds__(256) decode_levels_kernel(const Plan P, const Job J)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ unsigned s_odd[2];
-    decode_word_levels<PK, KIND, DT, EXACT>(P, J, J.word0 + blockIdx.x, smem_raw, s_odd);
+    __shared__ unsigned s_odd[4];
+    decode_word_levels<PK, KIND, DT, EXACT, PF>(P, J, J.word0 + blockIdx.x, smem_raw, s_odd);
 }
 
 // The level-scheduled kernel for PackF16x2h: a CTA holds frames 2h, 2h+1 of word g

@@ -16,4 +16,17 @@ const void* kernel_table_simd4(int kind, int variant)
     return table[kind][variant];
 }
 
+// the per-frame early stop (LDPC_FLAG_EARLY_STOP_FRAMES): [kind: MS, OMS, NMS, -, LEARNED][variant]
+#define LDPC_ENTRY_PF(PK, KIND, D, EX) (const void*)decode_levels_kernel<PK, KIND, D, EX, true>,
+#define LDPC_ROW_PF(KIND) {LDPC_DEGREE_VARIANTS(LDPC_ENTRY_PF, PackSIMD4, KIND)},
+
+const void* kernel_table_simd4_pf(int kind, int variant)
+{
+    static const void* table[4][5] = {LDPC_ROW_PF(KIND_MS) LDPC_ROW_PF(KIND_OMS) LDPC_ROW_PF(KIND_NMS)
+                                      LDPC_ROW_PF(KIND_LEARNED)};
+    const int row = kind == KIND_LEARNED ? 3 : kind;
+    if (kind == KIND_2NMS || row < 0 || row > 3 || variant < 0 || variant > 4) return nullptr;
+    return table[row][variant];
+}
+
 }  // namespace ldpc

@@ -101,6 +101,25 @@ struct PackSIMD4 {
     __device__ __forceinline__ static void update(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& ov,
                                                   const uint16_t* lut)
     {
+        const R s = update_row<KIND, DT, EXACT>(x, m, d, noclip, lut);
+        ov += __popc(s) >> 3;  // odd (row, frame) pairs: s is 0xff in each odd byte
+    }
+
+    // update() with the odd rows counted per frame: lanes 0 and 1 in the 16-bit halves of
+    // oc01, lanes 2 and 3 in those of oc23 (the per-frame early stop)
+    template <int KIND, int DT, bool EXACT>
+    __device__ __forceinline__ static void update_lanes(R (&x)[DT], R (&m)[DT], int d, bool noclip, R& oc01,
+                                                        R& oc23, const uint16_t* lut)
+    {
+        const R s = update_row<KIND, DT, EXACT>(x, m, d, noclip, lut);
+        oc01 += __byte_perm(s, 0, 0x4140) & 0x00010001u;
+        oc23 += __byte_perm(s, 0, 0x4342) & 0x00010001u;
+    }
+
+    // the row update; returns the row's extrinsic sign parity, 0xff in each odd byte lane
+    template <int KIND, int DT, bool EXACT>
+    __device__ __forceinline__ static R update_row(R (&x)[DT], R (&m)[DT], int d, bool noclip, const uint16_t* lut)
+    {
         R mn1 = 0x7f7f7f7fu, mn2 = 0x7f7f7f7fu, s = 0;
 #pragma unroll
         for (int j = 0; j < DT; j++) {
@@ -127,7 +146,7 @@ struct PackSIMD4 {
                 x[j] = __vaddss4(t, out);
             }
         }
-        ov += __popc(s) >> 3;  // odd (row, frame) pairs: s is 0xff in each odd byte
+        return s;
     }
 };
 
