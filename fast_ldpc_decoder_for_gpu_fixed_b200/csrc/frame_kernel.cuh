@@ -464,4 +464,259 @@ __global__ void __maxnreg__(80) decode_frame_kernel(const Plan P, const Job J,
     }
 }
 
+// ---- two frames per CTA (decoder path 3 when two frames' APP fit) ----
+//
+// The same stages, ring, producer warp and copy protocol as decode_frame_kernel, but the CTA
+// holds frames 2p and 2p + 1 of the launch as the two fp16 lanes of every word: its APP is
+// one u16 per variable (the two frames' int8 values), and each thread updates its row for
+// both frames at once, one edge per fp16x2 word, so the per-row work (record, dispatch,
+// minima, magnitudes) is shared by two frames.  Stage record: a 64-byte header (word 0 =
+// rows, word 1 = the record's bytes; bytes 32..63 = edge-slot offsets eoff[0..15], u16:
+// edge slot j holds edge j of every row of degree > j, the stage's row t at eoff[j] + t),
+// the row words (u32: degree | class << 8) padded to 16 bytes, then the columns, u16 per
+// edge-slot entry, padded to 16.  Messages: u16 per edge-slot entry (the two frames'
+// bytes 128 - msg), same index.  Each frame stops on its own: when it does, its decisions
+// and count are written at once; its lane then keeps running beside the other frame (the
+// lanes never mix, so that changes nothing the frame wrote).
+
+constexpr int FRAME2_HEADER = 64;
+
+// One check row of two frames (fp16 lanes 0 and 1 = frames 2p, 2p+1): the reference's
+// per-byte update (CUDA_OMS_SIMD.cu:40-134) in the biased negated arithmetic of namespace
+// h2, one edge per word.  cp / mp: this row's entry of edge slot 0 of the columns / the
+// messages; eo: the edge-slot offsets (u16 pairs).  odd: odd rows of frame 0 | frame 1 << 16.
+template <int KIND, int D>
+__device__ __forceinline__ void frame2_row(uint16_t* app, const uint16_t* cp, uint16_t* mp, const uint32_t (&eo)[8],
+                                           bool first, bool noclip, uint32_t& odd, const uint16_t* lut)
+{
+    using namespace h2;
+    uint32_t bt[D];
+    int ci[D], ei[D];
+    uint32_t mn1 = C127, mn2 = C127;
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+        ei[j] = (int)((j & 1) ? (eo[j >> 1] >> 16) : (eo[j >> 1] & 0xffffu));
+        ci[j] = cp[ei[j]];
+    }
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+        // x bytes of the two frames; 127 - x as an unsigned byte is x ^ 0x7f
+        const uint32_t w = (uint32_t)app[ci[j]] ^ 0x7f7fu;
+        const uint32_t b = add(__byte_perm(w, 0x6464u, 0x5140), CNEG1024);
+        uint32_t u = 0;  // negated old messages
+        if (!first) u = add(__byte_perm((uint32_t)mp[ei[j]], 0x6464u, 0x5140), FRAME_CNEG1152);
+        bt[j] = hmin(fma_relu(u, NEG1, b), C255);
+        const uint32_t ut = add(bt[j], CNEG127);
+        const uint32_t mx = max_xs(ut, mn1);
+        mn1 = min_xs(mn1, ut);
+        mn2 = min_xs(mn2, mx);
+    }
+    const uint32_t a1 = habs(mn1), a2 = habs(mn2);
+    uint32_t c1, c2;
+    if (KIND == KIND_LEARNED) {
+        // the integer tables of the I8 packing, one lookup per frame: c1 = lut[min2], c2 = lut[min1]
+        const uint32_t i2 = add(a2, C1024), i1 = add(a1, C1024);
+        const uint32_t c1l = lut[i2 & 0x7fu], c1h = lut[(i2 >> 16) & 0x7fu];
+        const uint32_t c2l = lut[i1 & 0x7fu], c2h = lut[(i1 >> 16) & 0x7fu];
+        c1 = add(0x64006400u | c1l | (c1h << 16), CNEG1024);
+        c2 = add(0x64006400u | c2l | (c2h << 16), CNEG1024);
+    } else {
+        h2::mags<KIND>(a1, a2, noclip, c1, c2, 0u, 0u);
+    }
+    const uint32_t c1s = c1 | (mn1 & SIGN), c2s = c2 | (mn1 & SIGN);
+    const uint32_t dcs = sub(c2s, c1s), na1 = a1 ^ SIGN;
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+        const uint32_t ut = add(bt[j], CNEG127);
+        const uint32_t fl = add_sat(habs(ut), na1);  // 0.0 on minimum edges, 1.0 elsewhere
+        const uint32_t mo = fma(fl, dcs, c1s) ^ (ut & SIGN);
+        const uint32_t bn = add(hmin(fma_relu(mo, ONE, bt[j]), C255), C1024) ^ 0x007f007fu;  // x bytes 0, 2
+        app[ci[j]] = (uint16_t)__byte_perm(bn, 0, 0x0020);
+        mp[ei[j]] = (uint16_t)__byte_perm(add(mo, FRAME_C1152), 0, 0x0020);
+    }
+    odd += ((mn1 >> 15) & 1u) | ((mn1 >> 31) << 16);
+}
+
+template <int KIND, int DT, bool EXACT>
+__device__ __forceinline__ void frame2_row_any(int deg, uint16_t* app, const uint16_t* cp, uint16_t* mp,
+                                               const uint32_t (&eo)[8], bool first, bool noclip, uint32_t& odd,
+                                               const uint16_t* lut)
+{
+    if (EXACT) return frame2_row<KIND, DT>(app, cp, mp, eo, first, noclip, odd, lut);
+#define LDPC_FRAME2_CASE(D)                                                                           \
+    case D:                                                                                           \
+        if (D <= DT) frame2_row<KIND, (D <= DT ? D : DT)>(app, cp, mp, eo, first, noclip, odd, lut);  \
+        return;
+    switch (deg) {
+        LDPC_FRAME2_CASE(1) LDPC_FRAME2_CASE(2) LDPC_FRAME2_CASE(3) LDPC_FRAME2_CASE(4) LDPC_FRAME2_CASE(5)
+        LDPC_FRAME2_CASE(6) LDPC_FRAME2_CASE(7) LDPC_FRAME2_CASE(8) LDPC_FRAME2_CASE(9) LDPC_FRAME2_CASE(10)
+        LDPC_FRAME2_CASE(11) LDPC_FRAME2_CASE(12) LDPC_FRAME2_CASE(13) LDPC_FRAME2_CASE(14)
+    }
+#undef LDPC_FRAME2_CASE
+}
+
+// Byte k of the result is nonzero in some thread when frame k (lane k of the APP words) has
+// a check of odd hard-decision parity (x > 0 is bit 1)
+__device__ __forceinline__ uint32_t frame2_rows_odd(const uint16_t* app, const Plan& P)
+{
+    uint32_t bad = 0;
+    for (int r = threadIdx.x; r < P.m; r += blockDim.x) {
+        const int d = __ldg(P.rowdeg + r);
+        uint32_t acc = 0;
+        for (int j = 0; j < d; j++) acc ^= __vcmpgts4((uint32_t)app[__ldg(P.cols + j * P.m + r)], 0u);
+        bad |= acc;
+    }
+    return bad & 0xffffu;
+}
+
+// Persistent CTAs: CTA c decodes frame pairs c, c + G, ... (pair p = frames 2p, 2p + 1 of the
+// launch), with slot c of the message scratch.  Shared memory: the pair's APP (2 npad bytes),
+// for KIND_LEARNED the iteration's tables (512 bytes), then the ring.  The copy protocol is
+// decode_frame_kernel's.
+template <int KIND, int DT, bool EXACT, bool ET>
+__global__ void __maxnreg__(120) decode_frame2_kernel(const Plan P, const Job J, const FrameStages S, long long frames)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint16_t* app = reinterpret_cast<uint16_t*>(smem_raw);                   // [npad]
+    int8_t* app8 = reinterpret_cast<int8_t*>(smem_raw);                      // byte 2v + k: frame k
+    uint16_t* slut = reinterpret_cast<uint16_t*>(smem_raw + 2 * P.npad);     // KIND_LEARNED
+    unsigned char* ring = smem_raw + 2 * P.npad + (KIND == KIND_LEARNED ? 512 : 0);
+    const int slot_sz = S.slot_sz;
+    __shared__ __align__(8) unsigned long long bars[FRAME_RING];
+    __shared__ unsigned s_odd[2];
+    __shared__ int s_abort;
+    const bool producer = threadIdx.x == blockDim.x - 1;
+    const unsigned char* gmsg_c = S.msg + (long long)blockIdx.x * S.slot_bytes;
+    unsigned char* gmsg = S.msg + (long long)blockIdx.x * S.slot_bytes;
+    const int nst = S.nst;
+    const int pd = nst >= FRAME_RING ? 2 : 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < FRAME_RING; i++) mbar_init(&bars[i]);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned long long G0 = 0;
+    const long long pairs = frames >> 1;
+    for (long long lp = blockIdx.x; lp < pairs; lp += gridDim.x) {
+        const long long lf0 = 2 * lp, f0 = 4 * J.word0 + lf0;
+        const long long total = (long long)J.iters * nst;
+        if (threadIdx.x < 2) s_odd[threadIdx.x] = 0;
+        if (producer && pd)
+            for (int g = 0; g < pd && g < total; g++)
+                stage_load(S, S.st[g], ring + ((G0 + g) % FRAME_RING) * slot_sz, gmsg_c, false,
+                           &bars[(G0 + g) % FRAME_RING]);
+        long long issued = pd ? (total < pd ? total : pd) : 0;
+        read_frame(P, J, f0, [&](int v, int x) { app8[2 * v] = (int8_t)x; });
+        read_frame(P, J, f0 + 1, [&](int v, int x) { app8[2 * v + 1] = (int8_t)x; });
+        __syncthreads();
+
+        unsigned live = 3u;  // frames of the pair still decoding (the same in every thread)
+        int its[2] = {0, 0};
+        int executed = 0;
+        long long g = 0;
+        for (int it = 0; it < J.iters; it++) {
+            uint32_t odd = 0;
+            const bool first = it == 0;
+            if (KIND == KIND_LEARNED) load_iteration_lut(J, it, slut);
+            for (int l = 0; l < nst; l++, g++) {
+                const unsigned long long gg = G0 + g;
+                unsigned char* slot = ring + (gg % FRAME_RING) * slot_sz;
+                if (pd) {
+                    if (g + pd < total) {
+                        const long long gn = g + pd;
+                        if (producer) {
+                            asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");
+                            stage_load(S, S.st[gn % nst], ring + ((G0 + gn) % FRAME_RING) * slot_sz, gmsg_c,
+                                       gn >= nst, &bars[(G0 + gn) % FRAME_RING]);
+                        }
+                        issued = gn + 1;
+                    }
+                } else {
+                    if (producer) {
+                        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                        stage_load(S, S.st[l], slot, gmsg_c, !first, &bars[gg % FRAME_RING]);
+                    }
+                    issued = g + 1;
+                }
+                if (!mbar_wait(&bars[gg % FRAME_RING], (uint32_t)((gg / FRAME_RING) & 1))) s_abort = 1;
+                const int t = threadIdx.x;
+                const int2 hd = *reinterpret_cast<const int2*>(slot);  // rows, record bytes
+                if (t < hd.x) {
+                    const uint4 e0 = reinterpret_cast<const uint4*>(slot)[2], e1 = reinterpret_cast<const uint4*>(slot)[3];
+                    const uint32_t eo[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+                    const uint32_t rw = reinterpret_cast<const uint32_t*>(slot + FRAME2_HEADER)[t];
+                    const int cols_off = FRAME2_HEADER + (4 * hd.x + 15) / 16 * 16;
+                    const uint16_t* cp = reinterpret_cast<const uint16_t*>(slot + cols_off) + t;
+                    uint16_t* mp = reinterpret_cast<uint16_t*>(slot + hd.y) + t;
+                    const int cls = (int)(rw >> 8);
+                    const bool noclip = J.quirk && first && cls;
+                    frame2_row_any<KIND, DT, EXACT>((int)(rw & 0xffu), app, cp, mp, eo, first, noclip, odd,
+                                                    slut + 128 * cls);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (s_abort) break;
+                if (producer) {
+                    const FrameStage st = S.st[l];
+                    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gmsg + st.msg_off),
+                                 "r"(smem_u32(slot + st.rec_bytes)), "r"(st.msg_bytes)
+                                 : "memory");
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+            }
+            if (s_abort) break;
+            executed = it + 1;
+            if (ET) {
+                const unsigned tot = odd_rows_total(odd, it, s_odd);
+                unsigned gate = live & (((tot & 0xffffu) <= J.early_slack ? 1u : 0u) |
+                                        ((tot >> 16) <= J.early_slack ? 2u : 0u));
+                if (gate) {
+                    const uint32_t bad = frame2_rows_odd(app, P);
+                    if ((gate & 1u) && __syncthreads_or(bad & 0xffu)) gate &= ~1u;
+                    if ((gate & 2u) && __syncthreads_or(bad & 0xff00u)) gate &= ~2u;
+                    for (int k = 0; k < 2; k++) {
+                        if (!((gate >> k) & 1u)) continue;
+                        // frame k stops here: its decisions, its count, its syndrome flag
+                        write_frame(P, J, f0 + k, [&](int v) { return (int)app8[2 * v + k]; });
+                        its[k] = it + 1;
+                        if (threadIdx.x == 0) {
+                            if (J.iters_out) J.iters_out[lf0 + k] = it + 1;
+                            if (J.synd_out) J.synd_out[lf0 + k] = 1;
+                        }
+                    }
+                    live &= ~gate;
+                    if (!live) break;
+                    if (gate) __syncthreads();  // write_frame read the APP the next stage updates
+                }
+            }
+        }
+        for (long long q = g; q < issued; q++) {
+            const unsigned long long gg = G0 + q;
+            if (!mbar_wait(&bars[gg % FRAME_RING], (uint32_t)((gg / FRAME_RING) & 1))) s_abort = 1;
+        }
+        if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        G0 += issued;
+        __syncthreads();
+        if (s_abort) {
+            if (threadIdx.x == 0) atomicExch(S.status, 1);
+            return;
+        }
+        // the frames still live ran every iteration
+        uint32_t bad = 0;
+        if (live && J.synd_out) bad = frame2_rows_odd(app, P);
+        for (int k = 0; k < 2; k++) {
+            if (!((live >> k) & 1u)) continue;
+            write_frame(P, J, f0 + k, [&](int v) { return (int)app8[2 * v + k]; });
+            if (J.iters_out && threadIdx.x == 0) J.iters_out[lf0 + k] = executed;
+            if (J.synd_out) {
+                const int o = __syncthreads_or((bad >> (8 * k)) & 0xffu);
+                if (threadIdx.x == 0) J.synd_out[lf0 + k] = o ? 0 : 1;
+            }
+        }
+        (void)its;
+        __syncthreads();  // the APP is refilled by the next pair
+    }
+}
+
 }  // namespace ldpc

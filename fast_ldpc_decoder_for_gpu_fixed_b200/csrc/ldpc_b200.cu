@@ -111,6 +111,8 @@ struct ldpc_decoder {
     // 3 = one frame per CTA, 4 = QC register-message, 2 frames per CTA, 5 = QC register-message with
     // per-frame early stop and lane refill (persistent CTAs)
     int path = 0;
+    bool pf_levels = false;  // path 0 with the per-frame early stop (SIMD4; counts per frame)
+    bool frame2 = false;     // path 3 with two frames per CTA (decode_frame2_kernel)
     int sms = 0;  // paths 3 and 5: multiprocessors (grid size)
     // path 3 (frame_kernel.cuh): the stages of one iteration, their records, the message
     // scratch (fslots CTA slots) and the status word the kernel sets when a copy wait gave up
@@ -329,8 +331,13 @@ const void* kernel_table_i8(int kind, int variant);
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, int et, int wpt);
 const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
 const void* kernel_table_qc_split(int kind, int dt, int layers, int split, bool et);
+const void* kernel_table_simd4_pf(int kind, int variant);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
+const void* kernel_table_frame2(int kind, int variant, bool et);
+#ifndef LDPC_FRAME2_DEFAULT
+#define LDPC_FRAME2_DEFAULT 1
+#endif
 const void* kernel_table_flood(int kind, int variant);
 }
 
@@ -538,7 +545,9 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
 // on an SM where the frame allows it) and lays out their records and message offsets,
 // 16-byte aligned for the bulk copies (FrameStage in frame_kernel.cuh).  base_smem: the
 // kernel's shared memory before the ring (the APP and the learned tables).
-static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_smem)
+// two: the layout of decode_frame2_kernel (edge slots of u16 columns, a 64-byte header, one
+// CTA per SM with two frames' APP).
+static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_smem, bool two)
 {
     const int T = d->threads - 32;  // the last warp is the producer's
     auto pad16 = [](long long x) { return (x + 15) / 16 * 16; };
@@ -548,11 +557,14 @@ static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_s
     CUDA_TRY(cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     // a stage slot holds the header, the row words, the column pairs and the messages of
     // its rows: at least one row of the largest degree
-    const int np_max = (c->dmax + 1) / 2;
-    const long long slot_min = FRAME_STAGE_HEADER + 16 + pad16(4ll * np_max) + pad16(2ll * np_max);
+    // entries per row: pairs of edges (one frame), or edges (two frames); 4 bytes of columns
+    // per pair entry or 2 per edge entry, 2 bytes of messages per entry either way
+    const int hdr = two ? FRAME2_HEADER : FRAME_STAGE_HEADER, cb = two ? 2 : 4;
+    auto entries = [&](int dg) { return two ? dg : (dg + 1) / 2; };
+    const long long slot_min = hdr + 16 + pad16((long long)cb * entries(c->dmax)) + pad16(2ll * entries(c->dmax));
     const long long static_smem = 512;  // the kernel's static shared memory, rounded up
     long long slot_cap = 0;
-    for (int ctas = 2; ctas >= 1 && slot_cap < slot_min; ctas--) {
+    for (int ctas = two ? 1 : 2; ctas >= 1 && slot_cap < slot_min; ctas--) {
         const long long avail = (long long)(ctas == 1 ? smem_blk : smem_sm / ctas - reserved) - static_smem -
                                 (long long)base_smem;
         slot_cap = avail / FRAME_RING / 16 * 16;
@@ -564,23 +576,24 @@ static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_s
     long long moff = 0;
     int slot_max = 0;
     auto slot_bytes = [&](int rows, int pairs) {
-        return FRAME_STAGE_HEADER + pad16(4ll * rows) + pad16(4ll * pairs) + pad16(2ll * pairs);
+        return hdr + pad16(4ll * rows) + pad16((long long)cb * pairs) + pad16(2ll * pairs);
     };
     auto emit = [&](int r0, int rows) {
-        // pair slots: rows sorted by decreasing degree, so slot p is a prefix of the rows
-        int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0}, poff[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        // entry slots (pairs, or edges): rows sorted by decreasing degree, so slot p is a
+        // prefix of the rows
+        int cnt[16] = {0}, poff[16] = {0};
         for (int i = 0; i < rows; i++) {
             const int r = c->order[r0 + i], dg = c->row_ptr[r + 1] - c->row_ptr[r];
-            for (int p = 0; p < (dg + 1) / 2; p++) cnt[p]++;
+            for (int p = 0; p < entries(dg); p++) cnt[p]++;
         }
         int pairs = 0;
-        for (int p = 0; p < 8; p++) {
+        for (int p = 0; p < 16; p++) {
             poff[p] = pairs;
             pairs += cnt[p];
         }
         FrameStage s{};
-        const long long cols_off = FRAME_STAGE_HEADER + pad16(4ll * rows);
-        s.rec_bytes = (int)(cols_off + pad16(4ll * pairs));
+        const long long cols_off = hdr + pad16(4ll * rows);
+        s.rec_bytes = (int)(cols_off + pad16((long long)cb * pairs));
         s.msg_bytes = (int)pad16(2ll * pairs);
         s.rec_off = (int)rec.size();
         s.msg_off = (int)moff;
@@ -588,10 +601,14 @@ static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_s
         unsigned char* b = rec.data() + s.rec_off;
         reinterpret_cast<int32_t*>(b)[0] = rows;
         reinterpret_cast<int32_t*>(b)[1] = s.rec_bytes;
-        for (int p = 0; p < 8; p++) reinterpret_cast<uint16_t*>(b + 16)[p] = (uint16_t)poff[p];
+        for (int p = 0; p < (two ? 16 : 8); p++) reinterpret_cast<uint16_t*>(b + (two ? 32 : 16))[p] = (uint16_t)poff[p];
         for (int i = 0; i < rows; i++) {
             const int r = c->order[r0 + i], e0 = c->row_ptr[r], dg = c->row_ptr[r + 1] - e0;
-            reinterpret_cast<uint32_t*>(b + FRAME_STAGE_HEADER)[i] = (uint32_t)dg | (uint32_t)c->row_class[r] << 8;
+            reinterpret_cast<uint32_t*>(b + hdr)[i] = (uint32_t)dg | (uint32_t)c->row_class[r] << 8;
+            if (two) {
+                for (int j = 0; j < dg; j++) reinterpret_cast<uint16_t*>(b + cols_off)[poff[j] + i] = (uint16_t)c->cols[e0 + j];
+                continue;
+            }
             for (int p = 0; p < (dg + 1) / 2; p++) {
                 const uint32_t lo = (uint32_t)c->cols[e0 + 2 * p];
                 const uint32_t hi = 2 * p + 1 < dg ? (uint32_t)c->cols[e0 + 2 * p + 1] : 0u;  // odd degree: dummy
@@ -605,7 +622,7 @@ static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_s
     for (const int2& lv : c->levels) {
         int r0 = lv.x, rows = 0, pairs = 0;
         for (int i = lv.x; i < lv.x + lv.y; i++) {
-            const int r = c->order[i], np = (c->row_ptr[r + 1] - c->row_ptr[r] + 1) / 2;
+            const int r = c->order[i], np = entries(c->row_ptr[r + 1] - c->row_ptr[r]);
             if (rows > 0 && (rows == T || slot_bytes(rows + 1, pairs + np) > slot_cap)) {
                 emit(r0, rows);
                 r0 = i;
@@ -743,19 +760,31 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->threads = c->z * split;
     } else if (frame) {
         const int k = kind == LDPC_XMS ? LDPC_OMS : kind;  // KIND_* values equal LDPC_* values
-        d->kfn = kernel_table_frame(k, degree_variant(c), early);
-        d->kfn_alt = kernel_table_frame(k, degree_variant(c), !early);
         d->path = 3;
         d->pack = LDPC_PACK_FRAME;
         d->grid_mult = 4;
         // the rows of a stage, then one warp whose last thread issues the bulk copies
         d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32)) + 32;
-        rc = frame_stages_setup(d, c, frame_smem);
-        if (rc) {
-            decoder_free(d);
-            return rc;
+        // two frames per CTA where their APP and a stage ring fit (odd-row counts of a frame
+        // below 2^16), else one
+        d->frame2 = LDPC_FRAME2_DEFAULT && c->m < 65536 &&
+                    frame_stages_setup(d, c, frame_smem + (size_t)npad, true) == LDPC_OK;
+        if (!d->frame2) {
+            cudaFree(d->d_fst);
+            cudaFree(d->d_frec);
+            cudaFree(d->d_status);
+            d->d_fst = nullptr;
+            d->d_frec = nullptr;
+            d->d_status = nullptr;
+            rc = frame_stages_setup(d, c, frame_smem, false);
+            if (rc) {
+                decoder_free(d);
+                return rc;
+            }
         }
-        d->smem = (int)(frame_smem + (size_t)FRAME_RING * d->fst.slot_sz);
+        d->kfn = (d->frame2 ? kernel_table_frame2 : kernel_table_frame)(k, degree_variant(c), early);
+        d->kfn_alt = (d->frame2 ? kernel_table_frame2 : kernel_table_frame)(k, degree_variant(c), !early);
+        d->smem = (int)(frame_smem + (d->frame2 ? (size_t)npad : 0) + (size_t)FRAME_RING * d->fst.slot_sz);
         if (d->smem > smem_max) {
             decoder_free(d);
             return fail(LDPC_ERR_UNSUPPORTED, "LDPC_PACK_FRAME: the frame and its stage ring need %d B of shared "
@@ -795,7 +824,14 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     } else {
-        d->kfn = kernel_for(pack, kind, degree_variant(c));
+        if (per_frame) {
+            // the level kernel with the per-frame early stop: SIMD4 only (one frame per byte lane)
+            const int k = kind == LDPC_XMS ? LDPC_OMS : (kind == LDPC_LEARNED ? KIND_LEARNED : kind);
+            d->kfn = pack == LDPC_PACK_SIMD4 ? kernel_table_simd4_pf(k, degree_variant(c)) : nullptr;
+            d->pf_levels = d->kfn != nullptr;
+        } else {
+            d->kfn = kernel_for(pack, kind, degree_variant(c));
+        }
         d->smem = (int)smem;
         d->threads = std::min(256, std::max(32, (c->widest + 31) / 32 * 32));
     }
@@ -803,10 +839,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         decoder_free(d);
         return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_PAIRS: needs a QC register kernel (decoder path 1 or 4)");
     }
-    if (per_frame && d->path != 3 && d->path != 5) {
+    if (per_frame && d->path != 3 && d->path != 5 && !d->pf_levels) {
         decoder_free(d);
-        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_FRAMES: needs the QC register kernel with 4 frames per "
-                                          "CTA (the regular 8x16 base, Z a power of two) or LDPC_PACK_FRAME");
+        return fail(LDPC_ERR_UNSUPPORTED, "LDPC_FLAG_EARLY_STOP_FRAMES: needs the level kernel with LDPC_PACK_SIMD4 "
+                                          "(or AUTO), the QC register kernel with 4 frames per CTA (the regular 8x16 "
+                                          "base, Z a power of two) or LDPC_PACK_FRAME");
     }
     if (d->path == 5 || d->path == 3) {
         cudaError_t ec = cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -864,6 +901,9 @@ extern "C" int ldpc_decoder_set_early_stop(ldpc_decoder* d, int enabled, int sla
     if (enabled && d->path == 2)
         return fail(LDPC_ERR_ARG, "early stop needs a decoder created with LDPC_FLAG_EARLY_STOP for this packing");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_decoder_set_early_stop: slack must be >= 0");
+    if (!enabled && d->pf_levels)
+        return fail(LDPC_ERR_ARG, "the per-frame early stop of this decoder cannot be turned off; create one "
+                                  "without LDPC_FLAG_EARLY_STOP_FRAMES");
     if ((d->path == 1 || d->path == 3 || d->path == 4 || d->path == 7) && (enabled != 0) != d->early)
         std::swap(d->kfn, d->kfn_alt);
     d->early = enabled != 0;
@@ -1008,7 +1048,7 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
     if (d->path == 3) {
         // persistent CTAs, one message-scratch slot each
         long long frames = 4 * words;
-        const long long grid = std::min(frames, d->fslots);
+        const long long grid = std::min(d->frame2 ? frames / 2 : frames, d->fslots);
         void* a[] = {(void*)&d->plan, (void*)&J, (void*)&d->fst, (void*)&frames};
         CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
         return LDPC_OK;
@@ -1044,7 +1084,7 @@ extern "C" int ldpc_decode_device_state(ldpc_decoder* d, const int8_t* d_llr, ui
 {
     int rc = check_decode_args(d, d_llr, d_hard, n_words, iters);
     if (rc) return rc;
-    if (d->path >= 3 && d->path != 6 && (d_app || d_msg))  // paths 3, 4, 5, 7
+    if (((d->path >= 3 && d->path != 6) || d->pf_levels) && (d_app || d_msg))  // paths 3, 4, 5, 7, per-frame 0
         return fail(LDPC_ERR_UNSUPPORTED, "this decoder (path %d) has no state dumps", d->path);
     CUDA_TRY(cudaSetDevice(d->device));
     return launch(d, d_llr, d_hard, 0, 0, (long long)n_words, (long long)n_words, iters, d_iters_out, d_app, d_msg,
@@ -1093,7 +1133,7 @@ static int decode_host_impl(ldpc_decoder* d, const int8_t* llr, void* out, int i
     CUDA_TRY(cudaSetDevice(d->device));
     const size_t W = d->nb_words, fb = 4 * (size_t)d->n;  // LLR bytes per word-group of frames
     const size_t ob = out_format == LDPC_OUT_PACKED ? 4 * (size_t)((d->n + 7) / 8) : fb;  // output bytes per word
-    const size_t ipw = (d->path == 3 || d->path == 5) ? 4 : 1;  // iteration counts per word
+    const size_t ipw = (d->path == 3 || d->path == 5 || d->pf_levels) ? 4 : 1;  // iteration counts per word
     if (!d->d_in) {
         CUDA_TRY(cudaMalloc(&d->d_in, W * fb));
         CUDA_TRY(cudaMalloc(&d->d_out, W * fb));
@@ -1275,6 +1315,7 @@ extern "C" int ldpc_probe_int_peak(double* lane_ops_per_s, void* stream)
 
 namespace ldpc {
 const void* kernel_table_batch(int pack, int kind, int variant);
+const void* kernel_table_batch_pf(int kind, int variant);
 size_t batch_code_bytes();
 void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, int32_t* iters_out, uint8_t* synd_out,
                      long long words, long long first_item, int quirk, int out_packed, int variant);
@@ -1283,6 +1324,7 @@ void batch_code_fill(void* rec, const Plan& plan, const int8_t* llr, void* out, 
 struct ldpc_batch {
     int kind = 0, device = 0, pack = LDPC_PACK_SIMD4, variant = 0;
     bool early = false, use_graph = false;
+    bool per_frame = false;  // LDPC_FLAG_EARLY_STOP_FRAMES: iteration counts per frame
     unsigned slack = LDPC_EARLY_STOP_DEFAULT_SLACK;
     std::vector<ldpc_decoder*> plans;  // each code's tables and schedule (decoder_setup)
     std::vector<int> cls;              // degree class of each code: 0 <= 8, 1 <= 16, 2 <= 32
@@ -1388,7 +1430,8 @@ static int batch_code_decoder(ldpc_batch* b, int i, int cand, ldpc_decoder** out
         const bool qc_cand = cand == CAND_QC || cand == CAND_QC_SPLIT;
         if (!qc_cand) c.qc = false;  // the level kernels, also for a QC code
         else if (!c.qc) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d is not quasi-cyclic", i);
-        const int flags = (b->early ? LDPC_FLAG_EARLY_STOP : 0) | (cand == CAND_FLOOD ? LDPC_FLAG_FLOODING : 0);
+        const int flags = (b->per_frame ? LDPC_FLAG_EARLY_STOP_FRAMES : (b->early ? LDPC_FLAG_EARLY_STOP : 0)) |
+                          (cand == CAND_FLOOD ? LDPC_FLAG_FLOODING : 0);
         // nb_frames only bounds the words of a call; the batch passes its own counts
         int rc = ldpc_decoder_create(&d, &c, b->kind, (size_t)1 << 40, pack, flags);
         if (rc) return rc;
@@ -1437,8 +1480,11 @@ static int batch_configure(ldpc_batch* b, int pack, int threads, int ctas_per_sm
         return LDPC_OK;
     }
     const int k = b->kind == LDPC_LEARNED ? 4 : b->kind;
-    const void* kfn = kernel_table_batch(pack, k, b->variant);
-    if (!kfn) return fail(LDPC_ERR_UNSUPPORTED, "batch: no kernel for pack %d", pack);
+    const void* kfn = b->per_frame ? (pack == LDPC_PACK_SIMD4 ? kernel_table_batch_pf(b->kind, b->variant) : nullptr)
+                                   : kernel_table_batch(pack, k, b->variant);
+    if (!kfn)
+        return fail(LDPC_ERR_UNSUPPORTED, "batch: no kernel for pack %d%s", pack,
+                    b->per_frame ? " with the per-frame early stop (SIMD4 only)" : "");
     const size_t smem = batch_smem(b, pack);
     if (smem > (size_t)smem_max)
         return fail(LDPC_ERR_UNSUPPORTED, "batch: the largest code needs %zu B of shared memory with pack %d", smem, pack);
@@ -1465,8 +1511,9 @@ extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes
     if (!out || !codes || n_codes < 1) return fail(LDPC_ERR_ARG, "ldpc_batch_create: no codes");
     if (kind < LDPC_MS || kind > LDPC_LEARNED || kind == LDPC_XMS)
         return fail(LDPC_ERR_ARG, "ldpc_batch_create: kind %d (xMS reads interleaved input; use OMS)", kind);
-    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_BATCH_GRAPH)) return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
-    if ((flags & LDPC_FLAG_EARLY_STOP) && kind == LDPC_2NMS)
+    if (flags & ~(LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES | LDPC_BATCH_GRAPH))
+        return fail(LDPC_ERR_ARG, "unknown flags 0x%x", flags);
+    if ((flags & (LDPC_FLAG_EARLY_STOP | LDPC_FLAG_EARLY_STOP_FRAMES)) && kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     if (pack != LDPC_PACK_AUTO && (pack < LDPC_PACK_SIMD4 || pack > LDPC_PACK_I8))
         return fail(LDPC_ERR_ARG, "ldpc_batch_create: pack %d (SIMD4, F16X2, I8 or AUTO)", pack);
@@ -1478,7 +1525,8 @@ extern "C" int ldpc_batch_create(ldpc_batch** out, const ldpc_code* const* codes
     if (dmax > kMaxDegree) return fail(LDPC_ERR_UNSUPPORTED, "row degree %d > %d", dmax, kMaxDegree);
     ldpc_batch* b = new ldpc_batch();
     b->kind = kind;
-    b->early = flags & LDPC_FLAG_EARLY_STOP;
+    b->per_frame = flags & LDPC_FLAG_EARLY_STOP_FRAMES;
+    b->early = (flags & LDPC_FLAG_EARLY_STOP) || b->per_frame;
     b->use_graph = flags & LDPC_BATCH_GRAPH;
     b->variant = dmax <= 8 ? 0 : (dmax <= 16 ? 1 : 2);
     cudaError_t e = cudaGetDevice(&b->device);
@@ -1562,6 +1610,9 @@ extern "C" int ldpc_batch_set_early_stop(ldpc_batch* b, int enabled, int slack)
     if (enabled && b->kind == LDPC_2NMS)
         return fail(LDPC_ERR_ARG, "LDPC_FLAG_EARLY_STOP: LDPC_2NMS has the reference's own early termination");
     if (slack < 0) return fail(LDPC_ERR_ARG, "ldpc_batch_set_early_stop: slack must be >= 0");
+    if (!enabled && b->per_frame)
+        return fail(LDPC_ERR_ARG, "the per-frame early stop of this batch cannot be turned off; create one without "
+                                  "LDPC_FLAG_EARLY_STOP_FRAMES");
     if (b->early != (enabled != 0)) batch_drop_decoders(b);  // per-code decoders: re-created with the flag
     b->early = enabled != 0;
     b->slack = (unsigned)slack;

@@ -218,7 +218,11 @@ class Batch:
         self.kind = kind.upper()
         arr = (ctypes.c_void_p * len(codes))(*[nc.handle.value for nc in self.natives])
         h = ctypes.c_void_p()
-        flags = (_lib.FLAG_EARLY_STOP if early_stop else 0) | (_lib.BATCH_GRAPH if graph else 0)
+        if early_stop == "frame":
+            flags = _lib.FLAG_EARLY_STOP_FRAMES
+        else:
+            flags = _lib.FLAG_EARLY_STOP if early_stop else 0
+        flags |= _lib.BATCH_GRAPH if graph else 0
         _lib.check(_lib.lib().ldpc_batch_create(ctypes.byref(h), arr, len(codes), _lib.KINDS[self.kind],
                                                 _lib.PACKS[pack.upper()], flags))
         self.handle = h

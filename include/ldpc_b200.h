@@ -144,14 +144,16 @@ void ldpc_code_destroy(ldpc_code* code);
 #define LDPC_EARLY_STOP_DEFAULT_SLACK 128
 
 /* Per-frame early stop (implies LDPC_FLAG_EARLY_STOP): the rule above applied to
- * each frame alone (its own odd rows against `slack`, its own syndrome), and a
- * frame that stops frees its slot for the next frame.  Decoder path 5: the QC
- * register kernel with 4 frames per CTA (ldpc_code_create_qc, the regular 8x16
- * base with Z a power of two, every kind but 2NMS) run as persistent CTAs that
- * refill finished frame slots with prefetched frames; with LDPC_PACK_FRAME (path 3)
- * it is that path's own rule.  Other decoders fail with LDPC_ERR_UNSUPPORTED.  On
- * path 5: d_iters_out receives one count per frame (4*n_words entries), iters <= 255,
- * no state dumps and no ldpc_simulate. */
+ * each frame alone (its own odd rows against `slack`, its own syndrome).  Decoder
+ * path 5: the QC register kernel with 4 frames per CTA (ldpc_code_create_qc, the
+ * regular 8x16 base with Z a power of two, every kind but 2NMS) run as persistent CTAs
+ * that refill a finished frame's slot with a prefetched frame; with LDPC_PACK_FRAME
+ * (path 3) it is that path's own rule; on the level kernel with LDPC_PACK_SIMD4 (path 0,
+ * what LDPC_PACK_AUTO gives a code without a QC register kernel) a frame that stops has
+ * its decisions written at once while the other frames of its word go on.  Other
+ * decoders fail with LDPC_ERR_UNSUPPORTED.  d_iters_out then receives one count per
+ * frame (4*n_words entries); no state dumps; on path 5 iters <= 255 and no
+ * ldpc_simulate.  The early stop of such a decoder cannot be turned off. */
 #define LDPC_FLAG_EARLY_STOP_FRAMES 4
 
 /* Flooding schedule (no reference counterpart; the reference is row-layered): every
@@ -335,7 +337,10 @@ int ldpc_decoder_status(ldpc_decoder* dec, int* status);
  * those of ldpc_decoder_create with the same kind and pack (level schedule).
  * kind: any but LDPC_XMS; pack: LDPC_PACK_SIMD4 / F16X2 / I8, or AUTO (the
  * smallest state that fits; ldpc_batch_autotune then picks the fastest).
- * flags: LDPC_FLAG_EARLY_STOP, LDPC_BATCH_GRAPH (launches captured once in a CUDA
+ * flags: LDPC_FLAG_EARLY_STOP, LDPC_FLAG_EARLY_STOP_FRAMES (each frame stops on its own:
+ * the persistent kernel with LDPC_PACK_SIMD4, and per code the SIMD4 level kernel or the
+ * QC refill kernel; d_iters_out then holds one count per frame, 4*n_words[i] entries per
+ * code), LDPC_BATCH_GRAPH (launches captured once in a CUDA
  * graph and replayed while buffers, sizes and settings stay the same; needs a
  * stream other than the legacy default stream).  The codes may be destroyed
  * after this call. */

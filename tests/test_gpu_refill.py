@@ -144,10 +144,15 @@ def test_refill_flag_errors(cuda):
     code = qc(256)
     with pytest.raises(LdpcError):
         Decoder(code, "2NMS", nb_frames=8, early_stop="frame")     # 2NMS keeps its own rule
+    # without the QC refill kernel (or with an explicit SIMD4) the per-frame stop runs on the
+    # SIMD4 level kernel (tests/test_gpu_frames_levels.py); F16X2 level kernels refuse it
+    for c, pack in ((load_table("4000x2000"), "AUTO"), (code, "SIMD4")):
+        d = Decoder(c, "OMS", nb_frames=8, pack=pack, early_stop="frame")
+        assert d.info()["path"] == 0
+        d.close()
+    c = load_table("4000x2000")
     with pytest.raises(LdpcError):
-        Decoder(load_table("4000x2000"), "OMS", nb_frames=8, early_stop="frame")  # no QC kernel
-    with pytest.raises(LdpcError):
-        Decoder(code, "OMS", nb_frames=8, pack="SIMD4", early_stop="frame")       # level kernel
+        Decoder(c, "OMS", nb_frames=8, pack="F16X2", early_stop="frame")
     dec = Decoder(code, "OMS", nb_frames=8, early_stop="frame")
     d_llr = torch.zeros(32 * code.n, dtype=torch.int8, device="cuda")
     d_out = torch.zeros(32 * code.n, dtype=torch.uint8, device="cuda")
