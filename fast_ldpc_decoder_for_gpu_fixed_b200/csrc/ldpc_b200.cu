@@ -335,9 +335,6 @@ const void* kernel_table_simd4_pf(int kind, int variant);
 const void* kernel_table_f16x2h(int kind, int variant);
 const void* kernel_table_frame(int kind, int variant, bool et);
 const void* kernel_table_frame2(int kind, int variant, bool et);
-#ifndef LDPC_FRAME2_DEFAULT
-#define LDPC_FRAME2_DEFAULT 1
-#endif
 const void* kernel_table_flood(int kind, int variant);
 }
 
@@ -549,7 +546,7 @@ static int decoder_setup(ldpc_decoder* d, const ldpc_code* c)
 // CTA per SM with two frames' APP).
 static int frame_stages_setup(ldpc_decoder* d, const ldpc_code* c, size_t base_smem, bool two)
 {
-    const int T = d->threads - 32;  // the last warp is the producer's
+    const int T = d->threads - 32;  // rows per stage; the last warp is the producer's
     auto pad16 = [](long long x) { return (x + 15) / 16 * 16; };
     int smem_sm = 0, reserved = 0, smem_blk = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d->device));
@@ -763,11 +760,11 @@ extern "C" int ldpc_decoder_create(ldpc_decoder** out, const ldpc_code* c, int k
         d->path = 3;
         d->pack = LDPC_PACK_FRAME;
         d->grid_mult = 4;
-        // the rows of a stage, then one warp whose last thread issues the bulk copies
+        // the rows of a stage, then one warp whose last thread issues the bulk copies; two
+        // frames per CTA where their APP and a stage ring fit (odd-row counts of a frame below
+        // 2^16), else one
         d->threads = std::min(FRAME_MAX_THREADS, std::max(32, (c->widest + 31) / 32 * 32)) + 32;
-        // two frames per CTA where their APP and a stage ring fit (odd-row counts of a frame
-        // below 2^16), else one
-        d->frame2 = LDPC_FRAME2_DEFAULT && c->m < 65536 &&
+        d->frame2 = c->m < 65536 &&
                     frame_stages_setup(d, c, frame_smem + (size_t)npad, true) == LDPC_OK;
         if (!d->frame2) {
             cudaFree(d->d_fst);

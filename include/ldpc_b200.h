@@ -70,11 +70,11 @@ extern "C" {
  * 4g+2, 4g+3) on its own and reports per word the larger of its two pairs' counts. */
 #define LDPC_PACK_F16X2 1
 #define LDPC_PACK_I8 2    /* 1 frame per thread lane, int8 storage, int32 math    */
-/* 1 frame per CTA: the frame's APP as int8 in shared memory (N bytes, two CTAs per
- * SM at N = 64800) and its c->v messages, one byte per edge (plus one per odd row
- * degree), in a message scratch the decoder allocates in device memory, one slot per
- * resident CTA (about 64 MB for N = 64800 rate 1/2 on 148 SMs); row records and
- * messages reach shared memory by bulk copies a stage ahead of their use.
+/* 2 frames per CTA (1 where two do not fit): the frames' APP as int8 in shared memory
+ * (2N bytes, one CTA per SM at N = 64800) and their c->v messages, one byte per edge and
+ * frame, in a message scratch the decoder allocates in device memory, one slot per
+ * resident CTA (about 58 MB for N = 64800 rate 1/2 on 148 SMs); row records and
+ * messages reach shared memory by bulk copies two stages ahead of their use.
  * For long codes whose 4-frame state exceeds shared memory.  Row degree <= 14.
  * LDPC_PACK_AUTO falls back to it when nothing else fits.  Not for LDPC_2NMS
  * (whose early termination is per 4-frame word).  With LDPC_FLAG_EARLY_STOP each
