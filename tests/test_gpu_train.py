@@ -108,7 +108,7 @@ def test_training_gains_over_plain_min_sum(cuda):
     decoder without a learned correction), quantisation-aware training on
     channel frames finds constants whose FER at 2.0 dB is a small fraction of
     min-sum's and close to hand-tuned OMS (offset 1), the reference's best
-    plain decoder, which stays the judge of FER."""
+    plain decoder, which stays the yardstick of FER."""
     from fast_ldpc_decoder_for_gpu_fixed_b200.learned import Trainer, evaluate
     code = qc_regular(z=256, mb=8, nb=16, wc=3, seed=2024, name="qc3x6_z256")
     tr = Trainer(code, iters=10, batch=2048, sub=512, lr=0.01, seed=3, weights="all", init_alpha=1.0,
