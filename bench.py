@@ -502,7 +502,8 @@ def main():
 
     # roofline of the decode kernel (one launch per step), from the iterations it executed
     int_peak = _int_peak()
-    one_lane = info["path"] == 3  # one frame per thread lane: one int32 op per frame-edge-update
+    # the algorithmic work of an edge-update (one frame, one edge, one iteration) is 8 int8
+    # lane-ops, i.e. 2 int32 word-ops at 4 lanes per word, whatever the packing of the kernel
     pair_iters = None
     if per_frame:
         edge_updates = float(d_its.sum().item()) * code.e
@@ -516,7 +517,7 @@ def main():
         edge_updates = float(pair_iters.sum().item()) * 2 * code.e
     else:
         edge_updates = float(d_its.sum().item()) * 4 * code.e if early else float(args.frames) * code.e * args.iters
-    alg_ops = (1.0 if one_lane else 2.0) * edge_updates
+    alg_ops = 2.0 * edge_updates
     achieved = alg_ops / (ms_step * 1e-3) / 1e12
     hbm_bytes = args.frames * code.n * 2  # int8 LLRs in + 0/1 bytes out
     peaks = _measured_peaks()
@@ -564,7 +565,7 @@ def main():
                          "peak_nominal": NOMINAL_INT_TOPS, "frac_nominal": achieved / NOMINAL_INT_TOPS,
                          "alg_ops_per_launch": alg_ops, "edge_updates_per_launch": edge_updates,
                          "mean_pair_iterations": float(pair_iters.float().mean()) if pair_iters is not None else None,
-                         "ops_per_edge_update": 1.0 if one_lane else 2.0,
+                         "ops_per_edge_update": 2.0,
                          "peak_source": "ldpc_probe_int_peak: best measured int32 lane-op rate (LOP3/IADD3 chains, "
                                         "all SMs; profiles/int_peak.md); peak_nominal: 148 SMs x 128 lanes x 1.965 GHz"},
             "roofline_hbm": {"achieved": hbm_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
