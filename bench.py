@@ -536,8 +536,9 @@ def main():
 
     if rank == 0:
         kernel = {0: "level_scheduled", 1: "qc_register_messages", 2: "level_scheduled_2f",
-                  3: "frame_per_cta_packed_rows", 4: "qc_register_messages_2f",
-                  5: "qc_register_messages_per_frame_refill"}[info["path"]]
+                  3: "long_code_tma_staged_rows", 4: "qc_register_messages_2f",
+                  5: "qc_register_messages_per_frame_refill", 6: "level_scheduled_flooding",
+                  7: "qc_register_messages_2f_split_rows"}[info["path"]]
         workload = workload_name(args)
         line = {
             "metric": "decoded info Gbit/s", "value": value, "unit": "Gbit/s", "n_gpus": world,
