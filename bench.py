@@ -59,7 +59,9 @@ def parse():
     ap.add_argument("--pack", default="AUTO")
     ap.add_argument("--ebn0", type=float, default=None, help="default 2.25 dB (learned), 2.0 (oms, table), 1.4 (ira)")
     ap.add_argument("--workload", default="learned", choices=["learned", "oms", "ira", "batch"])
-    ap.add_argument("--slack", type=int, default=None, help="early-stop slack (default: the library's)")
+    ap.add_argument("--slack", default=None,
+                    help="early-stop slack: an integer or 'any' (LDPC_EARLY_SLACK_ANY: every iteration a "
+                         "candidate; default: the library's)")
     ap.add_argument("--per-frame", action="store_true",
                     help="early stop per frame with slot refill (LDPC_FLAG_EARLY_STOP_FRAMES); same as --early-unit frame")
     ap.add_argument("--early-unit", default="word", choices=["word", "pairs", "frame"],
@@ -78,6 +80,10 @@ def parse():
     a = ap.parse_args()
     if a.table:
         a.workload = "oms"
+    if a.slack is None and a.workload == "learned":
+        a.slack = "any"  # the deployed decoder: every iteration a stop candidate (exact last-layer gate)
+    if a.slack is not None:
+        a.slack = (1 << 30) if str(a.slack).lower() == "any" else int(a.slack)
     if a.per_frame:
         a.early_unit = "frame"
     if a.ebn0 is None:
@@ -485,9 +491,10 @@ def main():
     # equal-FER evidence on more frames (untimed)
     fer_cmp = None
     if learned and rank == 0 and args.fer_frames > 0:
-        fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=es)
+        fl = evaluate(code, "LEARNED", args.iters, args.ebn0, args.fer_frames, constants=constants, early_stop=es,
+                      slack=args.slack)
         fp = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames)
-        fe = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames, early_stop=es)
+        fe = evaluate(code, "OMS", args.iters, args.ebn0, args.fer_frames, early_stop=es, slack=args.slack)
         fer_cmp = {"frames": fl["frames"], "ebn0_db": args.ebn0,
                    "learned_early_stop": {"fer": fl["fer"], "frame_errors": fl["frame_errors"], "ber": fl["ber"],
                                           "mean_iters": fl["mean_iters"]},
@@ -618,7 +625,11 @@ def _early_mode(args):
 def _early_name(args, per_frame):
     if per_frame:
         return "per_frame"
-    return "per_pair" if _early_mode(args) == "pairs" else "per_word"
+    unit = "per_pair" if _early_mode(args) == "pairs" else "per_word"
+    if args.slack is None:
+        return unit
+    # slack >= LDPC_EARLY_SLACK_ANY: every iteration a stop candidate
+    return unit + (", every iteration a candidate" if args.slack >= (1 << 30) else ", slack %d" % args.slack)
 
 
 def _sweep(code, constants, args, stream):
@@ -635,6 +646,8 @@ def _sweep(code, constants, args, stream):
     its = torch.zeros(4 * words if es == "frame" else words, dtype=torch.int32, device="cuda")
     ldec = Decoder(code, "LEARNED", nb_frames=words, early_stop=es)
     ldec.set_learned(*constants)
+    if args.slack is not None:
+        ldec.set_early_stop(True, args.slack)
     pdec = Decoder(code, "OMS", nb_frames=words)
     rows = []
     for e in (1.5, 1.75, 2.0, 2.25, 2.5):
@@ -648,7 +661,8 @@ def _sweep(code, constants, args, stream):
                 st()
             ms = _timed(st, 10, stream, False) / 10
             r = evaluate(code, "LEARNED" if d_its is not None else "OMS", args.iters, e, 1 << 18,
-                         constants=constants if d_its is not None else None, early_stop=es if d_its is not None else False)
+                         constants=constants if d_its is not None else None, early_stop=es if d_its is not None else False,
+                         slack=args.slack)
             row[name] = {"gbps": 4 * words * code.n_info / (ms * 1e-3) / 1e9, "fer": r["fer"],
                          "frame_errors": r["frame_errors"], "mean_iters": r["mean_iters"]}
         row["ratio"] = row["learned_early_stop"]["gbps"] / row["plain_oms"]["gbps"]

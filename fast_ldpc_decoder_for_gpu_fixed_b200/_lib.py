@@ -21,6 +21,7 @@ FLAG_FLOODING = 8
 FLAG_EARLY_STOP_PAIRS = 16
 BATCH_GRAPH = 2
 EARLY_STOP_DEFAULT_SLACK = 128
+EARLY_SLACK_ANY = 1 << 30
 TRAIN_QUANTIZED, TRAIN_FRAME_LOSS = 1, 2
 
 # every entry point declared in include/ldpc_b200.h: name -> (restype, argtypes)

@@ -26,12 +26,24 @@ def _stale(target, deps):
     return not os.path.exists(target) or any(os.path.getmtime(p) > os.path.getmtime(target) for p in deps)
 
 
+def _local_deps(path, seen=None):
+    """The file and every local header it includes (#include "..."), recursively."""
+    import re
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for inc in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), re.M):
+            _local_deps(os.path.join(os.path.dirname(path), inc), seen)
+    return seen
+
+
 def build_lib(force=False, verbose=False):
-    """Compiles every csrc/*.cu to an object (in parallel), then links the shared library."""
-    headers = _sources(CSRC, (".cuh", ".h")) + [os.path.join(ROOT, "include", "ldpc_b200.h")]
+    """Compiles every csrc/*.cu to an object (in parallel), then links the shared library.
+    A unit is recompiled when it or a local header it includes is newer than its object."""
     units = _sources(CSRC, (".cu",))
-    if not (force or _stale(LIB, headers + units)):
-        return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     base = [NVCC, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH,
@@ -42,12 +54,13 @@ def build_lib(force=False, verbose=False):
     for u in units:
         obj = os.path.join(objdir, os.path.basename(u)[:-3] + ".o")
         objs.append(obj)
-        if force or _stale(obj, headers + [u]):
+        if force or _stale(obj, sorted(_local_deps(u))):
             procs.append((u, subprocess.Popen(base + ["-c", "-o", obj, u])))
     for u, p in procs:
         if p.wait() != 0:
             raise RuntimeError("nvcc failed on %s" % u)
-    subprocess.check_call([NVCC, "-shared", *ARCH, "-o", LIB] + objs)
+    if procs or _stale(LIB, objs):
+        subprocess.check_call([NVCC, "-shared", *ARCH, "-o", LIB] + objs)
     return LIB
 
 

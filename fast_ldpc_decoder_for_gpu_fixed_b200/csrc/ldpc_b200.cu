@@ -330,6 +330,7 @@ const void* kernel_table_f16x2(int kind, int variant);
 const void* kernel_table_i8(int kind, int variant);
 const void* kernel_table_qc(int kind, int dt, bool exact, int layers, bool pow2, int et, int wpt);
 const void* kernel_table_qc_refill(int kind, int dt, bool exact, int layers, bool pow2);
+const void* kernel_qc_exact_of(const void* f);
 const void* kernel_table_qc_split(int kind, int dt, int layers, int split, bool et);
 const void* kernel_table_simd4_pf(int kind, int variant);
 const void* kernel_table_f16x2h(int kind, int variant);
@@ -1050,8 +1051,16 @@ static int launch(ldpc_decoder* d, const int8_t* llr, void* out, int out_packed,
         CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)grid), dim3(d->threads), a, d->smem, st));
         return LDPC_OK;
     }
+    const void* kfn = d->kfn;
+    if (d->path == 1 && d->early && d->early_slack >= LDPC_EARLY_SLACK_ANY) {
+        // every iteration a candidate: the 4-frame QC kernel's exact-gate twin, where it has one
+        if (const void* x = kernel_qc_exact_of(kfn)) {
+            if (d->smem > 48 * 1024) CUDA_TRY(ldpc_internal_raise_smem(x, d->smem));
+            kfn = x;
+        }
+    }
     void* args[] = {(d->path == 1 || d->path == 4 || d->path == 7) ? (void*)&d->qcp : (void*)&d->plan, (void*)&J};
-    CUDA_TRY(cudaLaunchKernel(d->kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
+    CUDA_TRY(cudaLaunchKernel(kfn, dim3((unsigned)(words * d->grid_mult)), dim3(d->threads), args, d->smem, st));
     return LDPC_OK;
 }
 

@@ -121,10 +121,17 @@ __device__ __noinline__ unsigned qc_rows_unsat_mask(const QCParams& Q, const cha
 // word) stops on its own: a stopped pair's rows are no longer updated and its APP stays
 // as it was, and the word reports the larger of its pairs' counts.  Without it the
 // extrinsic-parity count is dead code for every kind but 2NMS.
+// 3 = the CTA's frames stop together at the first iteration whose hard decisions are
+// codewords (the rule of modes 1 and 2 with an unbounded slack, LDPC_EARLY_SLACK_ANY).
+// No odd-row count: the rows of the last layer are checked from the registers that hold
+// their freshly updated APP (no later layer of the iteration touches those variables, so
+// their parity is final), reduced by the barrier that closes the layer; only when every
+// one of them holds are the other layers' rows checked from shared memory.
 template <int KIND, int DT, bool EXACT, int L, bool POW2, int ET, int WPT>
 __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const __grid_constant__ QCParams Q, const Job J)
 {
     static_assert(ET != 2 || WPT == 2, "per-pair early stop: 4 frames per CTA");
+    static_assert(ET != 3 || KIND != KIND_2NMS, "2NMS has its own early termination");
     constexpr bool PAIRS = ET == 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* app = reinterpret_cast<uint2*>(smem_raw);     // WPT = 2: [n] (pair-word 0, pair-word 1)
@@ -147,7 +154,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     }
     // the odd-row count of the early stop: a +-1 accumulator on the FMA pipe (row(), CMODE 2);
     // 2NMS keeps the exact popcount, which its own rule tests against zero
-    constexpr int CM = (ET && KIND != KIND_2NMS) ? 2 : 0;
+    constexpr int CM = ((ET == 1 || ET == 2) && KIND != KIND_2NMS) ? 2 : 0;
 
     Plan P;  // only n is used by the shared prologue / epilogue helpers
     P.n = Q.n;
@@ -171,6 +178,7 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     bool passed = false;  // stopped by the syndrome early stop: every check of every frame holds
     unsigned live = 3;    // PAIRS: bit p set while pair p is decoding (the same in every thread)
     for (int it = 0; it < J.iters; it++) {
+        bool last_ok = false;  // ET 3: every row of the last layer holds in every frame
         uint32_t ov = 0, ov1 = 0;  // PAIRS: ov1 is pair 1's odd-row accumulator
         const int lt = LRN ? min(it, J.lut_its - 1) : 0;  // constants of this iteration
 #pragma unroll
@@ -216,8 +224,21 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                         *reinterpret_cast<uint32_t*>(appb + off[j]) = b0[j];
                 }
             }
-            // with the early stop, the barrier of the odd-row count closes the last layer
-            if (!(ET && KIND != KIND_2NMS && l == L - 1)) __syncthreads();
+            if (ET == 3 && l == L - 1) {
+                // the parity of row k of the last layer in each frame, from the updated APP
+                uint32_t p0 = 0, p1 = 0;
+#pragma unroll
+                for (int j = 0; j < DT; j++) {
+                    if (EXACT || j < d) {
+                        p0 ^= qc_one_signs(b0[j]);
+                        if (WPT == 2) p1 ^= qc_one_signs(b1[j]);
+                    }
+                }
+                last_ok = !__syncthreads_or(((p0 | p1) & 0x80008000u) != 0);
+            } else if (!(ET && KIND != KIND_2NMS && l == L - 1)) {
+                // with the early stop (modes 1, 2), the barrier of the odd-row count closes the last layer
+                __syncthreads();
+            }
         }
         executed = it + 1;
         if (KIND == KIND_2NMS && it >= 1) {
@@ -244,6 +265,19 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
                 }
                 live &= ~gate;  // the pairs whose frames are codewords stop here
                 if (!live) {
+                    passed = true;
+                    break;
+                }
+            }
+        } else if (ET == 3) {
+            if (last_ok) {
+                // staged like mode 1: the first layers alone reject most words that are not codewords yet
+                constexpr int LS = L > 3 ? 2 : 1;
+                bool done = true;
+                if (L > 1) done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, 0, (L > 1 ? LS : 0), POW2, WPT>(Q, appb, k));
+                if (LS < L - 1 && done)
+                    done = !__syncthreads_or(qc_rows_unsatisfied<DT, EXACT, LS, (L > 1 ? L - 1 : 0), POW2, WPT>(Q, appb, k));
+                if (done) {
                     passed = true;
                     break;
                 }
@@ -500,6 +534,240 @@ __device__ __forceinline__ void qc_store_lane(const Job& J, const uint16_t* apph
                 if (v < n) acc |= bit(v) << j;
             }
             o[b] = (uint8_t)acc;
+        }
+    }
+}
+
+// ---- exact-gate early stop per frame pair (4 frames per CTA) ----
+//
+// true when row k of some layer in [L0, L1) has odd hard-decision parity in one of the two
+// frames of one pair-word of the 8-byte-per-variable APP; appb points at that pair's half
+// (byte 0 or 4 of each variable)
+template <int DT, bool EXACT, int L0, int L1, bool POW2>
+__device__ __noinline__ bool qc_rows_unsat_half(const QCParams& Q, const char* appb, int k)
+{
+    bool bad = false;
+    const int kb = 8 * k;
+#pragma unroll
+    for (int l = L0; l < L1; l++) {
+        const int d = EXACT ? DT : Q.deg[l];
+        uint32_t acc = 0;
+#pragma unroll
+        for (int j = 0; j < DT; j++)
+            if (EXACT || j < d)
+                acc ^= qc_one_signs(*reinterpret_cast<const uint32_t*>(appb + qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kb)));
+        bad |= (acc & 0x80008000u) != 0;
+    }
+    return bad;
+}
+
+// OR over the CTA of a 2-bit value (bit p: pair p): one barrier reduction per pair
+__device__ __forceinline__ unsigned cta_or_pairs(unsigned bits)
+{
+    const unsigned b0 = __syncthreads_or(bits & 1u) ? 1u : 0u;
+    return b0 | (__syncthreads_or(bits & 2u) ? 2u : 0u);
+}
+
+// The remaining pair of decode_qc_pairs_kernel decoding alone: its messages m, its APP
+// half at byte hoff of each 8-byte variable; runs from iteration it until the pair's
+// decisions are codewords (live = 0) or J.iters.  Every thread of the CTA calls it.
+template <int KIND, int DT, bool EXACT, int L, bool POW2>
+__device__ __forceinline__ void qc_one_pair(const QCParams& Q, const Job& J, char* appb, int hoff,
+                                            uint32_t (&m)[L][DT], const uint2 (*s_kb)[2], int& it, unsigned& live)
+{
+    constexpr bool LRN = KIND == KIND_LEARNED || KIND == KIND_LEARNED_OFS;
+    constexpr int LS = L > 3 ? 2 : 1;
+    const int k = threadIdx.x;
+    uint32_t ov = 0;  // unused extrinsic count of row()
+    while (live && it < J.iters) {
+        const int lt = LRN ? min(it, J.lut_its - 1) : 0;
+        bool last_bad = false;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+            const bool noclip = J.quirk && it == 0 && Q.cls[l];
+            int kk = 8 * k;
+            asm volatile("" : "+r"(kk));
+            int off[DT];
+            uint32_t b0[DT];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    off[j] = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk) + hoff;
+                    b0[j] = *reinterpret_cast<const uint32_t*>(appb + off[j]);
+                }
+            }
+            uint32_t lk = 0, lb = 0;
+            if (LRN) {
+                const uint2 kb = s_kb[lt][Q.cls[l]];
+                lk = kb.x;
+                lb = kb.y;
+            }
+            h2::row<KIND, DT, EXACT, 0>(b0, m[l], d, noclip, ov, lk, lb);
+#pragma unroll
+            for (int j = 0; j < DT; j++)
+                if (EXACT || j < d) *reinterpret_cast<uint32_t*>(appb + off[j]) = b0[j];
+            if (l == L - 1) {
+                uint32_t p0 = 0;
+#pragma unroll
+                for (int j = 0; j < DT; j++)
+                    if (EXACT || j < d) p0 ^= qc_one_signs(b0[j]);
+                last_bad = __syncthreads_or((p0 & 0x80008000u) != 0);
+            } else {
+                __syncthreads();
+            }
+        }
+        it++;
+        if (!last_bad) {
+            bool done = true;
+            if (L > 1) done = !__syncthreads_or(qc_rows_unsat_half<DT, EXACT, 0, (L > 1 ? LS : 0), POW2>(Q, appb + hoff, k));
+            if (done && LS < L - 1)
+                done = !__syncthreads_or(qc_rows_unsat_half<DT, EXACT, LS, (L > 1 ? L - 1 : 0), POW2>(Q, appb + hoff, k));
+            if (done) live = 0;
+        }
+    }
+}
+
+// The 4-frame QC decoder with each frame pair (frames 0, 1 and 2, 3 of word g: the two
+// fp16x2 pair-words) stopping on its own at the first iteration whose decisions are
+// codewords in both of its frames (the oracle's pair rule with an unbounded slack,
+// LDPC_EARLY_SLACK_ANY).  While both pairs decode, each layer updates both rows as in
+// decode_qc_kernel and the last layer's rows are checked from registers (per pair); the
+// other layers' rows only when a pair's last-layer rows all hold.  When one pair stops,
+// its APP and messages stay as they were and the CTA goes on with the other pair alone:
+// one row per layer, about 0.55 of a two-pair iteration (qc_one_pair, inlined once for
+// each pair so that its messages stay in their own registers).
+// The word's count is the iteration at which its last pair stopped.  Every kind but 2NMS.
+template <int KIND, int DT, bool EXACT, int L, bool POW2>
+__global__ void __launch_bounds__(256, 2) decode_qc_pairs_kernel(const __grid_constant__ QCParams Q, const Job J)
+{
+    static_assert(KIND != KIND_2NMS, "2NMS has its own early termination");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint2* app = reinterpret_cast<uint2*>(smem_raw);
+    char* appb = reinterpret_cast<char*>(smem_raw);
+    const long long g = J.word0 + blockIdx.x;
+    const int k = threadIdx.x;
+    constexpr bool LRN = KIND == KIND_LEARNED || KIND == KIND_LEARNED_OFS;
+    __shared__ uint2 s_kb[LRN ? QC_LUT_ITS : 1][2];
+    if (LRN && k < 2 * J.lut_its) {
+        uint2 kb = *reinterpret_cast<const uint2*>(J.lut + (k >> 1) * 256 + (k & 1) * 128);
+        if (KIND == KIND_LEARNED_OFS) kb.y = h2::add(kb.y, 0x37803780u);  // b + 15/32 = -offset (scale 1)
+        s_kb[k >> 1][k & 1] = kb;
+    }
+    Plan P;
+    P.n = Q.n;
+    read_group(P, J, g, [&](int v, uint32_t w) {
+        app[v] = make_uint2(Access<PackF16x2>::pair(w, 0), Access<PackF16x2>::pair(w, 2));
+    });
+    __syncthreads();
+
+    uint32_t msg[2][L][DT];
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int j = 0; j < DT; j++) msg[w][l][j] = 0;
+
+    constexpr int LS = L > 3 ? 2 : 1;  // staged check: layers [0, LS), then [LS, L - 1)
+    unsigned live = 3;  // bit p set while pair p is decoding (the same in every thread)
+    int it = 0;
+    uint32_t ov = 0;    // unused extrinsic count of row()
+    // both pairs
+    while (it < J.iters) {
+        const int lt = LRN ? min(it, J.lut_its - 1) : 0;
+        unsigned last_bad = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+            const bool noclip = J.quirk && it == 0 && Q.cls[l];
+            int kk = 8 * k;
+            asm volatile("" : "+r"(kk));
+            int off[DT];
+            uint32_t b0[DT], b1[DT];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    off[j] = qc_var_off<POW2>(Q, l * QC_MAX_DEG + j, kk);
+                    const uint2 v = *reinterpret_cast<const uint2*>(appb + off[j]);
+                    b0[j] = v.x;
+                    b1[j] = v.y;
+                }
+            }
+            uint32_t lk = 0, lb = 0;
+            if (LRN) {
+                const uint2 kb = s_kb[lt][Q.cls[l]];
+                lk = kb.x;
+                lb = kb.y;
+            }
+            h2::row<KIND, DT, EXACT, 0>(b0, msg[0][l], d, noclip, ov, lk, lb);
+            h2::row<KIND, DT, EXACT, 0>(b1, msg[1][l], d, noclip, ov, lk, lb);
+#pragma unroll
+            for (int j = 0; j < DT; j++)
+                if (EXACT || j < d) *reinterpret_cast<uint2*>(appb + off[j]) = make_uint2(b0[j], b1[j]);
+            if (l == L - 1) {
+                uint32_t p0 = 0, p1 = 0;
+#pragma unroll
+                for (int j = 0; j < DT; j++) {
+                    if (EXACT || j < d) {
+                        p0 ^= qc_one_signs(b0[j]);
+                        p1 ^= qc_one_signs(b1[j]);
+                    }
+                }
+                last_bad = cta_or_pairs(((p0 & 0x80008000u) ? 1u : 0u) | ((p1 & 0x80008000u) ? 2u : 0u));
+            } else {
+                __syncthreads();
+            }
+        }
+        it++;
+        unsigned gate = ~last_bad & 3u;  // pairs whose last-layer rows all hold
+        if (gate && L > 1) {
+            unsigned m = qc_rows_unsat_mask<DT, EXACT, 0, (L > 1 ? LS : 0), POW2, 2>(Q, appb, k);
+            gate &= ~cta_or_pairs(((m & 3u) ? 1u : 0u) | ((m & 12u) ? 2u : 0u));
+            if (gate && LS < L - 1) {
+                m = qc_rows_unsat_mask<DT, EXACT, LS, (L > 1 ? L - 1 : 0), POW2, 2>(Q, appb, k);
+                gate &= ~cta_or_pairs(((m & 3u) ? 1u : 0u) | ((m & 12u) ? 2u : 0u));
+            }
+        }
+        live &= ~gate;
+        if (live != 3) break;
+    }
+    // one pair left: it goes on alone with its own message registers and APP half
+    if (live == 1u)
+        qc_one_pair<KIND, DT, EXACT, L, POW2>(Q, J, appb, 0, msg[0], s_kb, it, live);
+    else if (live == 2u)
+        qc_one_pair<KIND, DT, EXACT, L, POW2>(Q, J, appb, 4, msg[1], s_kb, it, live);
+
+    write_group(P, J, g, [&](int v) { uint2 a = app[v]; return Access<PackF16x2>::unbias(a.x, a.y); });
+    if (J.iters_out && threadIdx.x == 0) J.iters_out[g - J.word0] = it;
+    if (J.synd_out) {
+        // a stopped pair holds codewords; the rest are checked on their final APP
+        const unsigned bad = live ? qc_rows_unsat_mask<DT, EXACT, 0, L, POW2, 2>(Q, appb, k) : 0u;
+        write_syndrome_flags(J, 4 * (g - J.word0), bad, 0xF, true);
+    }
+    if (J.app_out) {
+        uint32_t* ao = reinterpret_cast<uint32_t*>(J.app_out);
+        for (int v = threadIdx.x; v < Q.n; v += blockDim.x) {
+            uint2 a = app[v];
+            ao[(long long)v * J.total_words + g] = Access<PackF16x2>::unbias(a.x, a.y);
+        }
+    }
+    if (J.msg_out) {
+        uint32_t* mo = reinterpret_cast<uint32_t*>(J.msg_out);
+        long long e0 = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int d = EXACT ? DT : Q.deg[l];
+#pragma unroll
+            for (int j = 0; j < DT; j++) {
+                if (EXACT || j < d) {
+                    auto x = [](uint32_t h) { return (uint32_t)(uint8_t)(int8_t)(-__half2int_rn(__ushort_as_half((uint16_t)h))); };
+                    const uint32_t lo = msg[0][l][j], hi = msg[1][l][j];
+                    const uint32_t wv = x(lo & 0xffff) | (x(lo >> 16) << 8) | (x(hi & 0xffff) << 16) | (x(hi >> 16) << 24);
+                    mo[(e0 + (long long)k * d + j) * J.total_words + g] = wv;
+                }
+            }
+            e0 += (long long)Q.z * d;
         }
     }
 }

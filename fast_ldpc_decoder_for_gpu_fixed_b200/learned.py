@@ -192,18 +192,21 @@ class Trainer:
 
 
 def evaluate(code, kind, iters, ebn0, frames, seed=11, constants=None, n_codewords=256, words_per_call=4096,
-             pack="AUTO", early_stop=False):
+             pack="AUTO", early_stop=False, slack=None):
     """Frame and bit error rates and mean iterations of the int8 decoder ``kind``
     (with LDPC_LEARNED ``constants`` = (offsets, scales)) at ``ebn0`` dB over at
     least ``frames`` frames of seeded random codewords: channel kernel, decode
     with per-word iteration counts, error-count kernel.  Errors are counted over
     all n bits.  ``early_stop="frame"``: the per-frame early stop, and mean_iters is
-    per frame.  Returns dict(frames, bit_errors, frame_errors, fer, ber, mean_iters)."""
+    per frame.  ``slack``: the early stop's slack (ldpc_decoder_set_early_stop; None: the
+    library's default).  Returns dict(frames, bit_errors, frame_errors, fer, ber, mean_iters)."""
     import torch
     words = min(words_per_call, max(1, (frames + 3) // 4))
     dec = Decoder(code, kind, nb_frames=words, pack=pack, early_stop=early_stop)
     if constants is not None:
         dec.set_learned(*constants)
+    if early_stop and slack is not None:
+        dec.set_early_stop(True, slack)
     cw = torch.from_numpy(random_codewords(code, n_codewords, seed + 3)).cuda()
     llr = torch.empty(4 * words * code.n, dtype=torch.int8, device="cuda")
     hard = torch.empty(4 * words * code.n, dtype=torch.uint8, device="cuda")

@@ -143,6 +143,14 @@ void ldpc_code_destroy(ldpc_code* code);
 #define LDPC_FLAG_EARLY_STOP 1
 #define LDPC_EARLY_STOP_DEFAULT_SLACK 128
 
+/* A slack of at least LDPC_EARLY_SLACK_ANY makes every iteration a candidate: a word
+ * stops after the first iteration whose hard decisions are codewords.  The 4-frame
+ * QC register kernel (path 1, per-word stop) then keeps no odd-row count: it checks
+ * the rows of the last layer from the APP it has just updated, and the other layers'
+ * rows only when those all hold.  The other paths check the syndrome after every
+ * iteration. */
+#define LDPC_EARLY_SLACK_ANY 1073741824
+
 /* Per-frame early stop (implies LDPC_FLAG_EARLY_STOP): the rule above applied to
  * each frame alone (its own odd rows against `slack`, its own syndrome).  Decoder
  * path 5: the QC register kernel with 4 frames per CTA (ldpc_code_create_qc, the

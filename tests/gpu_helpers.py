@@ -19,7 +19,8 @@ def make_llr(kind, count, seed, sigma=None, value=0):
     return llr_gen.llr(kind, count, seed, sigma=sigma, value=value)
 
 
-def gpu_decode(code, kind, llr, iters, words, pack="AUTO", state=True, early_stop=False, constants=None):
+def gpu_decode(code, kind, llr, iters, words, pack="AUTO", state=True, early_stop=False, constants=None,
+               slack=None):
     """Decodes 4*words frames on cuda:0; returns hard [frames, n], app/msg (reference
     device layouts, bytes) and the per-word iteration counts."""
     import pytest
@@ -29,6 +30,8 @@ def gpu_decode(code, kind, llr, iters, words, pack="AUTO", state=True, early_sto
         dec = Decoder(code, kind, nb_frames=words, pack=pack, early_stop=early_stop)
         if constants is not None:
             dec.set_learned(*constants)
+        if slack is not None:
+            dec.set_early_stop(True, slack)
     except LdpcError as e:
         if e.code == -3:  # the code's state does not fit one CTA with this packing
             pytest.skip(str(e))

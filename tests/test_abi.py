@@ -41,6 +41,7 @@ def test_header_constants_match_python():
               "LDPC_FLAG_EARLY_STOP_FRAMES": _lib.FLAG_EARLY_STOP_FRAMES,
               "LDPC_BATCH_GRAPH": _lib.BATCH_GRAPH,
               "LDPC_EARLY_STOP_DEFAULT_SLACK": _lib.EARLY_STOP_DEFAULT_SLACK,
+              "LDPC_EARLY_SLACK_ANY": _lib.EARLY_SLACK_ANY,
               "LDPC_TRAIN_QUANTIZED": _lib.TRAIN_QUANTIZED, "LDPC_TRAIN_FRAME_LOSS": _lib.TRAIN_FRAME_LOSS}
     expect.update({v: k for k, v in _lib.ERRORS.items()})
     expect.update({"LDPC_" + k: v for k, v in _lib.KINDS.items() if k != "FMS"})

@@ -72,6 +72,47 @@ def test_early_stop_slack(cuda, slack):
         assert np.array_equal(d_hard.cpu().numpy().reshape(4 * words, code.n), ref["hard"])
 
 
+@pytest.mark.parametrize("kind", ["OMS", "NMS", "MS", "LEARNED", "LEARNED_OFS"])
+def test_early_stop_exact_gate_qc_kernel(cuda, kind):
+    """LDPC_EARLY_SLACK_ANY on the 4-frame QC kernel: its last-layer gate stops each word
+    at the first iteration whose decisions are codewords, like the oracle with an
+    unbounded slack (decisions, APP, messages, counts)."""
+    import torch
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
+    code = _qc()
+    words = 48
+    llr = np.concatenate([make_llr("awgn", 4 * 16 * code.n, 61 + i, sigma=llr_gen.sigma_for(e, 0.5))
+                          for i, e in enumerate((1.5, 2.25, 3.0))])
+    constants = None
+    if kind == "LEARNED":
+        constants = (np.array([[1, 1]] * 3 + [[0, 0]] * 7, dtype=np.int8), np.array([[112, 112]] * 10, dtype=np.uint8))
+    elif kind == "LEARNED_OFS":  # every scale 1.0: the offset-only learned kernel
+        kind, constants = "LEARNED", (np.array([[0, 0]] * 2 + [[1, 1]] * 8, dtype=np.int8),
+                                      np.array([[128, 128]] * 10, dtype=np.uint8))
+    if constants is not None:
+        oracle.set_learned(*constants)
+    ref = oracle.decode(code, kind, llr, 20, interleaved=False, want_state=True, early_stop=True,
+                        early_slack=_lib.EARLY_SLACK_ANY)
+    got = gpu_decode(code, kind, llr, 20, words, early_stop=True, constants=constants, slack=_lib.EARLY_SLACK_ANY)
+    assert got["info"]["path"] == 1
+    assert_same(got, ref)
+    assert ref["iters"].min() < 8 and ref["iters"].max() == 20
+    # the per-frame syndrome flags of the same decode
+    dec = Decoder(code, kind, nb_frames=words, early_stop=True)
+    if constants is not None:
+        dec.set_learned(*constants)
+    dec.set_early_stop(True, _lib.EARLY_SLACK_ANY)
+    d_llr = torch.from_numpy(llr).cuda()
+    d_hard = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    d_ok = torch.zeros(4 * words, dtype=torch.uint8, device="cuda")
+    dec.decode_device(d_llr, d_hard, words, 20, d_syndrome=d_ok)
+    torch.cuda.synchronize()
+    dec.close()
+    want_ok = (code.syndrome(ref["hard"]).max(axis=1) == 0).astype(np.uint8)
+    assert np.array_equal(d_ok.cpu().numpy(), want_ok)
+    assert np.array_equal(d_hard.cpu().numpy().reshape(4 * words, code.n), ref["hard"])
+
+
 def test_early_stop_learned(cuda):
     code = _qc()
     words = 16
