@@ -727,11 +727,11 @@ NOMINAL_INT_TOPS = 148 * 128 * 1.965e9 / 1e12
 
 # DRAM bytes (read + write) per frame of the dominant decode kernel, from one ncu capture
 # of a smaller batch of the same workload, scaled here by the frames of a launch
-# (profiles/decode_qc_oms_early_stop_qc3x6_n4096_32768f.md: 134.4 MB + 93.5 MB for
+# (profiles/decode_qc_exact_gate_qc3x6_n4096_32768f.md: 134.5 MB + 92.3 MB for
 # 32 768 frames; the kernel streams each frame's LLRs once and writes its decisions once,
 # so the traffic grows with the frames; path 3: profiles/decode_frame_ira_n64800_296f.md,
 # 20.0 MB + 74.4 MB for 296 frames of 12 iterations, most of the message traffic in L2)
-TRAFFIC_PER_FRAME = {1: (134.4e6 + 93.5e6) / 32768}
+TRAFFIC_PER_FRAME = {1: (134.5e6 + 92.3e6) / 32768}
 
 
 def _traffic(path, args):

@@ -120,6 +120,42 @@ def test_pairs_exact_gate_match_oracle(cuda, kind, constants):
     assert_same(got, ref)
 
 
+@pytest.mark.parametrize("kind,constants", [("OMS", None), ("LEARNED", LEARNED_GENERAL)], ids=["OMS", "LEARNED"])
+def test_pairs_exact_gate_large_batch(cuda, kind, constants):
+    """The per-pair exact-gate decode (decode_qc_pairs_kernel) on more words than the GPU
+    holds at once, at four noise levels: every pair's decisions, its word's count, the
+    syndrome flags and the final state must equal the oracle's pair rule."""
+    import torch
+    from gpu_helpers import assert_same
+    from fast_ldpc_decoder_for_gpu_fixed_b200 import _lib
+    code = qc_code()
+    words = 1200
+    llr = _mixed(code, words, 641, (1.75, 2.25, 2.75, 3.5))
+    if constants is not None:
+        oracle.set_learned(*constants)
+    ref = oracle.decode(code, kind, llr, 12, interleaved=False, want_state=True, early_stop=True,
+                        early_slack=_lib.EARLY_SLACK_ANY, pairs=True)
+    hard, its, syn = _run(code, kind, llr, 12, words, constants=constants, slack=_lib.EARLY_SLACK_ANY)
+    assert np.array_equal(its, ref["iters"])
+    assert np.array_equal(hard, ref["hard"])
+    assert np.array_equal(syn, _flags(code, ref["hard"]))
+    dec = Decoder(code, kind, nb_frames=words, early_stop="pairs")
+    if constants is not None:
+        dec.set_learned(*constants)
+    dec.set_early_stop(True, _lib.EARLY_SLACK_ANY)
+    d_llr = torch.from_numpy(llr).cuda()
+    d_hard = torch.zeros(4 * words * code.n, dtype=torch.uint8, device="cuda")
+    d_it = torch.zeros(words, dtype=torch.int32, device="cuda")
+    d_app = torch.zeros(4 * words * code.n, dtype=torch.int8, device="cuda")
+    d_msg = torch.zeros(4 * words * code.e, dtype=torch.int8, device="cuda")
+    dec.decode_device_state(d_llr, d_hard, words, 12, d_it, d_app, d_msg, stream=torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    dec.close()
+    got = {"hard": d_hard.cpu().numpy().reshape(4 * words, code.n), "iters": d_it.cpu().numpy(),
+           "app": d_app.cpu().numpy(), "msg": d_msg.cpu().numpy()}
+    assert_same(got, ref)
+
+
 def test_pairs_slack_and_toggle(cuda):
     code = qc_code()
     words = 24
