@@ -156,6 +156,20 @@ __global__ void __launch_bounds__(256, WPT == 2 ? 2 : 1) decode_qc_kernel(const 
     // 2NMS keeps the exact popcount, which its own rule tests against zero
     constexpr int CM = ((ET == 1 || ET == 2) && KIND != KIND_2NMS) ? 2 : 0;
 
+    // The LLRs of the word that will take this CTA's place, about one wave of resident CTAs
+    // (2 per SM) later, go into L2 by one TMA bulk prefetch, so that its prologue loads hit L2:
+    // a CTA that stops early starts its successor sooner, and the prologue's HBM latency
+    // would otherwise fall on every one of them.
+    if (WPT == 2 && threadIdx.x == 0 && !J.gen && !J.interleaved && (Q.n & 3) == 0) {
+        unsigned nsm;
+        asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+        const long long gn = g + 2 * (long long)nsm;
+        if (gn < J.word0 + (long long)gridDim.x) {
+            const int8_t* src = J.llr + 4 * (gn - J.word0) * (long long)Q.n;
+            if (((uintptr_t)src & 15) == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(4u * (unsigned)Q.n) : "memory");
+        }
+    }
     Plan P;  // only n is used by the shared prologue / epilogue helpers
     P.n = Q.n;
     read_group(P, J, g, [&](int v, uint32_t w) {
