@@ -144,11 +144,11 @@ void ldpc_code_destroy(ldpc_code* code);
 #define LDPC_EARLY_STOP_DEFAULT_SLACK 128
 
 /* A slack of at least LDPC_EARLY_SLACK_ANY makes every iteration a candidate: a word
- * stops after the first iteration whose hard decisions are codewords.  The 4-frame
- * QC register kernel (path 1, per-word stop) then keeps no odd-row count: it checks
- * the rows of the last layer from the APP it has just updated, and the other layers'
- * rows only when those all hold.  The other paths check the syndrome after every
- * iteration. */
+ * (or, with LDPC_FLAG_EARLY_STOP_PAIRS, a frame pair) stops after the first iteration
+ * whose hard decisions are codewords.  The 4-frame QC register kernel (path 1) then
+ * keeps no odd-row count: it checks the rows of the last layer from the APP it has
+ * just updated, and the other layers' rows only when those all hold.  The other paths
+ * check the syndrome after every iteration. */
 #define LDPC_EARLY_SLACK_ANY 1073741824
 
 /* Per-frame early stop (implies LDPC_FLAG_EARLY_STOP): the rule above applied to
