@@ -11,8 +11,9 @@ Default workload (the metric: learned-offset decoder vs plain OMS at equal FER):
                offsets in fast_ldpc_decoder_for_gpu_fixed_b200/trained/qc3x6_z256_T10_offsets.json,
                trained with every scale held at 1.0; --constants for another set, such as the
                offsets-and-scales set qc3x6_z256_T10.json,
-               syndrome early stop per 4-frame word; --early-unit pairs|frame for the
-               other units), kernel only, LLRs resident in HBM
+               syndrome early stop per frame pair, each pair stopping at its first codeword
+               iteration (LDPC_EARLY_SLACK_ANY); --early-unit word|frame and --slack for the
+               other rules), kernel only, LLRs resident in HBM
   plain_oms  : the plain 8-bit OMS kernel (offset 1, 10 fixed iterations) on the same
                batch and GPU; vs_plain_oms = value / plain_oms.value
   oms_early_stop : plain OMS with the same early stop; early_stop_gain = its value /
@@ -64,9 +65,9 @@ def parse():
                          "candidate; default: the library's)")
     ap.add_argument("--per-frame", action="store_true",
                     help="early stop per frame with slot refill (LDPC_FLAG_EARLY_STOP_FRAMES); same as --early-unit frame")
-    ap.add_argument("--early-unit", default="word", choices=["word", "pairs", "frame"],
+    ap.add_argument("--early-unit", default="pairs", choices=["word", "pairs", "frame"],
                     help="frames that stop together under the early stop of the learned workload: the 4-frame word "
-                         "(LDPC_FLAG_EARLY_STOP, default), each frame pair (LDPC_FLAG_EARLY_STOP_PAIRS) or each frame")
+                         "(LDPC_FLAG_EARLY_STOP), each frame pair (LDPC_FLAG_EARLY_STOP_PAIRS, default) or each frame")
     ap.add_argument("--fer-frames", type=int, default=1 << 20)
     ap.add_argument("--no-sweep", dest="sweep", action="store_false",
                     help="skip the learned-vs-plain ratio over Eb/N0 1.5..2.5 dB")

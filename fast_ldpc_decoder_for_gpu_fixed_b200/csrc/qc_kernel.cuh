@@ -668,6 +668,17 @@ __global__ void __launch_bounds__(256, 2) decode_qc_pairs_kernel(const __grid_co
         if (KIND == KIND_LEARNED_OFS) kb.y = h2::add(kb.y, 0x37803780u);  // b + 15/32 = -offset (scale 1)
         s_kb[k >> 1][k & 1] = kb;
     }
+    // the successor word's LLRs into L2, as in decode_qc_kernel
+    if (threadIdx.x == 0 && !J.gen && !J.interleaved && (Q.n & 3) == 0) {
+        unsigned nsm;
+        asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+        const long long gn = g + 2 * (long long)nsm;
+        if (gn < J.word0 + (long long)gridDim.x) {
+            const int8_t* src = J.llr + 4 * (gn - J.word0) * (long long)Q.n;
+            if (((uintptr_t)src & 15) == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(4u * (unsigned)Q.n) : "memory");
+        }
+    }
     Plan P;
     P.n = Q.n;
     read_group(P, J, g, [&](int v, uint32_t w) {
